@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark: Poisson solves/s at relative residual 1e-6 on the screened 2048^2 workload.
+
+Workload (one "step" = one solve): 2048x2048 RGBA f32 screened-Poisson,
+lambda = 0.01, a random 12-vertex star mask covering 30% (+-2%), relative
+residual 1e-6, at most 2000 sweeps per channel, omega 1.8 (the op's fixed SOR
+factor). Inputs come from the seeded generator in paintop_b200/synth.py.
+
+Arms:
+  default            the cuda backend. `value`: solves/s with inputs resident in
+                     HBM (device pointers); `e2e`: solves/s through the C ABI with
+                     pinned host buffers, host<->device copies inside the timed
+                     region.
+  --impl reference   the reference op's CPU algorithm (the oracle restatement of
+                     crates/paintop-cpu/src/poisson.rs) on the host cores, one
+                     channel solve per step as a bounded sample.
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own instance
+(weak scaling, no data-path collective); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="screened_2048", width=2048, height=2048, channels=4, lam=0.01,
+                tolerance=1e-6, max_iterations=2000, omega=1.8)
+METRIC = "Poisson solves/s @ rel-res 1e-6 (screened 2048x2048 RGBA, lambda 0.01, star 30%)"
+UNIT = "solves/s"
+
+# algorithmic bytes per interior unknown per channel: one red+black sweep reads
+# u, b' and the cell flag and writes u (13 B); one FP64 residual evaluation
+# reads u, b' and the cell flag (9 B)
+BYTES_PER_SWEEP = 13
+BYTES_PER_RESIDUAL = 9
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """DRAM bytes per k_solve launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "k_solve_screened_2048.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_instance(seed: int):
+    from paintop_b200 import synth
+    return synth.screened_2048(seed)
+
+
+def reference_arm(args):
+    """CPU arm: the oracle restatement of the reference op, single thread."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    inst = make_instance(1)
+    W, H, C = inst.width, inst.height, inst.channels
+    src = inst.source.reshape(-1)
+    tgt = inst.target.reshape(-1)
+    mask = inst.mask.reshape(-1)
+    # one channel per step: the reference solves channels serially and
+    # independently, so a solve costs the sum of its channel solves
+    chans = [np.ascontiguousarray(x.reshape(H, W, C)[:, :, k]).reshape(-1)
+             for x in (src, tgt) for k in range(C)]
+    srcs, tgts = chans[:C], chans[C:]
+
+    def step(k):
+        c = k % C
+        t0 = time.perf_counter()
+        O.blend_channels(srcs[c], tgts[c], mask, 1, W, H, WORKLOAD["max_iterations"],
+                         WORKLOAD["tolerance"], WORKLOAD["lam"], WORKLOAD["omega"])
+        return time.perf_counter() - t0
+
+    for k in range(args.warmup):
+        step(k)
+    times = [step(args.warmup + k) for k in range(args.steps)]
+    per_channel = float(np.mean(times))
+    value = 1.0 / (C * per_channel)
+    sample = (f"one channel of the {W}x{H}x{C} solve per step (channels rotate), "
+              f"solve time = {C} x mean channel time")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_channel * C * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded sinusoid-plus-noise images, star polygon mask)",
+        "config": {"workload": WORKLOAD["name"], **{k: v for k, v in WORKLOAD.items()
+                                                      if k != "name"}},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample(inst):
+    """Time one full solve (all channels) of the oracle on one host core."""
+    from oracle import oracle as O
+    O.build()
+    W, H, C = inst.width, inst.height, inst.channels
+    t0 = time.perf_counter()
+    O.blend_channels(inst.source.reshape(-1), inst.target.reshape(-1), inst.mask.reshape(-1), C,
+                     W, H, WORKLOAD["max_iterations"], WORKLOAD["tolerance"], WORKLOAD["lam"],
+                     WORKLOAD["omega"])
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"one full {W}x{H}x{C} solve ({dt:.1f} s) of the restated reference op"}
+
+
+def gpu_arm(args):
+    import torch
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    from paintop_b200 import _lib
+    ctx = _lib.Context(dev.index)
+
+    inst = make_instance(1 + rank)
+    W, H, C = inst.width, inst.height, inst.channels
+    n_img, n_mask = W * H * C, W * H
+    src_h = torch.from_numpy(inst.source.reshape(-1)).pin_memory()
+    tgt_h = torch.from_numpy(inst.target.reshape(-1)).pin_memory()
+    mask_h = torch.from_numpy(inst.mask.reshape(-1)).pin_memory()
+    out_h = torch.empty(n_img, dtype=torch.float32).pin_memory()
+    src_d, tgt_d, mask_d = src_h.to(dev), tgt_h.to(dev), mask_h.to(dev)
+    out_d = torch.empty(n_img, dtype=torch.float32, device=dev)
+    hist_cap = WORKLOAD["max_iterations"]
+    hist_d = torch.empty(C * hist_cap, dtype=torch.float64, device=dev)
+    hist_h = torch.empty(C * hist_cap, dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    interior = int((inst.mask[1:-1, 1:-1] > 0.5).sum())
+
+    import ctypes as Ct
+    L = _lib.lib()
+    reps = (_lib.PtReport * (C + 1))()
+
+    def problem(device_ptrs: bool):
+        s, t, m = (src_d, tgt_d, mask_d) if device_ptrs else (src_h, tgt_h, mask_h)
+        return _lib.PtProblem(W, H, C, s.data_ptr(), t.data_ptr(), m.data_ptr(),
+                              WORKLOAD["lam"], WORKLOAD["max_iterations"], WORKLOAD["tolerance"],
+                              WORKLOAD["omega"],
+                              _lib.PT_FLAG_DEVICE_POINTERS if device_ptrs else 0, None)
+
+    p_dev, p_host = problem(True), problem(False)
+
+    def solve(device_ptrs: bool):
+        if device_ptrs:
+            st = L.pt_poisson_solve(ctx.h, Ct.byref(p_dev), out_d.data_ptr(), reps,
+                                    hist_d.data_ptr())
+        else:
+            st = L.pt_poisson_solve(ctx.h, Ct.byref(p_host), out_h.data_ptr(), reps,
+                                    hist_h.data_ptr())
+        if st != _lib.PT_OK:
+            raise _lib.CudaError(st, ctx.last_error())
+
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident arm -------------------------------------------------
+    for _ in range(args.warmup):
+        solve(True)
+    barrier()
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    kernel_ms, iters, refines, launches = [], [], [], 0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        solve(True)
+        k, _, nl = ctx.last_timing()
+        kernel_ms.append(k)
+        launches += nl
+        iters.append([reps[c].iterations for c in range(C)])
+        refines.append([reps[c].refinements for c in range(C)])
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    clocks = sampler.stop()
+    converged = all(reps[c].converged for c in range(C))
+    worst_res = max(reps[c].final_residual for c in range(C))
+
+    # ---- end-to-end arm (pinned host buffers through the C ABI) --------------
+    for _ in range(max(1, args.warmup)):
+        solve(False)
+    barrier()
+    ev2 = torch.cuda.Event(enable_timing=True)
+    ev3 = torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(args.steps):
+        solve(False)
+        launches += ctx.last_timing()[2]
+    ev3.record(stream)
+    ev3.synchronize()
+    barrier()
+    e2e_elapsed = max_over_ranks(ev2.elapsed_time(ev3) / 1e3)
+
+    value = ws * args.steps / elapsed
+    e2e_value = ws * args.steps / e2e_elapsed
+    h2d = 4 * (2 * n_img + n_mask)
+    d2h = 4 * n_img + 8 * C * hist_cap + 64 * (C + 1)
+
+    # roofline for the persistent solve kernel
+    it = np.array(iters, dtype=np.float64)       # steps x C sweeps
+    rf = np.array(refines, dtype=np.float64)
+    alg_bytes = interior * (BYTES_PER_SWEEP * it.sum(axis=1) +
+                            BYTES_PER_RESIDUAL * (it.sum(axis=1) + rf.sum(axis=1)))
+    kms = np.array(kernel_ms)
+    achieved = float(np.mean(alg_bytes / (kms / 1e3)) / 1e9)
+    peak, peak_kind = _peaks()
+    traffic = _profile_traffic()
+
+    line = None
+    if rank == 0:
+        cpu = cpu_baseline_sample(inst) if (ws == 1 and not args.no_cpu_baseline) else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded sinusoid-plus-noise images, star polygon mask)",
+            "config": {"workload": WORKLOAD["name"], "width": W, "height": H, "channels": C,
+                       "lambda": WORKLOAD["lam"], "tolerance": WORKLOAD["tolerance"],
+                       "max_iterations": WORKLOAD["max_iterations"], "omega": WORKLOAD["omega"],
+                       "interior_px": interior, "l2": "inputs larger than L2 (151 MB/solve)",
+                       "tile_config": ctx.last_config(),
+                       "parallelism": f"instances sharded over {ws} GPU(s)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "ptk::k_solve", "peak_kind": peak_kind,
+                         "kernel_ms_mean": float(kms.mean()),
+                         "algorithmic_bytes_per_launch": float(alg_bytes.mean())},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
+                       "converged": converged, "worst_final_residual": worst_res},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "cuda":
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

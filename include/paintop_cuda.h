@@ -1,0 +1,221 @@
+/*
+ * paintop_cuda.h -- C ABI of the B200 `cuda` backend for paintop's Poisson /
+ * screened-Poisson ops (`repair.poisson_blend@1`, `repair.screened_poisson@1`).
+ *
+ * This is the seam a Rust FFI crate binds. In the reference, an op backend is a
+ * Rust `OpImplementation` (crates/paintop-core/src/executor/op_impl.rs:51-70)
+ * registered with `ImplRegistry::register_backend`
+ * (crates/paintop-core/src/executor/op_impl.rs:142-172); its compute() calls
+ * `blend_channels` (crates/paintop-cpu/src/poisson_blend.rs:168-236), which calls
+ * `poisson::solve` (crates/paintop-cpu/src/poisson.rs:167-240) per channel. The
+ * entry points below replace that chain:
+ *
+ *   pt_poisson_solve        replaces blend_channels + solve for one image
+ *                           (poisson_blend.rs:168-246, poisson.rs:167-240)
+ *   pt_poisson_solve_batch  many independent images in one persistent launch
+ *                           (no reference counterpart: the reference solves one
+ *                           image per op call)
+ *   pt_op_compute           replaces PoissonBlend::compute / ScreenedPoisson::compute
+ *                           (poisson_blend.rs:534-600, screened_poisson.rs:361-430)
+ *                           including resolve_controls / check_shapes validation
+ *                           (poisson_blend.rs:102-139,417-445; screened_poisson.rs:66-112)
+ *   pt_status_str           message for a status code (the reference's typed
+ *                           errors: crates/paintop-ir/src/error.rs:23-114)
+ *
+ * Conventions: plain C types only; all image buffers are row-major,
+ * channel-interleaved f32 (the reference's ResourceValue samples,
+ * crates/paintop-core/src/executor/value.rs:35-69). Unless PT_FLAG_DEVICE_POINTERS
+ * is set, every pointer is a host pointer owned by the caller. The library owns
+ * device memory inside the context (reused across calls, grown to a high-water
+ * mark). No function aborts, throws or panics across the ABI. A context is
+ * internally serialised by a mutex; distinct contexts are independent, so the
+ * library is reentrant across contexts. Results are deterministic: a rerun on the
+ * same device with the same inputs is byte-identical.
+ */
+#ifndef PAINTOP_CUDA_H
+#define PAINTOP_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Mapping to the reference's error classes
+ * (crates/paintop-ir/src/error.rs:23-114): PT_NO_DEVICE -> Policy (exit 4,
+ * mirrors E_GPU_UNAVAILABLE in crates/paintop-wgpu/src/gpu/error.rs:17);
+ * PT_INVALID_ARG -> Schema/Semantic as reported in pt_error; the rest ->
+ * Execution (exit 5). */
+typedef enum pt_status {
+  PT_OK = 0,
+  PT_NO_DEVICE = 1,     /* no CUDA device / driver, or the device is not sm_100 */
+  PT_INVALID_ARG = 2,   /* a null pointer, a bad size, or an out-of-range control */
+  PT_LAUNCH_FAILED = 3, /* a CUDA launch or copy failed */
+  PT_TIMEOUT = 4,       /* the device watchdog expired (bounded waits, wall budget) */
+  PT_OOM = 5,           /* device or pinned-host allocation failed */
+  PT_INTERNAL = 6       /* any other failure */
+} pt_status;
+
+/* pt_problem.flags */
+#define PT_FLAG_WARM_START 0x1u      /* initial_guess holds the interior start values */
+#define PT_FLAG_DEVICE_POINTERS 0x2u /* every buffer (inputs, outputs, history) is device memory */
+#define PT_FLAG_OMEGA_AUTO 0x4u      /* ignore `omega`; pick the red-black optimum per channel */
+
+/* Stop reasons: the kebab-case SolverStopReason of
+ * crates/paintop-ir/src/resource.rs:1185-1194 in declaration order. */
+#define PT_STOP_CONVERGED 0
+#define PT_STOP_MAX_ITERATIONS 1
+#define PT_STOP_STALLED 2
+
+typedef struct pt_ctx pt_ctx;
+
+/* One image to solve: the arguments of blend_channels (poisson_blend.rs:168-175)
+ * plus the SolveControls (poisson.rs:145-154). For poisson_blend,
+ * source_or_guidance = source and target_or_anchor = target; for
+ * screened_poisson, guidance and anchor (screened_poisson.rs:394-401). */
+typedef struct pt_problem {
+  uint32_t width, height, channels;
+  const float *source_or_guidance; /* width*height*channels */
+  const float *target_or_anchor;   /* width*height*channels */
+  const float *mask;               /* width*height coverage; > 0.5 is interior */
+  double lambda;                   /* >= 0, finite */
+  uint32_t max_iterations;         /* sweeps per channel */
+  double tolerance;                /* relative residual ||r_k|| / ||r(anchor)|| */
+  double omega;                    /* SOR factor in (0, 2); the op uses 1.8 */
+  uint32_t flags;                  /* PT_FLAG_* */
+  const float *initial_guess;      /* width*height*channels or NULL */
+} pt_problem;
+
+/* SolveReport (poisson.rs:126-141) without the history vector, plus what the
+ * GPU method adds. */
+typedef struct pt_report {
+  uint32_t iterations;  /* sweeps run (the last block is clipped exactly) */
+  int32_t converged;    /* 1 iff stop_reason == PT_STOP_CONVERGED */
+  int32_t stop_reason;  /* PT_STOP_* */
+  double tolerance;     /* the requested tolerance */
+  double final_residual;/* == history[iterations-1], an FP64 residual; 0 if none */
+  uint32_t history_len; /* == iterations */
+  double omega_used;    /* the SOR factor the sweeps used */
+  uint32_t refinements; /* FP64 residual-correction steps (incl. the final check) */
+  int32_t channel;      /* the channel index (for the worst entry: which channel) */
+} pt_report;
+
+pt_status pt_ctx_create(int device, pt_ctx **out);
+pt_status pt_ctx_destroy(pt_ctx *ctx);
+
+/* Solve one image, every channel independently.
+ *   out_candidate: width*height*channels f32 (caller-owned); equals the target
+ *                  bit for bit at every non-interior pixel.
+ *   reports:       channels + 1 entries: one per channel, then the worst channel
+ *                  by (iterations, final_residual) as worse_of (poisson_blend.rs:240-246).
+ *   history:       channels * max_iterations doubles, channel-major (may be NULL).
+ */
+pt_status pt_poisson_solve(pt_ctx *ctx, const pt_problem *p, float *out_candidate,
+                           pt_report *reports, double *history);
+
+/* Solve n independent images in one persistent launch. outs[i], reports[i]
+ * (channels_i + 1 entries) and histories[i] (channels_i * max_iterations_i, or
+ * NULL; `histories` itself may be NULL) follow pt_poisson_solve. */
+pt_status pt_poisson_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n,
+                                 float *const *outs, pt_report *const *reports,
+                                 double *const *histories);
+
+/* ---- op-level entry (the OpImplementation::compute seam) ------------------ */
+
+/* Resource kinds of an input port (crates/paintop-ir ResourceKind). */
+#define PT_KIND_IMAGE 0
+#define PT_KIND_MASK 1
+
+typedef struct pt_port {
+  const char *name;      /* "source"/"target"/"mask" or "guidance"/"anchor"/"mask" */
+  uint32_t kind;         /* PT_KIND_* */
+  uint32_t width, height;
+  uint32_t channels;     /* channel count of the layout (mask: 1) */
+  const float *samples;  /* width*height*channels, host memory */
+  size_t sample_count;   /* length of samples */
+} pt_port;
+
+/* The reference's Error (crates/paintop-ir/src/error.rs): class token
+ * ("schema", "reference", "type", "semantic", "policy", "execution"), stable
+ * code (e.g. "E_POISSON_BLEND_PARAM") and message. */
+typedef struct pt_error {
+  char error_class[16];
+  char code[40];
+  char message[256];
+  char actual[96];
+} pt_error;
+
+/* SolverData (crates/paintop-ir/src/resource.rs:1130-1178) built as
+ * solver_data() does (poisson_blend.rs:249-266). */
+typedef struct pt_solver_data {
+  char kind[24];          /* "poisson" or "screened-poisson" */
+  uint32_t steps;
+  double stability_number;
+  double stability_limit;
+  int32_t stable;
+  double total_energy;
+  uint32_t iterations;
+  int32_t stop_reason;    /* PT_STOP_* */
+  int32_t converged;
+  double tolerance;
+  double final_residual;
+  uint32_t history_len;   /* residual_history length */
+} pt_solver_data;
+
+/* Run the op (ctx may be NULL: the inputs and params are then validated and,
+ * if valid, PT_NO_DEVICE is returned with E_CUDA_UNAVAILABLE). op_id is
+ * "repair.poisson_blend@1" or "repair.screened_poisson@1";
+ * params_json the op's JSON params object (e.g. {"tolerance":1e-6}). On PT_OK,
+ * candidate (width*height*channels f32, caller-owned) and *solver are filled,
+ * residual_history receives min(history_len, history_cap) entries and
+ * *all_finite the report's all_finite flag. On PT_INVALID_ARG, *err carries the
+ * reference's error class, code and message. */
+pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port *inputs,
+                        uint32_t n_inputs, const char *params_json, float *candidate,
+                        size_t candidate_count, pt_solver_data *solver,
+                        double *residual_history, uint32_t history_cap,
+                        int32_t *all_finite, pt_error *err);
+
+const char *pt_status_str(pt_status s);
+
+/* Last CUDA / watchdog detail recorded on this context ("" if none). */
+const char *pt_ctx_last_error(const pt_ctx *ctx);
+
+/* Wall budget of one persistent solve in seconds (default 600). A solve that
+ * exceeds it stops at the next step boundary and returns PT_TIMEOUT; the
+ * context stays usable. */
+pt_status pt_ctx_set_budget(pt_ctx *ctx, double seconds);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or events with the library's. */
+void *pt_ctx_stream(const pt_ctx *ctx);
+
+/* Timing of the context's last solve, from CUDA events on its stream: the
+ * persistent solve kernel alone, the whole call (first upload to last
+ * download), and the number of kernels the call launched. */
+pt_status pt_ctx_last_timing(const pt_ctx *ctx, double *solve_kernel_ms, double *call_ms,
+                             int64_t *kernel_launches);
+
+/* ---- tile configurations and the autotuner (no reference counterpart: the
+ * reference has a single sequential sweep) -------------------------------- */
+
+/* Number of compiled tile configurations (sweeps per step S, tile shape). */
+uint32_t pt_tile_config_count(void);
+pt_status pt_tile_config_info(uint32_t idx, int32_t *sweeps_per_step, int32_t *tile_w,
+                              int32_t *tile_h);
+/* Force a configuration for this context's solves (-1: use the tuned table). */
+pt_status pt_ctx_set_config(pt_ctx *ctx, int32_t cfg);
+/* The configuration the context's last solve used. */
+int32_t pt_ctx_last_config(const pt_ctx *ctx);
+/* Time every configuration on this batch, store the fastest in the shape-keyed
+ * table (persisted to $PAINTOP_CUDA_TUNE_TABLE when set) and report it. Later
+ * solves of the same shape read the table; they never re-time. */
+pt_status pt_autotune(pt_ctx *ctx, const pt_problem *ps, uint32_t n, uint32_t repeats,
+                      float *const *outs, pt_report *const *reports, int32_t *chosen,
+                      double *ms_per_config);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAINTOP_CUDA_H */

@@ -1,0 +1,157 @@
+// autotune.cpp -- choice of tile configuration (sweeps per step S, tile shape).
+//
+// The iterate does not depend on the configuration (temporal blocking
+// reproduces whole-grid red-black sweeps exactly), but the refinement points
+// and the order of the FP64 partial sums do, so a solve must never re-time its
+// configuration: the choice comes from a fixed table keyed by the problem's
+// shape. The table starts from built-in defaults and can be replaced by the
+// measured optimum of pt_autotune (see tune_table.json written by it).
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+#include <map>
+
+#include "../../include/paintop_cuda.h"
+#include "ctx.h"
+#include "rbsor_launch.h"
+
+namespace {
+
+std::mutex g_mu;
+std::map<uint32_t, int> g_table;  // key -> config index
+bool g_loaded = false;
+
+// Shape key: log2 of the total pixel count (all channels), log2 of the largest
+// image, whether lambda is zero for all, batch > 1.
+uint32_t shape_key(const pt_problem *ps, uint32_t n) {
+  double total = 0.0, largest = 1.0;
+  bool lam0 = true;
+  for (uint32_t i = 0; i < n; ++i) {
+    const double px = (double)ps[i].width * ps[i].height;
+    total += px * ps[i].channels;
+    if (px > largest) largest = px;
+    if (ps[i].lambda != 0.0) lam0 = false;
+  }
+  const uint32_t lt = (uint32_t)std::max(0.0, std::floor(std::log2(std::max(total, 1.0))));
+  const uint32_t ll = (uint32_t)std::max(0.0, std::floor(std::log2(largest)));
+  return (lt << 16) | (ll << 8) | (lam0 ? 2u : 0u) | (n > 1 ? 1u : 0u);
+}
+
+const char *table_path() {
+  const char *p = std::getenv("PAINTOP_CUDA_TUNE_TABLE");
+  return p && *p ? p : nullptr;
+}
+
+void load_table_locked() {
+  if (g_loaded) return;
+  g_loaded = true;
+  const char *path = table_path();
+  if (!path) return;
+  FILE *f = std::fopen(path, "r");
+  if (!f) return;
+  unsigned key = 0;
+  int cfg = 0;
+  // one "key cfg" pair per line
+  while (std::fscanf(f, "%x %d", &key, &cfg) == 2)
+    if (cfg >= 0 && cfg < ptk::tile_config_count()) g_table[key] = cfg;
+  std::fclose(f);
+}
+
+void save_table_locked() {
+  const char *path = table_path();
+  if (!path) return;
+  FILE *f = std::fopen(path, "w");
+  if (!f) return;
+  for (const auto &kv : g_table) std::fprintf(f, "%08x %d\n", kv.first, kv.second);
+  std::fclose(f);
+}
+
+}  // namespace
+
+// Built-in default: the tall 3-sweep tile unless the whole batch is small
+// enough that shorter tiles are needed to give every SM work.
+int ptk_default_config(const pt_problem *ps, uint32_t n) {
+  double total = 0.0;
+  for (uint32_t i = 0; i < n; ++i) total += (double)ps[i].width * ps[i].height * ps[i].channels;
+  return total < 4.0e6 ? 3 : 2;
+}
+
+int ptk_choose_config(pt_ctx *ctx, const pt_problem *ps, uint32_t n) {
+  if (ctx && ctx->forced_cfg >= 0) return ctx->forced_cfg;
+  std::lock_guard<std::mutex> lock(g_mu);
+  load_table_locked();
+  auto it = g_table.find(shape_key(ps, n));
+  if (it != g_table.end()) return it->second;
+  return ptk_default_config(ps, n);
+}
+
+pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
+                          pt_report *const *reports, double *const *histories, int force_cfg);
+
+extern "C" {
+
+uint32_t pt_tile_config_count(void) { return (uint32_t)ptk::tile_config_count(); }
+
+pt_status pt_tile_config_info(uint32_t idx, int32_t *sweeps_per_step, int32_t *tile_w,
+                              int32_t *tile_h) {
+  if (idx >= (uint32_t)ptk::tile_config_count()) return PT_INVALID_ARG;
+  const ptk::TileConfig tc = ptk::tile_config((int)idx);
+  if (sweeps_per_step) *sweeps_per_step = tc.S;
+  if (tile_w) *tile_w = tc.tw;
+  if (tile_h) *tile_h = tc.th;
+  return PT_OK;
+}
+
+pt_status pt_ctx_set_config(pt_ctx *ctx, int32_t cfg) {
+  if (!ctx || cfg >= ptk::tile_config_count()) return PT_INVALID_ARG;
+  ctx->forced_cfg = cfg < 0 ? -1 : cfg;
+  return PT_OK;
+}
+
+int32_t pt_ctx_last_config(const pt_ctx *ctx) { return ctx ? ctx->last_cfg : -1; }
+
+// Time every configuration on this batch (repeats runs each, best time kept),
+// record the fastest in the table under the batch's shape key and persist the
+// table to $PAINTOP_CUDA_TUNE_TABLE when set. ms_per_config (optional) receives
+// pt_tile_config_count() entries.
+pt_status pt_autotune(pt_ctx *ctx, const pt_problem *ps, uint32_t n, uint32_t repeats,
+                      float *const *outs, pt_report *const *reports, int32_t *chosen,
+                      double *ms_per_config) {
+  if (!ctx || !ps || n == 0 || !outs || !reports) return PT_INVALID_ARG;
+  if (repeats == 0) repeats = 1;
+  int best = -1;
+  double best_ms = 0.0;
+  for (int cfg = 0; cfg < ptk::tile_config_count(); ++cfg) {
+    double cfg_best = -1.0;
+    for (uint32_t r = 0; r < repeats; ++r) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, ctx->stream);
+      const pt_status st = ptk_solve_batch(ctx, ps, n, outs, reports, nullptr, cfg);
+      cudaEventRecord(b, ctx->stream);
+      cudaEventSynchronize(b);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      if (st != PT_OK) return st;
+      if (cfg_best < 0 || ms < cfg_best) cfg_best = ms;
+    }
+    if (ms_per_config) ms_per_config[cfg] = cfg_best;
+    if (best < 0 || cfg_best < best_ms) { best = cfg; best_ms = cfg_best; }
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    load_table_locked();
+    g_table[shape_key(ps, n)] = best;
+    save_table_locked();
+  }
+  if (chosen) *chosen = best;
+  return PT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,679 @@
+// rbsor_kernels.cu -- device kernels of the red-black SOR solver (sm_100a).
+// See rbsor.cuh for the method, the HBM layout and the control scheme.
+#include "rbsor.cuh"
+#include "rbsor_launch.h"
+
+#include <cmath>
+#include <cstdio>
+
+namespace ptk {
+
+// ----------------------------------------------------------------------------
+// small device helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_vol(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
+
+// Deterministic block sum: fixed xor-butterfly inside each warp, then warps in
+// index order. The total is valid in thread 0. Uses sred[0..kWarps).
+__device__ __forceinline__ double block_sum(double v, double *sred) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) sred[warp] = v;
+  __syncthreads();
+  double tot = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kWarps; ++w) tot += sred[w];
+  __syncthreads();
+  return tot;
+}
+
+__device__ __forceinline__ long long plane_index(const SysDesc &d, int c, int y, int i) {
+  return d.off + (long long)c * d.plane + (long long)y * d.pw + i;
+}
+
+// Bounded grid barrier over a cooperative launch (all blocks co-resident).
+// Returns false if an error was raised anywhere or the wait gave up.
+__device__ bool grid_sync(unsigned *bar, int *err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen = ld_acquire(bar + 1);
+    __threadfence();
+    const unsigned prev = atomicAdd(bar, 1u);
+    if (prev == gridDim.x - 1) {
+      // every block has arrived: snapshot the done counter for this step (a
+      // block that leaves the barrier early may already bump bar[2] in the next
+      // step, so blocks must not read bar[2] itself to decide to exit)
+      atomicExch(bar + 3, atomicAdd(bar + 2, 0u));
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      // A step is at most milliseconds; 20 s without a release means something
+      // is wrong: record it and leave instead of waiting forever.
+      const unsigned long long give_up = gtimer() + 20ull * 1000000000ull;
+      while (ld_acquire(bar + 1) == gen) {
+        if (ld_vol(err) != 0) { ok = 0; break; }
+        if (gtimer() > give_up) { atomicCAS(err, 0, KERR_BARRIER_TIMEOUT); ok = 0; break; }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    s_ok = ok && (ld_vol(err) == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ----------------------------------------------------------------------------
+// geometry of one tile configuration
+// ----------------------------------------------------------------------------
+template <int S, int TH>
+struct Geo {
+  static constexpr int H = halo_y(S);
+  static constexpr int HX = halo_x(S);
+  static constexpr int TW = tile_w(S);
+  static constexpr int LH = TH + 2 * H;
+  static constexpr int PLANE = LH * kPWL;  // elements per shared plane
+  static constexpr int XOFF = HX - H;      // unused loaded columns on each side
+  static_assert(HX >= H, "x halo must cover the sweep halo");
+  static_assert(TW > 0 && TW % 8 == 0, "tile width must keep plane loads 16-byte aligned");
+  static constexpr size_t kSmem = (size_t)2 * PLANE * sizeof(float)   // e
+                                  + (size_t)2 * PLANE * sizeof(float) // g
+                                  + (size_t)2 * PLANE                 // cell
+                                  + 64 * sizeof(double);              // reduction scratch
+};
+
+// ----------------------------------------------------------------------------
+// assembly kernels
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ bool interior_at(const SysDesc &d, int x, int y) {
+  if (d.W < 3 || d.H < 3) return false;                  // poisson.rs:342-345
+  if (x < 1 || y < 1 || x > d.W - 2 || y > d.H - 2) return false;
+  return d.mask[(long long)y * d.W + x] > 0.5f;           // poisson.rs:349 (strict >)
+}
+
+// Interior cells per tile (owned region only).
+__global__ void k_tile_count(KParams P, int TW, int TH) {
+  const Tile tl = P.tiles[blockIdx.x];
+  const SysDesc d = P.sys[tl.sys];
+  int n = 0;
+  const int x0 = tl.tx * TW, y0 = tl.ty * TH;
+  for (int k = threadIdx.x; k < TW * TH; k += blockDim.x) {
+    const int x = x0 + k % TW, y = y0 + k / TW;
+    if (x < d.W && y < d.H && interior_at(d, x, y)) ++n;
+  }
+  __shared__ int s[32];
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = n;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
+    P.tcount[blockIdx.x] = t;
+  }
+}
+
+__device__ __forceinline__ bool tile_support(const KParams &P, const SysDesc &d, int tx, int ty) {
+  for (int dy = -1; dy <= 1; ++dy)
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int x = tx + dx, y = ty + dy;
+      if (x < 0 || y < 0 || x >= d.ntx || y >= d.nty) continue;
+      if (P.tcount[d.tile0 + y * d.ntx + x] > 0) return true;
+    }
+  return false;
+}
+
+// Assemble one tile of one system (owned cells only). Writes cell, bp, u, g and
+// zeroes e0/e1; accumulates ||r(anchor)||^2 and ||r(u_init)||^2 partials.
+// Arithmetic of b and r follows poisson.rs:364-373 (guidance_laplacian) and
+// poisson.rs:315-321 (residual), operand for operand.
+__global__ void __launch_bounds__(kThreads) k_assemble(KParams P, int TW, int TH) {
+  __shared__ double sred[kWarps];
+  const int t = blockIdx.x;
+  const Tile tl = P.tiles[t];
+  const SysDesc d = P.sys[tl.sys];
+  if (!tile_support(P, d, tl.tx, tl.ty)) return;
+  const int C = d.C, ch = d.chan;
+  const double lam = d.lambda;
+  double acc_a = 0.0, acc_u = 0.0;
+  const int half = TW / 2;
+  for (int k = threadIdx.x; k < 2 * TH * half; k += blockDim.x) {
+    const int c = k / (TH * half);
+    const int r = k - c * (TH * half);
+    const int y = tl.ty * TH + r / half;
+    const int i = tl.tx * half + r % half;
+    if (y >= d.H || i >= d.pw) continue;
+    const int x = 2 * i + ((c + y) & 1);
+    const long long o = plane_index(d, c, y, i);
+    P.e0[o] = 0.0f;
+    P.e1[o] = 0.0f;
+    if (x >= d.W) {  // padding column beyond the image
+      P.cell[o] = 0; P.bp[o] = 0.0; P.u[o] = 0.0; P.g[o] = 0.0f;
+      continue;
+    }
+    const long long px = (long long)y * d.W + x;
+    const double a = (double)d.tgt[px * C + ch];
+    if (!interior_at(d, x, y)) {
+      P.cell[o] = 0; P.bp[o] = 0.0; P.u[o] = a; P.g[o] = 0.0f;
+      continue;
+    }
+    // interior: all four neighbours are inside the image
+    const long long pl = px - 1, pr = px + 1, pu = px - d.W, pd = px + d.W;
+    const double sc = (double)d.src[px * C + ch];
+    const double ns = (((double)d.src[pl * C + ch] + (double)d.src[pr * C + ch]) +
+                       (double)d.src[pu * C + ch]) + (double)d.src[pd * C + ch];
+    const double b = fma(4.0, -sc, ns);
+    const double bp = fma(lam, -a, b);
+    const double na = (((double)d.tgt[pl * C + ch] + (double)d.tgt[pr * C + ch]) +
+                       (double)d.tgt[pu * C + ch]) + (double)d.tgt[pd * C + ch];
+    const double ra = fma(lam + 4.0, -a, na) - bp;
+    acc_a = fma(ra, ra, acc_a);
+    double uc = a, ru = ra;
+    if (d.warm) {
+      auto guess_or_anchor = [&](long long q, int qx, int qy) -> double {
+        return interior_at(d, qx, qy) ? (double)d.guess[q * C + ch] : (double)d.tgt[q * C + ch];
+      };
+      uc = (double)d.guess[px * C + ch];
+      const double nu = ((guess_or_anchor(pl, x - 1, y) + guess_or_anchor(pr, x + 1, y)) +
+                         guess_or_anchor(pu, x, y - 1)) + guess_or_anchor(pd, x, y + 1);
+      ru = fma(lam + 4.0, -uc, nu) - bp;
+    }
+    acc_u = fma(ru, ru, acc_u);
+    P.cell[o] = 1;
+    P.bp[o] = bp;
+    P.u[o] = uc;
+    P.g[o] = (float)(-ru);
+  }
+  acc_a = block_sum(acc_a, sred);
+  acc_u = block_sum(acc_u, sred);
+  if (threadIdx.x == 0) {
+    P.fpart[t] = acc_a;
+    P.fpart[P.ntiles + t] = acc_u;
+  }
+}
+
+// Per-system initial state from the assembly partials (tile order).
+__global__ void k_init(KParams P) {
+  __shared__ double sred[kWarps];
+  const int sys = blockIdx.x;
+  const SysDesc d = P.sys[sys];
+  double sa = 0.0, su = 0.0;
+  int nact = 0;
+  for (int k = threadIdx.x; k < d.ntiles; k += blockDim.x) {
+    const int t = d.tile0 + k;
+    if (P.tcount[t] == 0) continue;
+    sa += P.fpart[t];
+    su += P.fpart[P.ntiles + t];
+    ++nact;
+  }
+  sa = block_sum(sa, sred);
+  su = block_sum(su, sred);
+  for (int o = 16; o > 0; o >>= 1) nact += __shfl_xor_sync(0xffffffffu, nact, o);
+  __shared__ int sn[kWarps];
+  if ((threadIdx.x & 31) == 0) sn[threadIdx.x >> 5] = nact;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  int n = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) n += sn[w];
+  SysState s;
+  s.mode = M_SWEEP; s.s = 0; s.iterations = 0; s.cur = 0;
+  s.pending = P_NONE; s.status = -1; s.refinements = 0; s.since = 0;
+  s.isince = 0; s.nact = n; s.out_anchor = 0; s.pad = 0;
+  s.arrive = 0; s.pad2 = 0;
+  s.r0 = sqrt(sa); s.outer = sqrt(su);
+  s.best = INFINITY; s.ibest = INFINITY; s.last = 1.0; s.ibase = s.outer;
+  // poisson.rs:172-189: no unknowns or a satisfied system -> 0 iterations, converged.
+  if (n == 0 || s.r0 == 0.0) {
+    s.mode = M_DONE; s.status = STOP_CONVERGED; s.last = 0.0; s.out_anchor = 1;
+    atomicAdd(P.bar + 2, 1u);
+  } else if (d.max_it <= 0) {
+    // poisson.rs:202: an empty sweep loop reports the cap with last_relative = 1.
+    s.mode = M_DONE; s.status = STOP_MAX; s.last = 1.0; s.out_anchor = 1;
+    atomicAdd(P.bar + 2, 1u);
+  } else {
+    s.s = d.max_it < P.S ? d.max_it : P.S;
+  }
+  P.st[sys] = s;
+}
+
+// Interleave the result: interior cells take (float)u (the reference's `as f32`,
+// poisson_blend.rs:211-219); every other pixel copies the target bit for bit.
+__global__ void k_emit(KParams P, int sys0, int TW, int TH) {
+  const SysDesc d0 = P.sys[sys0];
+  const long long npx = (long long)d0.W * d0.H;
+  for (long long px = blockIdx.x * (long long)blockDim.x + threadIdx.x; px < npx;
+       px += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(px / d0.W), x = (int)(px - (long long)y * d0.W);
+    const int tx = x / TW, ty = y / TH;
+    const int c = (x + y) & 1, i = x >> 1;
+    for (int ch = 0; ch < d0.C; ++ch) {
+      const SysDesc &d = P.sys[sys0 + ch];
+      float v = d.tgt[px * d.C + ch];
+      if (P.tcount[d.tile0 + ty * d.ntx + tx] > 0 && !P.st[sys0 + ch].out_anchor) {
+        const long long o = plane_index(d, c, y, i);
+        if (P.cell[o]) v = (float)P.u[o];
+      }
+      d.out[px * d.C + ch] = v;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// the persistent solve kernel
+// ----------------------------------------------------------------------------
+template <int S, int TH>
+__device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile &tl, int s,
+                           int cur, float *sE, float *sG, uint8_t *sC, double *sred) {
+  using G = Geo<S, TH>;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int X0 = tl.tx * G::TW - G::HX;  // loaded column 0, a multiple of 8
+  const int Y0 = tl.ty * TH - G::H;
+  const int gi0 = X0 >> 1;                // plane index of loaded column 0, a multiple of 4
+  const float *__restrict__ ein = cur ? P.e1 : P.e0;
+  float *__restrict__ eout = cur ? P.e0 : P.e1;
+
+  // ---- load tile + halo (16-byte vectors; outside the image reads as boundary 0)
+  constexpr int V = kPWL / 4;
+  for (int k = tid; k < 2 * G::LH * V; k += kThreads) {
+    const int c = k / (G::LH * V);
+    const int r = k - c * (G::LH * V);
+    const int ly = r / V, v = r - ly * V;
+    const int gy = Y0 + ly, gi = gi0 + 4 * v;
+    float4 ev = make_float4(0.f, 0.f, 0.f, 0.f), gv = ev;
+    uint32_t cv = 0;
+    if (gy >= 0 && gy < d.H && gi >= 0 && gi < d.pw) {
+      const long long o = plane_index(d, c, gy, gi);
+      ev = __ldcg(reinterpret_cast<const float4 *>(ein + o));
+      gv = __ldcg(reinterpret_cast<const float4 *>(P.g + o));
+      cv = __ldg(reinterpret_cast<const uint32_t *>(P.cell + o));
+    }
+    const int so = c * G::PLANE + ly * kPWL + 4 * v;
+    *reinterpret_cast<float4 *>(sE + so) = ev;
+    *reinterpret_cast<float4 *>(sG + so) = gv;
+    *reinterpret_cast<uint32_t *>(sC + so) = cv;
+  }
+  __syncthreads();
+
+  const int pl = Y0 & 1;  // colour parity of loaded row 0 (column 0 is even)
+  const float w = d.omega, inv = d.inv_denom;
+  const double dd = 4.0 + d.lambda;
+  for (int j = 0; j < s; ++j) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int tt = 2 * j + h + 1;  // half-sweep number: valid window shrinks by tt
+      float *Ec = sE + h * G::PLANE;
+      const float *Eo = sE + (1 - h) * G::PLANE;
+      const float *Gc = sG + h * G::PLANE;
+      const uint8_t *Cc = sC + h * G::PLANE;
+      const int yhi = G::LH - 1 - tt;
+      const int xlo = G::XOFF + tt, xhi = kLW - 1 - G::XOFF - tt;
+      for (int ly = tt + warp; ly <= yhi; ly += kWarps) {
+        const int q = (h + ly + pl) & 1;
+        const int ilo = (xlo - q + 1) >> 1, ihi = (xhi - q) >> 1;
+        const int rb = ly * kPWL;
+        for (int i = ilo + lane; i <= ihi; i += 32) {
+          const int o = rb + i;
+          if (Cc[o]) {
+            const float ns = ((Eo[o - 1 + q] + Eo[o + q]) + Eo[o - kPWL]) + Eo[o + kPWL];
+            const float tg = (ns - Gc[o]) * inv;
+            const float e = Ec[o];
+            Ec[o] = fmaf(w, tg - e, e);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // FP64 residual of the owned cells after sweep j.
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float *Ec = sE + c * G::PLANE;
+      const float *Eo = sE + (1 - c) * G::PLANE;
+      const float *Gc = sG + c * G::PLANE;
+      const uint8_t *Cc = sC + c * G::PLANE;
+      for (int ly = G::H + warp; ly < G::H + TH; ly += kWarps) {
+        const int q = (c + ly + pl) & 1;
+        const int rb = ly * kPWL;
+        for (int i = G::HX / 2 + lane; i < G::HX / 2 + G::TW / 2; i += 32) {
+          const int o = rb + i;
+          if (Cc[o]) {
+            const double ns = (((double)Eo[o - 1 + q] + (double)Eo[o + q]) + (double)Eo[o - kPWL]) +
+                              (double)Eo[o + kPWL];
+            const double r = fma(-dd, (double)Ec[o], ns) - (double)Gc[o];
+            acc = fma(r, r, acc);
+          }
+        }
+      }
+    }
+    acc = block_sum(acc, sred);
+    if (tid == 0) P.partial[(long long)j * P.ntiles + t] = acc;
+  }
+
+  // ---- write the owned cells
+  constexpr int OV = G::TW / 8;  // float4 per owned plane row
+  for (int k = tid; k < 2 * TH * OV; k += kThreads) {
+    const int c = k / (TH * OV);
+    const int r = k - c * (TH * OV);
+    const int ly = G::H + r / OV, v = G::HX / 8 + r % OV;
+    const int gy = Y0 + ly, gi = gi0 + 4 * v;
+    if (gy < d.H && gi < d.pw) {
+      const int so = c * G::PLANE + ly * kPWL + 4 * v;
+      *reinterpret_cast<float4 *>(eout + plane_index(d, c, gy, gi)) =
+          *reinterpret_cast<const float4 *>(sE + so);
+    }
+  }
+}
+
+// u += e on interior cells; e = 0 (owned cells of the tile).
+template <int S, int TH>
+__device__ void fold_tile(const KParams &P, const SysDesc &d, const Tile &tl, int cur) {
+  using G = Geo<S, TH>;
+  float *ec = cur ? P.e1 : P.e0;
+  constexpr int OV = G::TW / 8;
+  for (int k = threadIdx.x; k < 2 * TH * OV; k += kThreads) {
+    const int c = k / (TH * OV);
+    const int r = k - c * (TH * OV);
+    const int gy = tl.ty * TH + r / OV;
+    const int gi = tl.tx * (G::TW / 2) + 4 * (r % OV);
+    if (gy >= d.H || gi >= d.pw) continue;
+    const long long o = plane_index(d, c, gy, gi);
+    const float4 e = __ldcg(reinterpret_cast<const float4 *>(ec + o));
+    const uint32_t cv = __ldg(reinterpret_cast<const uint32_t *>(P.cell + o));
+    double2 u01 = __ldcg(reinterpret_cast<const double2 *>(P.u + o));
+    double2 u23 = __ldcg(reinterpret_cast<const double2 *>(P.u + o + 2));
+    if (cv & 0xffu) u01.x += (double)e.x;
+    if (cv & 0xff00u) u01.y += (double)e.y;
+    if (cv & 0xff0000u) u23.x += (double)e.z;
+    if (cv & 0xff000000u) u23.y += (double)e.w;
+    *reinterpret_cast<double2 *>(P.u + o) = u01;
+    *reinterpret_cast<double2 *>(P.u + o + 2) = u23;
+    *reinterpret_cast<float4 *>(ec + o) = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// g = -r(u) with r in FP64 exactly as residual_l2 (poisson.rs:315-321); partial ||r||^2.
+template <int S, int TH>
+__device__ void resid_tile(const KParams &P, const SysDesc &d, int t, const Tile &tl, double *sred) {
+  using G = Geo<S, TH>;
+  constexpr int half = G::TW / 2;
+  const double lam4 = d.lambda + 4.0;
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < 2 * TH * half; k += kThreads) {
+    const int c = k / (TH * half);
+    const int r = k - c * (TH * half);
+    const int gy = tl.ty * TH + r / half;
+    const int gi = tl.tx * half + r % half;
+    if (gy >= d.H || gi >= d.pw) continue;
+    const long long o = plane_index(d, c, gy, gi);
+    if (!__ldg(P.cell + o)) continue;
+    const int q = (c + gy) & 1;
+    const long long oo = d.off + (long long)(1 - c) * d.plane;
+    const double L = __ldcg(P.u + oo + (long long)gy * d.pw + gi - 1 + q);
+    const double R = __ldcg(P.u + oo + (long long)gy * d.pw + gi + q);
+    const double U = __ldcg(P.u + oo + (long long)(gy - 1) * d.pw + gi);
+    const double D = __ldcg(P.u + oo + (long long)(gy + 1) * d.pw + gi);
+    const double lhs = fma(lam4, -__ldcg(P.u + o), ((L + R) + U) + D);
+    const double res = lhs - __ldg(P.bp + o);
+    P.g[o] = (float)(-res);
+    acc = fma(res, res, acc);
+  }
+  acc = block_sum(acc, sred);
+  if (threadIdx.x == 0) P.partial[t] = acc;
+}
+
+__device__ __forceinline__ void apply_stall(SysState &s, double rel, int &done) {
+  // poisson.rs:219-228
+  if (rel < s.best * (1.0 - kStallImprovement)) {
+    s.best = rel;
+    s.since = 0;
+  } else {
+    s.since += 1;
+    if ((unsigned)s.since >= kStallWindow) done = 1;
+  }
+}
+
+__device__ SysState load_state(const SysState *p) {
+  SysState s;
+  const int *pi = reinterpret_cast<const int *>(p);
+  int *si = reinterpret_cast<int *>(&s);
+  for (int k = 0; k < (int)(sizeof(SysState) / sizeof(int)); ++k) si[k] = __ldcg(pi + k);
+  return s;
+}
+
+// The state machine step run by the last tile of a system to finish a step
+// (thread 0 only). sums[j] = sum of the tile partials of sweep j (tile order).
+__device__ void advance(const KParams &P, const SysDesc &d, SysState *stp, int mode,
+                        const double *sums) {
+  SysState s = load_state(stp);
+  double *hist = P.hist + d.hist_off;
+  const int cap = P.S;
+  switch (mode) {
+    case M_SWEEP: {
+      int kind = P_NONE, stop_j = -1;
+      bool refine = false;
+      for (int j = 0; j < s.s; ++j) {
+        const double nrm = sqrt(sums[j]);
+        const double rel = nrm / s.r0;  // poisson.rs:206
+        s.iterations += 1;
+        hist[s.iterations - 1] = rel;
+        s.last = rel;
+        if (rel <= d.tol) { kind = P_CONV; stop_j = j; break; }  // poisson.rs:210-214
+        int stalled = 0;
+        apply_stall(s, rel, stalled);
+        if (stalled) { kind = P_STALL; stop_j = j; break; }
+        if (s.iterations >= d.max_it) { kind = P_MAX; stop_j = j; break; }
+        // residual-correction trigger (does not change the iterate, only when
+        // the FP64 fold happens, so it waits for the end of the block)
+        if (nrm <= kRefineFactor * s.ibase) refine = true;
+        if (nrm < s.ibest * kInnerGain) { s.ibest = nrm; s.isince = 0; }
+        else if (++s.isince >= kInnerWindow) refine = true;
+      }
+      if (kind == P_NONE) {
+        s.cur ^= 1;
+        if (refine) { s.pending = P_REFINE; s.mode = M_FOLD; }
+        else { s.mode = M_SWEEP; s.s = min(cap, d.max_it - s.iterations); }
+      } else if (stop_j == s.s - 1) {
+        s.cur ^= 1; s.pending = kind; s.mode = M_FOLD;
+      } else {
+        // stop inside the block: re-run the block from the same start with
+        // exactly stop_j+1 sweeps (identical arithmetic), so the iterate kept is
+        // the one after the reported sweep.
+        s.pending = kind; s.mode = M_REDO; s.s = stop_j + 1;
+      }
+    } break;
+    case M_REDO:
+      s.cur ^= 1;
+      s.mode = M_FOLD;
+      break;
+    case M_FOLD:
+      s.mode = M_RESID;
+      break;
+    case M_RESID: {
+      const double nrm = sqrt(sums[0]);
+      const double rel = nrm / s.r0;
+      s.outer = nrm;
+      s.ibase = nrm;
+      s.ibest = INFINITY;
+      s.isince = 0;
+      s.refinements += 1;
+      if (s.iterations > 0) { hist[s.iterations - 1] = rel; s.last = rel; }
+      int stop = -1;
+      if (rel <= d.tol) stop = STOP_CONVERGED;
+      else if (s.pending == P_STALL) stop = STOP_STALLED;
+      else if (s.pending == P_MAX || s.iterations >= d.max_it) stop = STOP_MAX;
+      else if (s.pending == P_CONV) {
+        // the per-sweep estimate met the tolerance but the FP64 residual does
+        // not: apply the stall rule the estimate skipped, then keep sweeping
+        int stalled = 0;
+        apply_stall(s, rel, stalled);
+        if (stalled) stop = STOP_STALLED;
+      }
+      s.pending = P_NONE;
+      if (stop >= 0) {
+        s.mode = M_DONE;
+        s.status = stop;
+        atomicAdd(P.bar + 2, 1u);
+      } else {
+        s.mode = M_SWEEP;
+        s.s = min(cap, d.max_it - s.iterations);
+      }
+    } break;
+    default:
+      break;
+  }
+  s.arrive = 0;
+  *stp = s;
+  __threadfence();
+}
+
+template <int S, int TH>
+__global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
+  using G = Geo<S, TH>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *sE = reinterpret_cast<float *>(smem);
+  float *sG = sE + 2 * G::PLANE;
+  uint8_t *sC = reinterpret_cast<uint8_t *>(sG + 2 * G::PLANE);
+  double *sred = reinterpret_cast<double *>(sC + 2 * G::PLANE);
+  __shared__ int s_last;
+  const unsigned long long t_start = gtimer();
+
+  for (;;) {
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+      if (__ldg(P.tcount + t) == 0) continue;
+      const Tile tl = P.tiles[t];
+      SysState *stp = P.st + tl.sys;
+      const int mode = __ldcg(&stp->mode);
+      if (mode == M_DONE) continue;
+      const int s = __ldcg(&stp->s);
+      const int cur = __ldcg(&stp->cur);
+      const SysDesc d = P.sys[tl.sys];
+      if (mode == M_SWEEP || mode == M_REDO) {
+        sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
+      } else if (mode == M_FOLD) {
+        fold_tile<S, TH>(P, d, tl, cur);
+      } else {
+        resid_tile<S, TH>(P, d, t, tl, sred);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned a = atomicAdd(&stp->arrive, 1u);
+        s_last = (a == (unsigned)__ldcg(&stp->nact) - 1u);
+        __threadfence();
+      }
+      __syncthreads();
+      if (s_last) {
+        // this block finished the system's step last: reduce in tile order
+        double part[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) part[j] = 0.0;
+        const int nsum = (mode == M_SWEEP) ? s : (mode == M_RESID ? 1 : 0);
+        if (nsum > 0) {
+          for (int k = d.tile0 + threadIdx.x; k < d.tile0 + d.ntiles; k += kThreads) {
+            if (__ldg(P.tcount + k) == 0) continue;
+#pragma unroll
+            for (int j = 0; j < S; ++j)
+              if (j < nsum) part[j] += __ldcg(P.partial + (long long)j * P.ntiles + k);
+          }
+#pragma unroll
+          for (int j = 0; j < S; ++j)
+            if (j < nsum) part[j] = block_sum(part[j], sred);
+        }
+        if (threadIdx.x == 0) advance(P, d, stp, mode, part);
+        __syncthreads();
+      }
+    }
+    if (!grid_sync(P.bar, P.err)) break;
+    if (__ldcg(P.bar + 3) >= (unsigned)P.nsys) break;
+    if (gtimer() - t_start > P.budget_ns) {
+      atomicCAS(P.err, 0, KERR_DEADLINE);
+      break;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// launch entry points (host)
+// ----------------------------------------------------------------------------
+template <int S, int TH>
+static cudaError_t launch_solve_t(const KParams &P, int sms, cudaStream_t stream, int *grid_out) {
+  using G = Geo<S, TH>;
+  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)G::kSmem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH>, kThreads, G::kSmem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int grid = per_sm * sms;
+  if (grid > P.ntiles) grid = P.ntiles > 0 ? P.ntiles : 1;
+  *grid_out = grid;
+  KParams Pc = P;
+  Pc.S = S;
+  void *args[] = {&Pc};
+  return cudaLaunchCooperativeKernel((const void *)k_solve<S, TH>, dim3(grid), dim3(kThreads),
+                                     args, G::kSmem, stream);
+}
+
+int tile_config_count() { return 4; }
+
+TileConfig tile_config(int idx) {
+  switch (idx) {
+    case 0: return {1, 64, tile_w(1)};
+    case 1: return {2, 64, tile_w(2)};
+    case 2: return {3, 64, tile_w(3)};
+    default: return {3, 32, tile_w(3)};
+  }
+}
+
+size_t tile_config_smem(int idx) {
+  switch (idx) {
+    case 0: return Geo<1, 64>::kSmem;
+    case 1: return Geo<2, 64>::kSmem;
+    case 2: return Geo<3, 64>::kSmem;
+    default: return Geo<3, 32>::kSmem;
+  }
+}
+
+cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_tile_count<<<P.ntiles, 256, 0, stream>>>(P, tc.tw, tc.th);
+  k_assemble<<<P.ntiles, kThreads, 0, stream>>>(P, tc.tw, tc.th);
+  k_init<<<P.nsys, 256, 0, stream>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid) {
+  switch (cfg) {
+    case 0: return launch_solve_t<1, 64>(P, sms, stream, grid);
+    case 1: return launch_solve_t<2, 64>(P, sms, stream, grid);
+    case 2: return launch_solve_t<3, 64>(P, sms, stream, grid);
+    default: return launch_solve_t<3, 32>(P, sms, stream, grid);
+  }
+}
+
+cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,
+                        cudaStream_t stream) {
+  if (npx <= 0) return cudaSuccess;
+  long long blocks = (npx + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_emit<<<(int)blocks, 256, 0, stream>>>(P, sys0, tc.tw, tc.th);
+  return cudaGetLastError();
+}
+
+}  // namespace ptk

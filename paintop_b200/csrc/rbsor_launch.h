@@ -1,0 +1,27 @@
+// rbsor_launch.h -- host-visible launch entry points of the solver kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "rbsor.cuh"
+
+namespace ptk {
+
+// One tile configuration: sweeps per step S, owned tile height th and width tw.
+struct TileConfig {
+  int S, th, tw;
+};
+
+int tile_config_count();
+TileConfig tile_config(int idx);
+size_t tile_config_smem(int idx);
+
+// k_tile_count + k_assemble + k_init on the stream.
+cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream);
+// The persistent cooperative solve; *grid receives the block count used.
+cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid);
+// Interleave one image's channels sys0 .. sys0+C-1 into its output.
+cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,
+                        cudaStream_t stream);
+
+}  // namespace ptk

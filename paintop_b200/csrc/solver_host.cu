@@ -1,0 +1,499 @@
+// solver_host.cu -- context, planning and the C-ABI solve entry points.
+//
+// pt_poisson_solve / pt_poisson_solve_batch replace the reference's per-channel
+// chain blend_channels -> solve (crates/paintop-cpu/src/poisson_blend.rs:168-246,
+// crates/paintop-cpu/src/poisson.rs:167-240) with one persistent launch over all
+// channels of all images. Planning (tile grid, pool layout) needs only the
+// problem extents, so a call issues no host synchronisation between its upload
+// and its download.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/paintop_cuda.h"
+#include "ctx.h"
+#include "rbsor_launch.h"
+
+using namespace ptk;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+pt_status fail(pt_ctx *ctx, pt_status s, const std::string &msg) {
+  if (ctx) ctx->last_error = msg;
+  return s;
+}
+
+pt_status cuda_fail(pt_ctx *ctx, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (ctx) ctx->last_error = m;
+  if (e == cudaErrorMemoryAllocation) return PT_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return PT_NO_DEVICE;
+  return PT_LAUNCH_FAILED;
+}
+
+// Host fault injection for tests of the error paths (no GPU fault involved):
+// PAINTOP_CUDA_FAULT = "no-device" | "oom" | "launch".
+int injected_fault() {
+  const char *f = std::getenv("PAINTOP_CUDA_FAULT");
+  if (!f) return 0;
+  if (!std::strcmp(f, "no-device")) return 1;
+  if (!std::strcmp(f, "oom")) return 2;
+  if (!std::strcmp(f, "launch")) return 3;
+  return 0;
+}
+
+bool finite(double v) { return std::isfinite(v); }
+
+pt_status validate(pt_ctx *ctx, const pt_problem &p) {
+  if (p.channels > 0 && (p.width == 0 || p.height == 0))
+    return fail(ctx, PT_INVALID_ARG, "width and height must be >= 1");
+  const unsigned long long px = (unsigned long long)p.width * p.height;
+  if (px > (1ull << 31) || px * (p.channels ? p.channels : 1) > (1ull << 34))
+    return fail(ctx, PT_INVALID_ARG, "image too large");
+  if (p.channels > 0 && (!p.source_or_guidance || !p.target_or_anchor || !p.mask))
+    return fail(ctx, PT_INVALID_ARG, "source, target and mask must be non-null");
+  if ((p.flags & PT_FLAG_WARM_START) && !p.initial_guess)
+    return fail(ctx, PT_INVALID_ARG, "PT_FLAG_WARM_START needs initial_guess");
+  if (!finite(p.lambda) || p.lambda < 0.0)
+    return fail(ctx, PT_INVALID_ARG, "lambda must be a finite value >= 0");
+  if (!finite(p.tolerance) || p.tolerance <= 0.0)
+    return fail(ctx, PT_INVALID_ARG, "tolerance must be a finite value > 0");
+  if (!(p.flags & PT_FLAG_OMEGA_AUTO) && (!finite(p.omega) || p.omega <= 0.0 || p.omega >= 2.0))
+    return fail(ctx, PT_INVALID_ARG, "omega must be in (0, 2)");
+  if (p.max_iterations > 1000000u)
+    return fail(ctx, PT_INVALID_ARG, "max_iterations must be <= 1000000");
+  return PT_OK;
+}
+
+// Red-black SOR optimum for the discrete operator of a region: the Jacobi
+// spectral radius of (4+lambda)I - N is (4 - mu_min)/(4 + lambda) with mu_min the
+// smallest Dirichlet eigenvalue of the 5-point Laplacian on the region; for a
+// region spanning a box of a x b cells mu_min ~ pi^2 (1/a^2 + 1/b^2) (a
+// rectangle's value; other shapes of that extent are close to it). Young's
+// formula then gives omega = 2 / (1 + sqrt(1 - rho^2)).
+double auto_omega(double lambda, double a, double b) {
+  a = std::max(a, 1.0);
+  b = std::max(b, 1.0);
+  const double pi2 = 9.869604401089358;
+  const double mu = pi2 * (1.0 / (a * a) + 1.0 / (b * b));
+  const double rho = std::min(std::max((4.0 - mu) / (4.0 + lambda), 0.0), 1.0 - 1e-15);
+  return 2.0 / (1.0 + std::sqrt(1.0 - rho * rho));
+}
+
+// Span of the interior cells of a mask (host side, for PT_FLAG_OMEGA_AUTO).
+void interior_span(const pt_problem &p, double *a, double *b) {
+  long long x0 = p.width, x1 = -1, y0 = p.height, y1 = -1;
+  if (p.width >= 3 && p.height >= 3)
+    for (uint32_t y = 1; y + 1 < p.height; ++y)
+      for (uint32_t x = 1; x + 1 < p.width; ++x)
+        if (p.mask[(size_t)y * p.width + x] > 0.5f) {
+          x0 = std::min<long long>(x0, x); x1 = std::max<long long>(x1, x);
+          y0 = std::min<long long>(y0, y); y1 = std::max<long long>(y1, y);
+        }
+  *a = x1 >= x0 ? double(x1 - x0 + 2) : 1.0;
+  *b = y1 >= y0 ? double(y1 - y0 + 2) : 1.0;
+}
+
+struct Plan {
+  int cfg;
+  TileConfig tc;
+  std::vector<SysDesc> sys;
+  std::vector<Tile> tiles;
+  long long cells = 0;     // elements per cell pool
+  long long hist = 0;      // history entries
+  long long in_floats = 0; // staged input floats (images + guesses)
+  long long mask_floats = 0;
+  long long out_floats = 0;
+};
+
+// Arena layout (byte offsets) for one call.
+struct Layout {
+  size_t sys, st, tiles, tcount, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in, mask,
+      out, total;
+};
+
+Layout layout(const Plan &pl, bool stage) {
+  Layout L{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o = align_up(o + std::max<size_t>(bytes, 1), kAlign); return r; };
+  const size_t nt = pl.tiles.size(), ns = pl.sys.size();
+  L.sys = take(ns * sizeof(SysDesc));
+  L.st = take(ns * sizeof(SysState));
+  L.tiles = take(nt * sizeof(Tile));
+  L.tcount = take(nt * sizeof(int));
+  L.e0 = take(pl.cells * sizeof(float));
+  L.e1 = take(pl.cells * sizeof(float));
+  L.g = take(pl.cells * sizeof(float));
+  L.cell = take(pl.cells);
+  L.u = take(pl.cells * sizeof(double));
+  L.bp = take(pl.cells * sizeof(double));
+  L.partial = take((size_t)pl.tc.S * nt * sizeof(double));
+  L.fpart = take(2 * nt * sizeof(double));
+  L.hist = take(pl.hist * sizeof(double));
+  L.bar = take(4 * sizeof(unsigned));
+  L.err = take(sizeof(int));
+  L.in = stage ? take(pl.in_floats * sizeof(float)) : 0;
+  L.mask = stage ? take(pl.mask_floats * sizeof(float)) : 0;
+  L.out = stage ? take(pl.out_floats * sizeof(float)) : 0;
+  L.total = o;
+  return L;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// tile-configuration choice (the autotuner's table; see autotune.cpp)
+// ---------------------------------------------------------------------------
+int ptk_choose_config(pt_ctx *ctx, const pt_problem *ps, uint32_t n);
+
+pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
+                          pt_report *const *reports, double *const *histories, int force_cfg) {
+  if (!ctx) return PT_INVALID_ARG;
+  if (n > 0 && (!ps || !outs || !reports)) return fail(ctx, PT_INVALID_ARG, "null batch arrays");
+  for (uint32_t i = 0; i < n; ++i) {
+    pt_status s = validate(ctx, ps[i]);
+    if (s != PT_OK) return s;
+    if (ps[i].channels > 0 && !outs[i]) return fail(ctx, PT_INVALID_ARG, "null output buffer");
+    if (!reports[i]) return fail(ctx, PT_INVALID_ARG, "null report buffer");
+  }
+  const int fault = injected_fault();
+  if (fault == 1) return fail(ctx, PT_NO_DEVICE, "injected: no device");
+  if (fault == 2) return fail(ctx, PT_OOM, "injected: allocation failure");
+  if (fault == 3) return fail(ctx, PT_LAUNCH_FAILED, "injected: launch failure");
+
+  const bool devptr = n > 0 && (ps[0].flags & PT_FLAG_DEVICE_POINTERS);
+  for (uint32_t i = 0; i < n; ++i)
+    if (((ps[i].flags & PT_FLAG_DEVICE_POINTERS) != 0) != devptr)
+      return fail(ctx, PT_INVALID_ARG, "PT_FLAG_DEVICE_POINTERS must agree across a batch");
+
+  // ---- plan
+  Plan pl;
+  pl.cfg = force_cfg >= 0 ? force_cfg : ptk_choose_config(ctx, ps, n);
+  pl.tc = tile_config(pl.cfg);
+  std::vector<int> sys0(n, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    const pt_problem &p = ps[i];
+    sys0[i] = (int)pl.sys.size();
+    const int W = (int)p.width, H = (int)p.height, C = (int)p.channels;
+    const int pw = (int)align_up((size_t)(W + 1) / 2, 4);
+    const int ntx = (W + pl.tc.tw - 1) / pl.tc.tw, nty = (H + pl.tc.th - 1) / pl.tc.th;
+    double omega = p.omega;
+    if (p.flags & PT_FLAG_OMEGA_AUTO) {
+      double a = 1, b = 1;
+      if (!devptr) interior_span(p, &a, &b);
+      else { a = W; b = H; }
+      omega = auto_omega(p.lambda, a, b);
+    }
+    const long long img = (long long)W * H;
+    for (int c = 0; c < C; ++c) {
+      SysDesc d{};
+      d.inst = (int)i; d.chan = c; d.W = W; d.H = H; d.C = C; d.pw = pw;
+      d.ntx = ntx; d.nty = nty;
+      d.plane = (long long)H * pw;
+      d.off = pl.cells;
+      pl.cells += 2 * d.plane;
+      d.tile0 = (int)pl.tiles.size();
+      d.ntiles = ntx * nty;
+      for (int ty = 0; ty < nty; ++ty)
+        for (int tx = 0; tx < ntx; ++tx) pl.tiles.push_back(Tile{(int)pl.sys.size(), tx, ty, 0});
+      d.hist_off = pl.hist;
+      pl.hist += p.max_iterations;
+      d.omega = (float)omega;
+      d.inv_denom = (float)(1.0 / (4.0 + p.lambda));
+      d.lambda = p.lambda;
+      d.tol = p.tolerance;
+      d.max_it = (int)p.max_iterations;
+      d.warm = (p.flags & PT_FLAG_WARM_START) ? 1 : 0;
+      pl.sys.push_back(d);
+    }
+    if (C > 0) {
+      pl.in_floats += img * C * (1 + 1 + ((p.flags & PT_FLAG_WARM_START) ? 1 : 0));
+      pl.mask_floats += img;
+      pl.out_floats += img * C;
+    }
+  }
+  const int nsys = (int)pl.sys.size();
+  if (nsys == 0) {
+    for (uint32_t i = 0; i < n; ++i) {
+      pt_report r{};
+      r.converged = 1; r.stop_reason = PT_STOP_CONVERGED; r.tolerance = ps[i].tolerance;
+      r.channel = -1;
+      reports[i][0] = r;
+    }
+    return PT_OK;
+  }
+
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaSetDevice");
+  const Layout L = layout(pl, !devptr);
+  if (!ctx->reserve(L.total)) return fail(ctx, PT_OOM, "device arena allocation failed");
+  char *base = static_cast<char *>(ctx->arena);
+  cudaStream_t st = ctx->stream;
+  for (auto &e : ctx->ev)
+    if (!e && cudaEventCreate(&e) != cudaSuccess) return fail(ctx, PT_LAUNCH_FAILED, "event create");
+  cudaEventRecord(ctx->ev[0], st);
+
+  // ---- stage inputs and bind the per-system image pointers
+  {
+    size_t in_off = 0, mask_off = 0, out_off = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const pt_problem &p = ps[i];
+      if (p.channels == 0) continue;
+      const size_t img = (size_t)p.width * p.height, nf = img * p.channels;
+      const float *src = p.source_or_guidance, *tgt = p.target_or_anchor, *mask = p.mask,
+                  *guess = p.initial_guess;
+      float *out = outs[i];
+      if (!devptr) {
+        float *in = reinterpret_cast<float *>(base + L.in) + in_off;
+        float *dm = reinterpret_cast<float *>(base + L.mask) + mask_off;
+        ce = cudaMemcpyAsync(in, src, nf * sizeof(float), cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess)
+          ce = cudaMemcpyAsync(in + nf, tgt, nf * sizeof(float), cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess)
+          ce = cudaMemcpyAsync(dm, mask, img * sizeof(float), cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess && (p.flags & PT_FLAG_WARM_START))
+          ce = cudaMemcpyAsync(in + 2 * nf, guess, nf * sizeof(float), cudaMemcpyHostToDevice, st);
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "input upload");
+        src = in; tgt = in + nf; mask = dm;
+        guess = (p.flags & PT_FLAG_WARM_START) ? in + 2 * nf : nullptr;
+        out = reinterpret_cast<float *>(base + L.out) + out_off;
+        in_off += nf * ((p.flags & PT_FLAG_WARM_START) ? 3 : 2);
+        mask_off += img;
+        out_off += nf;
+      }
+      for (uint32_t c = 0; c < p.channels; ++c) {
+        SysDesc &d = pl.sys[sys0[i] + c];
+        d.src = src; d.tgt = tgt; d.mask = mask; d.out = out;
+        d.guess = (p.flags & PT_FLAG_WARM_START) ? guess : nullptr;
+      }
+    }
+  }
+  ce = cudaMemcpyAsync(base + L.sys, pl.sys.data(), pl.sys.size() * sizeof(SysDesc),
+                       cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(base + L.tiles, pl.tiles.data(), pl.tiles.size() * sizeof(Tile),
+                         cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.bar, 0, 4 * sizeof(unsigned), st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.err, 0, sizeof(int), st);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "plan upload");
+
+  KParams P{};
+  P.sys = reinterpret_cast<const SysDesc *>(base + L.sys);
+  P.st = reinterpret_cast<SysState *>(base + L.st);
+  P.tiles = reinterpret_cast<const Tile *>(base + L.tiles);
+  P.tcount = reinterpret_cast<int *>(base + L.tcount);
+  P.ntiles = (int)pl.tiles.size();
+  P.nsys = nsys;
+  P.e0 = reinterpret_cast<float *>(base + L.e0);
+  P.e1 = reinterpret_cast<float *>(base + L.e1);
+  P.g = reinterpret_cast<float *>(base + L.g);
+  P.cell = reinterpret_cast<uint8_t *>(base + L.cell);
+  P.u = reinterpret_cast<double *>(base + L.u);
+  P.bp = reinterpret_cast<double *>(base + L.bp);
+  P.partial = reinterpret_cast<double *>(base + L.partial);
+  P.fpart = reinterpret_cast<double *>(base + L.fpart);
+  P.hist = reinterpret_cast<double *>(base + L.hist);
+  P.bar = reinterpret_cast<unsigned *>(base + L.bar);
+  P.err = reinterpret_cast<int *>(base + L.err);
+  P.budget_ns = (unsigned long long)(ctx->budget_s * 1e9);
+  P.S = pl.tc.S;
+
+  ce = launch_assembly(P, pl.tc, st);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "assembly launch");
+  int grid = 0;
+  cudaEventRecord(ctx->ev[1], st);
+  ce = launch_solve(P, pl.cfg, ctx->sms, st, &grid);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "solve launch");
+  cudaEventRecord(ctx->ev[2], st);
+  long long launches = 4;  // tile count, assembly, init, solve
+  ctx->last_grid = grid;
+  ctx->last_cfg = pl.cfg;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (ps[i].channels == 0) continue;
+    ce = launch_emit(P, sys0[i], pl.tc, (long long)ps[i].width * ps[i].height, st);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "emit launch");
+    ++launches;
+  }
+
+  // ---- download
+  std::vector<SysState> states(nsys);
+  int kerr = 0;
+  ce = cudaMemcpyAsync(states.data(), base + L.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&kerr, base + L.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!devptr && ce == cudaSuccess) {
+    for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
+      if (ps[i].channels == 0) continue;
+      const size_t nf = (size_t)ps[i].width * ps[i].height * ps[i].channels;
+      ce = cudaMemcpyAsync(outs[i], pl.sys[sys0[i]].out, nf * sizeof(float), cudaMemcpyDeviceToHost, st);
+    }
+  }
+  if (histories && ce == cudaSuccess) {
+    for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
+      if (!histories[i]) continue;
+      for (uint32_t c = 0; c < ps[i].channels && ce == cudaSuccess; ++c) {
+        const SysDesc &d = pl.sys[sys0[i] + c];
+        const size_t cnt = ps[i].max_iterations;
+        if (!cnt) continue;
+        ce = cudaMemcpyAsync(histories[i] + (size_t)c * cnt,
+                             reinterpret_cast<double *>(base + L.hist) + d.hist_off, cnt * sizeof(double),
+                             devptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st);
+      }
+    }
+  }
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "result download");
+  cudaEventRecord(ctx->ev[3], st);
+  ce = cudaStreamSynchronize(st);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "stream synchronize");
+  {
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+    ctx->last_solve_ms = a;
+    ctx->last_call_ms = b;
+    ctx->last_launches = launches;
+  }
+  if (kerr != KERR_NONE)
+    return fail(ctx, PT_TIMEOUT, kerr == KERR_DEADLINE ? "solve exceeded its wall budget"
+                                                       : "grid barrier wait gave up");
+
+  // ---- reports
+  for (uint32_t i = 0; i < n; ++i) {
+    const pt_problem &p = ps[i];
+    int worst = -1;
+    for (uint32_t c = 0; c < p.channels; ++c) {
+      const SysState &s = states[sys0[i] + c];
+      pt_report r{};
+      r.iterations = (uint32_t)s.iterations;
+      r.stop_reason = s.status;
+      r.converged = s.status == PT_STOP_CONVERGED;
+      r.tolerance = p.tolerance;
+      r.final_residual = s.last;
+      r.history_len = r.iterations;
+      r.omega_used = pl.sys[sys0[i] + c].omega;
+      r.refinements = (uint32_t)s.refinements;
+      r.channel = (int)c;
+      reports[i][c] = r;
+      // worse_of (poisson_blend.rs:240-246)
+      if (worst < 0) worst = (int)c;
+      else {
+        const pt_report &a = reports[i][worst];
+        const bool b_worse = (r.iterations != a.iterations) ? (r.iterations > a.iterations)
+                                                             : (r.final_residual > a.final_residual);
+        if (b_worse) worst = (int)c;
+      }
+    }
+    if (worst >= 0) {
+      reports[i][p.channels] = reports[i][worst];
+    } else {
+      pt_report r{};
+      r.converged = 1; r.stop_reason = PT_STOP_CONVERGED; r.tolerance = p.tolerance; r.channel = -1;
+      reports[i][0] = r;
+    }
+  }
+  return PT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+pt_status pt_ctx_create(int device, pt_ctx **out) {
+  if (!out) return PT_INVALID_ARG;
+  *out = nullptr;
+  if (injected_fault() == 1) return PT_NO_DEVICE;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= 0) return PT_NO_DEVICE;
+  if (device < 0 || device >= count) return PT_INVALID_ARG;
+  cudaDeviceProp prop{};
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return PT_NO_DEVICE;
+  if (prop.major != 10) return PT_NO_DEVICE;  // built for sm_100a only
+  if (!prop.cooperativeLaunch) return PT_NO_DEVICE;
+  pt_ctx *c = new (std::nothrow) pt_ctx();
+  if (!c) return PT_OOM;
+  c->device = device;
+  c->sms = prop.multiProcessorCount;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return PT_LAUNCH_FAILED;
+  }
+  *out = c;
+  return PT_OK;
+}
+
+pt_status pt_ctx_destroy(pt_ctx *ctx) {
+  if (!ctx) return PT_OK;
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->release();
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+  return PT_OK;
+}
+
+pt_status pt_poisson_solve(pt_ctx *ctx, const pt_problem *p, float *out_candidate, pt_report *reports,
+                           double *history) {
+  if (!ctx || !p || !reports) return PT_INVALID_ARG;
+  float *outs[1] = {out_candidate};
+  pt_report *reps[1] = {reports};
+  double *hists[1] = {history};
+  return ptk_solve_batch(ctx, p, 1, outs, reps, hists, -1);
+}
+
+pt_status pt_poisson_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
+                                 pt_report *const *reports, double *const *histories) {
+  return ptk_solve_batch(ctx, ps, n, outs, reports, histories, -1);
+}
+
+const char *pt_status_str(pt_status s) {
+  switch (s) {
+    case PT_OK: return "ok";
+    case PT_NO_DEVICE: return "E_CUDA_UNAVAILABLE: no usable sm_100 CUDA device";
+    case PT_INVALID_ARG: return "invalid argument";
+    case PT_LAUNCH_FAILED: return "CUDA launch or copy failed";
+    case PT_TIMEOUT: return "device watchdog expired";
+    case PT_OOM: return "out of memory";
+    case PT_INTERNAL: return "internal error";
+  }
+  return "unknown status";
+}
+
+const char *pt_ctx_last_error(const pt_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+void *pt_ctx_stream(const pt_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+pt_status pt_ctx_last_timing(const pt_ctx *ctx, double *solve_kernel_ms, double *call_ms,
+                             int64_t *kernel_launches) {
+  if (!ctx) return PT_INVALID_ARG;
+  if (solve_kernel_ms) *solve_kernel_ms = ctx->last_solve_ms;
+  if (call_ms) *call_ms = ctx->last_call_ms;
+  if (kernel_launches) *kernel_launches = ctx->last_launches;
+  return PT_OK;
+}
+
+pt_status pt_ctx_set_budget(pt_ctx *ctx, double seconds) {
+  if (!ctx || !(seconds > 0.0) || !std::isfinite(seconds)) return PT_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->budget_s = seconds;
+  return PT_OK;
+}
+
+}  // extern "C"

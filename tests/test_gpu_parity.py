@@ -1,0 +1,356 @@
+"""GPU parity: the CUDA backend against the oracle and the reference's contract.
+
+Tolerances (stated here, measured against the FP64 CG oracle driven to 1e-12):
+  * converged solves at tolerance t: max |u_gpu - u_cg| <= bound(t), where the
+    discrete error is at most ||r|| / lambda_min(A); the tests use tight
+    tolerances where this bound is below the reference's bounded tier
+    (1e-4 max-abs, 1e-5 RMS; crates/paintop-testkit/src/differential.rs:58-62);
+  * every non-interior pixel equals the target bit for bit;
+  * reruns are byte-identical.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BOUNDED_MAX_ABS = 1e-4   # differential.rs:58-62
+BOUNDED_RMS = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ops(cuda_lib):
+    from paintop_b200 import ops as O
+    O.context()
+    return O
+
+
+def square_mask(w, h, lo, hi):
+    m = np.zeros((h, w), dtype=np.float32)
+    m[lo:hi, lo:hi] = 1.0
+    return m.reshape(-1)
+
+
+def run(ops, op, w, h, a, b, mask, params):
+    if op == "blend":
+        inputs = {"source": ops.gray_image(w, h, a), "target": ops.gray_image(w, h, b),
+                  "mask": ops.mask_value(w, h, mask)}
+        out = ops.PoissonBlend().compute(inputs, params)
+    else:
+        inputs = {"guidance": ops.gray_image(w, h, a), "anchor": ops.gray_image(w, h, b),
+                  "mask": ops.mask_value(w, h, mask)}
+        out = ops.ScreenedPoisson().compute(inputs, params)
+    return out["candidate"].samples, out["report"].as_report()
+
+
+# ---- the reference's op suites through the cuda backend ----------------------------
+
+def test_blend_boundary_pixels_keep_the_target(ops):
+    w = h = 16
+    tgt = np.full(w * h, 0.1, np.float32)
+    mask = square_mask(w, h, 5, 11)
+    cand, _ = run(ops, "blend", w, h, np.full(w * h, 0.9, np.float32), tgt, mask, {})
+    assert np.array_equal(cand[mask <= 0.5], tgt[mask <= 0.5])
+
+
+def test_blend_uniform_source_over_uniform_target(ops):
+    w = h = 20
+    mask = square_mask(w, h, 6, 14)
+    cand, rep = run(ops, "blend", w, h, np.full(w * h, 0.7, np.float32),
+                    np.full(w * h, 0.25, np.float32), mask,
+                    {"tolerance": 1e-8, "max_iterations": 5000})
+    assert np.all(np.abs(cand[mask > 0.5] - 0.25) < 1e-3)
+    assert rep.solver.kind == "poisson" and rep.solver.converged
+
+
+def test_blend_linear_gradient_reproduced(ops):
+    w = h = 24
+    src = np.tile(np.arange(w, dtype=np.float32), h)
+    mask = square_mask(w, h, 6, 18)
+    cand, _ = run(ops, "blend", w, h, src, src.copy(), mask,
+                  {"tolerance": 1e-9, "max_iterations": 8000})
+    o = cand.reshape(h, w)
+    for row in range(7, 17):
+        for col in range(7, 17):
+            assert abs((o[row, col] - o[row, col - 1]) - 1.0) < 5e-2
+
+
+def test_blend_reruns_bit_identical(ops):
+    w, h = 18, 14
+    src = (((np.arange(w * h) * 7) % 13) / 13.0).astype(np.float32)
+    tgt = np.full(w * h, 0.3, np.float32)
+    mask = square_mask(w, h, 4, 12)
+    a, ra = run(ops, "blend", w, h, src, tgt, mask, {"max_iterations": 200})
+    b, rb = run(ops, "blend", w, h, src, tgt, mask, {"max_iterations": 200})
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert ra.solver.residual_history == rb.solver.residual_history
+
+
+def test_blend_report_carries_iterative_metrics(ops):
+    w = h = 16
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    src = (np.float32(0.01) * (xx * xx + yy * yy)).reshape(-1)
+    mask = square_mask(w, h, 4, 12)
+    _, rep = run(ops, "blend", w, h, src, np.full(w * h, 0.2, np.float32), mask,
+                 {"max_iterations": 3, "tolerance": 1e-12})
+    s = rep.solver
+    assert s.iterations == 3 and s.steps == 3 and s.stop_reason == "max-iterations"
+    assert s.converged is False and len(s.residual_history) == 3
+    assert s.tolerance > 0 and np.isfinite(s.final_residual)
+    assert s.final_residual == s.residual_history[-1]
+    assert s.stable and s.stability_number == 0.0 and s.total_energy == 0.0
+
+
+def test_screened_lambda_zero_recovers_guidance_gradient(ops):
+    w = h = 24
+    g = np.tile(np.arange(w, dtype=np.float32), h)
+    mask = square_mask(w, h, 6, 18)
+    cand, _ = run(ops, "screened", w, h, g, g.copy(), mask,
+                  {"lambda": 0.0, "tolerance": 1e-9, "max_iterations": 8000})
+    o = cand.reshape(h, w)
+    for row in range(7, 17):
+        for col in range(7, 17):
+            assert abs((o[row, col] - o[row, col - 1]) - 1.0) < 5e-2
+
+
+def bump(w, h):
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    return (np.float32(0.02) * (xx * xx + yy * yy)).reshape(-1)
+
+
+def test_screened_large_lambda_snaps_to_anchor(ops):
+    w = h = 20
+    mask = square_mask(w, h, 6, 14)
+    cand, _ = run(ops, "screened", w, h, bump(w, h), np.full(w * h, 0.4, np.float32), mask,
+                  {"lambda": 1e6, "tolerance": 1e-9, "max_iterations": 8000})
+    assert np.all(np.abs(cand[mask > 0.5] - 0.4) < 1e-2)
+
+
+def test_screened_larger_lambda_moves_closer_to_anchor(ops):
+    w = h = 20
+    mask = square_mask(w, h, 6, 14)
+    centre = (h // 2) * w + (w // 2)
+
+    def dist(lam):
+        cand, _ = run(ops, "screened", w, h, bump(w, h), np.full(w * h, 0.5, np.float32), mask,
+                      {"lambda": lam, "tolerance": 1e-8, "max_iterations": 8000})
+        return abs(cand[centre] - 0.5)
+
+    assert dist(10.0) < dist(0.01)
+
+
+def test_screened_boundary_pixels_keep_the_anchor(ops):
+    w = h = 16
+    anchor = np.full(w * h, 0.3, np.float32)
+    mask = square_mask(w, h, 5, 11)
+    g = np.tile(np.arange(w, dtype=np.float32), h)
+    cand, _ = run(ops, "screened", w, h, g, anchor, mask, {"lambda": 5.0})
+    assert np.array_equal(cand[mask <= 0.5], anchor[mask <= 0.5])
+
+
+def test_screened_report_kind_and_metrics(ops):
+    w = h = 16
+    mask = square_mask(w, h, 4, 12)
+    _, rep = run(ops, "screened", w, h, bump(w, h), np.full(w * h, 0.2, np.float32), mask,
+                 {"lambda": 1.0, "max_iterations": 3, "tolerance": 1e-12})
+    assert rep.solver.kind == "screened-poisson"
+    assert rep.solver.iterations == 3 and len(rep.solver.residual_history) == 3
+
+
+def test_negative_lambda_is_rejected(ops):
+    w = h = 8
+    z = np.zeros(64, np.float32)
+    with pytest.raises(ops.PaintopError) as e:
+        run(ops, "screened", w, h, z, z, z, {"lambda": -1.0})
+    assert e.value.code == "E_SCREENED_POISSON_PARAM"
+
+
+# ---- solver contract ----------------------------------------------------------------
+
+def random_problem(seed, w, h, c, density=0.6):
+    rng = np.random.default_rng(seed)
+    src = rng.random(w * h * c).astype(np.float32)
+    tgt = rng.random(w * h * c).astype(np.float32)
+    yy, xx = np.mgrid[0:h, 0:w]
+    mask = (((xx - w / 2) / (0.4 * w)) ** 2 + ((yy - h / 2) / (0.4 * h)) ** 2 <= 1.0)
+    mask = (mask & (rng.random((h, w)) < density + 0.4)).astype(np.float32).reshape(-1)
+    return src, tgt, mask
+
+
+@pytest.mark.parametrize("cap", [1, 2, 3, 4, 5, 7, 11, 64])
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3])
+def test_stops_exactly_at_the_cap(ctx, cap, cfg):
+    w, h, c = 150, 90, 2
+    src, tgt, mask = random_problem(cap, w, h, c)
+    ctx.set_config(cfg)
+    try:
+        out, per, worst = ctx.solve(src, tgt, mask, w, h, c, lam=0.0, max_iterations=cap,
+                                    tolerance=1e-14, omega=1.8)
+    finally:
+        ctx.set_config(-1)
+    for r in per:
+        assert r["iterations"] == cap and r["stop_reason"] == "max-iterations"
+        assert not r["converged"] and r["history_len"] == cap
+        assert len(r["residual_history"]) == cap
+        assert r["final_residual"] == r["residual_history"][-1]
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3])
+def test_history_matches_oracle_at_small_sizes(ctx, oracle, cfg):
+    # red-black and lexicographic iterates differ, but both must converge to the
+    # same fixed point; the GPU history is one FP64 residual per sweep.
+    w, h, c = 61, 47, 3
+    src, tgt, mask = random_problem(11, w, h, c)
+    ctx.set_config(cfg)
+    try:
+        out, per, worst = ctx.solve(src, tgt, mask, w, h, c, lam=0.05, max_iterations=4000,
+                                    tolerance=1e-9, omega=1.8)
+    finally:
+        ctx.set_config(-1)
+    cg, ach = oracle.cg_blend_channels(src, tgt, mask, c, w, h, lam=0.05, rel_tol=1e-13)
+    assert np.all(ach <= 1e-12)
+    err = np.abs(out.astype(np.float64) - cg)
+    assert err.max() <= 1e-6, err.max()
+    for r in per:
+        assert r["converged"] and r["final_residual"] <= 1e-9
+        assert len(r["residual_history"]) == r["iterations"]
+        assert r["final_residual"] == r["residual_history"][-1]
+    ref_out, ref_worst, _ = oracle.blend_channels(src, tgt, mask, c, w, h, 4000, 1e-9, 0.05, 1.8)
+    assert np.abs(out - ref_out).max() <= 1e-6
+
+
+def test_non_interior_pixels_equal_target_bitwise(ctx):
+    w, h, c = 203, 77, 4
+    src, tgt, mask = random_problem(5, w, h, c)
+    tgt[::17] = -0.0  # signed zeros and odd values must survive untouched
+    out, _, _ = ctx.solve(src, tgt, mask, w, h, c, lam=0.3, max_iterations=50, tolerance=1e-6)
+    from oracle import oracle as O
+    cells = O.classify_cells(mask, w, h)
+    keep = np.repeat(cells == 0, c)
+    assert np.array_equal(out[keep].view(np.uint32), tgt[keep].view(np.uint32))
+
+
+def test_reruns_byte_identical_large(ctx):
+    w, h, c = 700, 530, 3
+    src, tgt, mask = random_problem(9, w, h, c)
+    a, pa, _ = ctx.solve(src, tgt, mask, w, h, c, lam=0.01, max_iterations=300, tolerance=1e-6)
+    b, pb, _ = ctx.solve(src, tgt, mask, w, h, c, lam=0.01, max_iterations=300, tolerance=1e-6)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert [r["residual_history"] for r in pa] == [r["residual_history"] for r in pb]
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (2, 2), (3, 3), (2, 50), (50, 2), (1, 40), (3, 200)])
+def test_degenerate_grids(ctx, oracle, w, h):
+    c = 2
+    src, tgt, mask = random_problem(w * 100 + h, w, h, c, density=1.0)
+    mask[:] = 1.0
+    out, per, worst = ctx.solve(src, tgt, mask, w, h, c, max_iterations=100, tolerance=1e-8)
+    ref, rworst, rper = oracle.blend_channels(src, tgt, mask, c, w, h, 100, 1e-8, 0.0, 1.8)
+    if min(w, h) < 3:
+        assert np.array_equal(out, tgt)
+        assert all(r["iterations"] == 0 and r["converged"] for r in per)
+    else:
+        assert np.abs(out - ref).max() <= 1e-6
+
+
+def test_empty_mask_and_satisfied_system(ctx):
+    w, h, c = 40, 30, 3
+    src, tgt, _ = random_problem(1, w, h, c)
+    out, per, worst = ctx.solve(src, tgt, np.zeros(w * h, np.float32), w, h, c, max_iterations=10)
+    assert np.array_equal(out, tgt)
+    assert all(r["iterations"] == 0 and r["stop_reason"] == "converged" and
+               r["final_residual"] == 0.0 for r in per)
+    # source == target: r(anchor) = 0 -> 0 iterations (poisson.rs:177-189)
+    out, per, _ = ctx.solve(tgt, tgt, np.ones(w * h, np.float32), w, h, c, max_iterations=10)
+    assert all(r["iterations"] == 0 and r["converged"] for r in per)
+    assert np.array_equal(out, tgt)
+
+
+def test_batch_equals_single_solves(ctx):
+    probs = []
+    for k, (w, h) in enumerate([(64, 40), (130, 257), (300, 220), (17, 9), (512, 80)]):
+        src, tgt, mask = random_problem(20 + k, w, h, 3)
+        probs.append(dict(source=src, target=tgt, mask=mask, width=w, height=h, channels=3,
+                          lam=0.02 * k, max_iterations=500, tolerance=1e-7, omega=1.85))
+    ctx.set_config(3)
+    try:
+        batch = ctx.solve_batch(probs, want_history=True)
+        for p, (bo, bper, bw) in zip(probs, batch):
+            so, sper, sw = ctx.solve(p["source"], p["target"], p["mask"], p["width"], p["height"],
+                                     3, lam=p["lam"], max_iterations=500, tolerance=1e-7,
+                                     omega=1.85)
+            assert np.array_equal(bo.view(np.uint32), so.view(np.uint32))
+            assert [r["residual_history"] for r in bper] == [r["residual_history"] for r in sper]
+    finally:
+        ctx.set_config(-1)
+
+
+def test_warm_start(ctx, oracle):
+    w, h, c = 120, 96, 2
+    src, tgt, mask = random_problem(3, w, h, c)
+    plain, pp, _ = ctx.solve(src, tgt, mask, w, h, c, lam=0.1, max_iterations=3000, tolerance=1e-8)
+    # guess = anchor reproduces the plain solve bit for bit
+    same, ps, _ = ctx.solve(src, tgt, mask, w, h, c, lam=0.1, max_iterations=3000, tolerance=1e-8,
+                            initial_guess=tgt.copy())
+    assert np.array_equal(plain.view(np.uint32), same.view(np.uint32))
+    # guess = the exact solution converges at once, against the same absolute bar
+    cg, _ = oracle.cg_blend_channels(src, tgt, mask, c, w, h, lam=0.1, rel_tol=1e-13)
+    good, pg, _ = ctx.solve(src, tgt, mask, w, h, c, lam=0.1, max_iterations=3000, tolerance=1e-8,
+                            initial_guess=cg.astype(np.float32))
+    assert all(g["iterations"] < p["iterations"] for g, p in zip(pg, pp))
+    assert np.abs(good.astype(np.float64) - cg).max() <= 1e-6
+
+
+def test_watchdog_budget_returns_timeout_and_context_survives(cuda_lib):
+    from paintop_b200 import _lib
+    c = _lib.Context(0)
+    try:
+        w, h, ch = 1024, 1024, 1
+        src, tgt, mask = random_problem(2, w, h, ch)
+        c.set_budget(1e-4)
+        with pytest.raises(_lib.CudaError) as e:
+            c.solve(src, tgt, mask, w, h, ch, max_iterations=100000, tolerance=1e-14, omega=1.5)
+        assert e.value.status == _lib.PT_TIMEOUT
+        c.set_budget(600)
+        out, per, _ = c.solve(src[:4096], tgt[:4096], mask[:4096], 64, 64, 1, max_iterations=10)
+        assert per[0]["iterations"] <= 10
+    finally:
+        c.close()
+
+
+# ---- the benchmark configurations at parity-test sizes ------------------------------
+
+def test_clone_512_against_oracles(ctx, oracle):
+    """512x512 RGB seamless clone, omega 1.9, tol 1e-5, <= 5000 sweeps."""
+    from paintop_b200 import synth
+    inst = synth.clone_512(1)
+    src, tgt, mask = inst.source.reshape(-1), inst.target.reshape(-1), inst.mask.reshape(-1)
+    out, per, worst = ctx.solve(src, tgt, mask, 512, 512, 3, lam=0.0, max_iterations=5000,
+                                tolerance=1e-5, omega=1.9)
+    assert all(r["converged"] for r in per)
+    ref, rworst, rper = oracle.blend_channels(src, tgt, mask, 3, 512, 512, 5000, 1e-5, 0.0, 1.9)
+    assert rworst.converged
+    cg, _ = oracle.cg_blend_channels(src, tgt, mask, 3, 512, 512, lam=0.0, rel_tol=1e-12)
+    e_gpu = np.abs(out.astype(np.float64) - cg)
+    e_cpu = np.abs(ref.astype(np.float64) - cg)
+    # at rel-res 1e-5 the distance to the fixed point is set by the slowest
+    # mode (||r|| / lambda_min); both methods must sit inside the same envelope
+    assert e_gpu.max() <= max(2.0 * e_cpu.max(), 1e-4)
+    # same iteration count within the red-black / lexicographic difference
+    assert abs(worst["iterations"] - rworst.iterations) <= 0.25 * rworst.iterations
+
+
+def test_screened_star_512_within_bounded_tier(ctx, oracle):
+    """The 2048^2 screened workload's generator at 512^2: lambda 0.01, tol 1e-6."""
+    from paintop_b200 import synth
+    inst = synth.screened_2048(3, size=512)
+    src, tgt, mask = inst.source.reshape(-1), inst.target.reshape(-1), inst.mask.reshape(-1)
+    out, per, worst = ctx.solve(src, tgt, mask, 512, 512, 4, lam=0.01, max_iterations=2000,
+                                tolerance=1e-6, omega=1.8)
+    assert all(r["converged"] for r in per)
+    cg, _ = oracle.cg_blend_channels(src, tgt, mask, 4, 512, 512, lam=0.01, rel_tol=1e-12)
+    err = out.astype(np.float64) - cg
+    assert np.abs(err).max() <= BOUNDED_MAX_ABS
+    assert np.sqrt(np.mean(err ** 2)) <= BOUNDED_RMS
+    ref, rworst, _ = oracle.blend_channels(src, tgt, mask, 4, 512, 512, 2000, 1e-6, 0.01, 1.8)
+    d = out.astype(np.float64) - ref
+    assert np.abs(d).max() <= BOUNDED_MAX_ABS and np.sqrt(np.mean(d ** 2)) <= BOUNDED_RMS
