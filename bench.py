@@ -292,19 +292,21 @@ def gpu_arm(args):
     worst_res = max(reps[c].final_residual for c in range(C))
 
     # ---- end-to-end arm (pinned host buffers through the C ABI) --------------
-    for _ in range(max(1, args.warmup)):
-        solve(False)
-    barrier()
-    ev2 = torch.cuda.Event(enable_timing=True)
-    ev3 = torch.cuda.Event(enable_timing=True)
-    ev2.record(stream)
-    for _ in range(args.steps):
-        solve(False)
-        launches += ctx.last_timing()[2]
-    ev3.record(stream)
-    ev3.synchronize()
-    barrier()
-    e2e_elapsed = max_over_ranks(ev2.elapsed_time(ev3) / 1e3)
+    e2e_elapsed = float("nan")
+    if not args.device_only:
+        for _ in range(max(1, args.warmup)):
+            solve(False)
+        barrier()
+        ev2 = torch.cuda.Event(enable_timing=True)
+        ev3 = torch.cuda.Event(enable_timing=True)
+        ev2.record(stream)
+        for _ in range(args.steps):
+            solve(False)
+            launches += ctx.last_timing()[2]
+        ev3.record(stream)
+        ev3.synchronize()
+        barrier()
+        e2e_elapsed = max_over_ranks(ev2.elapsed_time(ev3) / 1e3)
 
     value = ws * args.steps / elapsed
     e2e_value = ws * args.steps / e2e_elapsed
@@ -323,7 +325,8 @@ def gpu_arm(args):
 
     line = None
     if rank == 0:
-        cpu = cpu_baseline_sample(inst) if (ws == 1 and not args.no_cpu_baseline) else None
+        cpu = cpu_baseline_sample(inst) if (ws == 1 and not args.no_cpu_baseline and
+                                             not args.device_only) else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
@@ -364,6 +367,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--device-only", action="store_true",
+                    help="time only the device-resident arm (for profiler runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "cuda":
         args.warmup = 3

@@ -99,6 +99,7 @@ typedef struct pt_report {
   double omega_used;    /* the SOR factor the sweeps used */
   uint32_t refinements; /* FP64 residual-correction steps (incl. the final check) */
   int32_t channel;      /* the channel index (for the worst entry: which channel) */
+  double initial_residual; /* ||r(anchor)||, the FP64 normaliser of every relative residual */
 } pt_report;
 
 pt_status pt_ctx_create(int device, pt_ctx **out);

@@ -7,6 +7,7 @@ Wraps ``oracle/_build/libpaintop_oracle.so`` (built by ``oracle/Makefile``):
 * :func:`blend_channels` -- ``blend_channels`` + ``worse_of``
   (crates/paintop-cpu/src/poisson_blend.rs:168-246) on interleaved f32 images.
 * :func:`cg_blend_channels` -- the FP64 CG tight oracle on the same system.
+* :func:`rb_blend_channels` -- FP64 red-black SOR: the GPU method in FP64.
 
 The C restatement is checked bit-for-bit against the pure-Python restatement in
 ``oracle/pyref.py`` and against the reference's analytic known-answer tests.
@@ -101,6 +102,10 @@ def lib():
                                            C.c_size_t, C.c_size_t, C.c_double, C.c_double,
                                            C.c_uint32, C.c_void_p, C.c_void_p]
         L.pr_cg_blend_channels.restype = C.c_int
+        L.pr_rb_blend_channels.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                           C.c_size_t, C.c_size_t, _Controls, C.c_double,
+                                           C.c_void_p, C.POINTER(_Report), C.c_void_p]
+        L.pr_rb_blend_channels.restype = C.c_int
         _lib = L
     return _lib
 
@@ -176,6 +181,30 @@ def blend_channels(source, target, mask, channels, width, height, max_iterations
     else:
         worst_rep = per[worst.value]
     return out, worst_rep, per
+
+
+def rb_blend_channels(source, target, mask, channels, width, height, max_iterations=2000,
+                      tolerance=1e-6, lam=0.0, omega=1.8):
+    """FP64 red-black SOR (the GPU method in FP64) -> (field f64 interleaved, per-channel reports)."""
+    source = np.ascontiguousarray(source, dtype=np.float32).reshape(-1)
+    target = np.ascontiguousarray(target, dtype=np.float32).reshape(-1)
+    mask = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1)
+    n = width * height
+    out = np.empty(n * channels, dtype=np.float64)
+    reps = (_Report * max(channels, 1))()
+    hist = np.zeros(max(channels, 1) * max(int(max_iterations), 1), dtype=np.float64)
+    rc = lib().pr_rb_blend_channels(_p(source), _p(target), _p(mask), channels, width, height,
+                                    _Controls(int(max_iterations), float(tolerance), float(omega)),
+                                    float(lam), _p(out), reps, _p(hist))
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    per = []
+    for c in range(channels):
+        r = reps[c]
+        h = hist[c * max_iterations: c * max_iterations + r.iterations].tolist()
+        per.append(SolveReport(r.iterations, bool(r.converged), STOP_REASONS[r.stop_reason],
+                               r.tolerance, r.final_residual, h))
+    return out, per
 
 
 def cg_blend_channels(source, target, mask, channels, width, height, lam=0.0, rel_tol=1e-12,

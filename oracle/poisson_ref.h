@@ -66,6 +66,14 @@ int pr_cg_blend_channels(const float *source, const float *target, const float *
                          double rel_tol, uint32_t max_iterations, double *out_f64,
                          double *achieved);
 
+/* FP64 red-black SOR (the GPU method in FP64): same controls and report. */
+void pr_rb_solve(const pr_system *s, pr_controls c, double *field, double *history,
+                 pr_report *rep);
+int pr_rb_blend_channels(const float *source, const float *target, const float *mask,
+                         size_t channels, size_t width, size_t height, pr_controls c,
+                         double lambda, double *out_f64, pr_report *per_channel,
+                         double *histories);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,6 +45,7 @@ class PtReport(C.Structure):
         ("iterations", C.c_uint32), ("converged", C.c_int32), ("stop_reason", C.c_int32),
         ("tolerance", C.c_double), ("final_residual", C.c_double), ("history_len", C.c_uint32),
         ("omega_used", C.c_double), ("refinements", C.c_uint32), ("channel", C.c_int32),
+        ("initial_residual", C.c_double),
     ]
 
     def as_dict(self, history=None):
@@ -52,7 +53,8 @@ class PtReport(C.Structure):
                  stop_reason=STOP_REASONS[self.stop_reason] if 0 <= self.stop_reason < 3 else "?",
                  tolerance=float(self.tolerance), final_residual=float(self.final_residual),
                  history_len=int(self.history_len), omega_used=float(self.omega_used),
-                 refinements=int(self.refinements), channel=int(self.channel))
+                 refinements=int(self.refinements), channel=int(self.channel),
+                 initial_residual=float(self.initial_residual))
         if history is not None:
             d["residual_history"] = history
         return d

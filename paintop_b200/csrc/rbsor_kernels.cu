@@ -26,7 +26,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 __device__ __forceinline__ int ld_vol(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
 // Deterministic block sum: fixed xor-butterfly inside each warp, then warps in
-// index order. The total is valid in thread 0. Uses sred[0..kWarps).
+// index order. The total is valid in thread 0. Uses sred[0 .. blockDim.x/32).
 __device__ __forceinline__ double block_sum(double v, double *sred) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -35,7 +35,7 @@ __device__ __forceinline__ double block_sum(double v, double *sred) {
   __syncthreads();
   double tot = 0.0;
   if (threadIdx.x == 0)
-    for (int w = 0; w < kWarps; ++w) tot += sred[w];
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sred[w];
   __syncthreads();
   return tot;
 }

@@ -383,6 +383,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       r.omega_used = pl.sys[sys0[i] + c].omega;
       r.refinements = (uint32_t)s.refinements;
       r.channel = (int)c;
+      r.initial_residual = s.r0;
       reports[i][c] = r;
       // worse_of (poisson_blend.rs:240-246)
       if (worst < 0) worst = (int)c;

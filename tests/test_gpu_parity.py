@@ -335,8 +335,15 @@ def test_clone_512_against_oracles(ctx, oracle):
     # at rel-res 1e-5 the distance to the fixed point is set by the slowest
     # mode (||r|| / lambda_min); both methods must sit inside the same envelope
     assert e_gpu.max() <= max(2.0 * e_cpu.max(), 1e-4)
-    # same iteration count within the red-black / lexicographic difference
-    assert abs(worst["iterations"] - rworst.iterations) <= 0.25 * rworst.iterations
+    # the GPU method (FP32 sweeps, FP64 residual correction) must take the
+    # sweeps the same red-black ordering takes in FP64: red-black SOR at this
+    # omega needs ~2x the sweeps of the reference's row-major order, which is a
+    # property of the ordering, not of the precision scheme
+    _, rb = oracle.rb_blend_channels(src, tgt, mask, 3, 512, 512, 5000, 1e-5, 0.0, 1.9)
+    for g, r in zip(per, rb):
+        assert abs(g["iterations"] - r.iterations) <= max(2, 0.01 * r.iterations)
+        k = min(g["iterations"], r.iterations) - 1
+        assert abs(g["residual_history"][k] - r.residual_history[k]) <= 1e-3 * r.residual_history[k] + 1e-9
 
 
 def test_screened_star_512_within_bounded_tier(ctx, oracle):
