@@ -216,6 +216,38 @@ pt_status pt_autotune(pt_ctx *ctx, const pt_problem *ps, uint32_t n, uint32_t re
                       float *const *outs, pt_report *const *reports, int32_t *chosen,
                       double *ms_per_config);
 
+/* ---- solving without allocating (no counterpart in the reference) -------- */
+
+/* Size of the fixed device scratch array behind pt_poisson_solve_noalloc.
+ * Every GPU that loads the library holds this much device memory until the
+ * process exits. 64 MiB fits one 1024x1024 single-channel image or one 512x512
+ * RGBA image with 2000 sweeps of history. */
+#define PT_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+/* pt_poisson_solve for callers that may not allocate memory: hosts whose device
+ * memory belongs to another allocator (a plugin inside a framework's caching
+ * pool must not call cudaMalloc/cudaFree behind it) and latency-critical threads
+ * that cannot take the device synchronisation cudaMalloc/cudaFree may cause. It
+ * needs no pt_ctx and makes no allocation call of any kind: its working memory
+ * is a file-scope device array of PT_NOALLOC_SCRATCH_BYTES.
+ *   p:         PT_FLAG_DEVICE_POINTERS must be set (inputs are the caller's
+ *              device buffers); PT_FLAG_WARM_START and PT_FLAG_OMEGA_AUTO are
+ *              not supported; at most 8 channels.
+ *   out_candidate: device buffer, width*height*channels f32.
+ *   reports:   host array of channels + 1 entries, as pt_poisson_solve.
+ *   history:   device buffer of channels * max_iterations doubles, or NULL.
+ *   stream:    the caller's cudaStream_t (NULL: the legacy default stream); the
+ *              call returns after that stream has finished the solve.
+ * Returns PT_OOM, before touching the GPU, when the problem needs more scratch
+ * than PT_NOALLOC_SCRATCH_BYTES. The first call on each device (made with that
+ * device current) looks up the array's device address once; make that first
+ * call before any stream capture. All calls share the one array and leave their
+ * contents in it; calls whose GPU work overlapped would race on it, so each call
+ * holds a process-wide lock and waits for its stream before returning. Uses the
+ * built-in tile configuration, never the tuned table. */
+pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_candidate, pt_report *reports,
+                                   double *history, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,8 +26,9 @@ EXPORTED = (
     "pt_ctx_create", "pt_ctx_destroy", "pt_poisson_solve", "pt_poisson_solve_batch",
     "pt_op_compute", "pt_status_str", "pt_ctx_last_error", "pt_tile_config_count",
     "pt_tile_config_info", "pt_ctx_set_config", "pt_ctx_last_config", "pt_autotune",
-    "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing",
+    "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_poisson_solve_noalloc",
 )
+PT_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 
 class PtProblem(C.Structure):
@@ -131,6 +132,8 @@ def lib():
     L.pt_ctx_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                      C.POINTER(C.c_int64)]
     L.pt_ctx_last_timing.restype = C.c_int
+    L.pt_poisson_solve_noalloc.argtypes = [C.POINTER(PtProblem), vp, C.POINTER(PtReport), vp, vp]
+    L.pt_poisson_solve_noalloc.restype = C.c_int
     _lib = L
     return L
 

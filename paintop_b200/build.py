@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "libpaintop_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                    "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["rbsor_kernels.cu", "solver_host.cu", "op_host.cpp", "autotune.cpp"]
+SOURCES = ["rbsor_kernels.cu", "solver_host.cu", "op_host.cpp", "autotune.cpp", "noalloc.cu"]
 
 
 def nvcc() -> str:
