@@ -100,13 +100,16 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   const long long ntiles = tps * C;
   const long long plane = (long long)H * pw;
   const long long cells = 2 * plane * C;
-  size_t o = 0, sys_o, st_o, tiles_o, tc_o, e0_o, e1_o, g_o, cell_o, u_o, bp_o, part_o, fpart_o,
+  size_t o = 0, sys_o, st_o, claim_o, arrive_o, tiles_o, tc_o, act_o, e0_o, e1_o, g_o, cell_o, u_o, bp_o, part_o, fpart_o,
          hist_o, bar_o, err_o;
   auto take = [&](size_t bytes) { size_t r = o; o = aup(o + (bytes ? bytes : 1)); return r; };
   sys_o = take(C * sizeof(SysDesc));
   st_o = take(C * sizeof(SysState));
+  claim_o = take(C * sizeof(unsigned long long));
+  arrive_o = take(C * sizeof(unsigned));
   tiles_o = take(ntiles * sizeof(Tile));
   tc_o = take(ntiles * sizeof(int));
+  act_o = take(ntiles * sizeof(int));
   e0_o = take(cells * sizeof(float));
   e1_o = take(cells * sizeof(float));
   g_o = take(cells * sizeof(float));
@@ -116,7 +119,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   part_o = take((size_t)tc.S * ntiles * sizeof(double));
   fpart_o = take(2 * ntiles * sizeof(double));
   hist_o = take((size_t)C * p->max_iterations * sizeof(double));
-  bar_o = take(4 * sizeof(unsigned));
+  bar_o = take(kBarWords * sizeof(unsigned));
   err_o = take(sizeof(int));
   if (o > (size_t)PT_NOALLOC_SCRATCH_BYTES) return PT_OOM;  // does not fit the fixed array
 
@@ -159,6 +162,9 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   P.st = reinterpret_cast<SysState *>(base + st_o);
   P.tiles = reinterpret_cast<const Tile *>(base + tiles_o);
   P.tcount = reinterpret_cast<int *>(base + tc_o);
+  P.act = reinterpret_cast<int *>(base + act_o);
+  P.claim = reinterpret_cast<unsigned long long *>(base + claim_o);
+  P.arrive = reinterpret_cast<unsigned *>(base + arrive_o);
   P.ntiles = (int)ntiles;
   P.nsys = (int)C;
   P.e0 = reinterpret_cast<float *>(base + e0_o);
@@ -177,7 +183,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
 
   // the array keeps the previous call's contents: zero what must start at zero
   cudaError_t e = cudaMemcpyAsync(base + sys_o, descs, C * sizeof(SysDesc), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(base + bar_o, 0, 4 * sizeof(unsigned), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + bar_o, 0, kBarWords * sizeof(unsigned), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(base + err_o, 0, sizeof(int), st);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(base + hist_o, 0, (size_t)C * p->max_iterations * sizeof(double), st);

@@ -32,13 +32,16 @@
 // residual of the owned cells after every sweep, and writes the owned cells to
 // the other ping-pong buffer. Tiles without interior cells are never swept.
 //
-// Control. One persistent cooperative kernel runs all steps of all systems.
-// After each step the last tile of a system to finish (per-system arrival
-// counter) sums that system's per-tile partials in tile order -- a fixed order
-// that depends on nothing but the tile grid, so reruns are byte-identical --
-// and advances the system's state machine (record history, test tolerance,
-// stall, cap; choose the next mode). A grid barrier with bounded waits
-// separates steps.
+// Control. One persistent kernel runs all steps of all systems as a dataflow:
+// each system publishes its current step through a claim word (generation,
+// next tile); any block takes the next tile of any system whose step is open.
+// The last tile of a system to finish a step (per-system arrival counter) sums
+// that system's per-tile partials in tile order -- a fixed order that depends
+// on nothing but the tile grid, so reruns are byte-identical -- advances the
+// system's state machine (record history, test tolerance, stall, cap; choose
+// the next mode) and publishes the next generation. Systems therefore advance
+// independently; no block ever waits for a particular other block, and an
+// idle block's wait for work is bounded by a watchdog.
 #pragma once
 
 #include <cstdint>
@@ -63,7 +66,7 @@ enum Pending : int { P_NONE = 0, P_CONV = 1, P_STALL = 2, P_MAX = 3, P_REFINE = 
 enum Stop : int { STOP_CONVERGED = 0, STOP_MAX = 1, STOP_STALLED = 2 };
 
 // Error codes written to the kernel error word.
-enum KErr : int { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_DEADLINE = 2 };
+enum KErr : int { KERR_NONE = 0, KERR_STALLED = 1, KERR_DEADLINE = 2 };
 
 // poisson.rs:80,85 -- stall window and improvement fraction.
 constexpr unsigned kStallWindow = 16;
@@ -103,10 +106,17 @@ struct SysDesc {
 struct SysState {
   int mode, s, iterations, cur;
   int pending, status, refinements, since;
-  int isince, nact, out_anchor, pad;
-  unsigned arrive, pad2;
+  int isince, nact, out_anchor, steps;
+  int pad0, pad1;
   double r0, outer, best, ibest, last, ibase;
 };
+
+// Control words of the persistent kernel: [2] systems done. The host zeroes
+// them before every launch.
+constexpr int kBarWords = 16;
+// A claim word's low half once its system is done: never below any tile count,
+// and far from overflowing into the generation half however often it is bumped.
+constexpr unsigned kClaimDone = 0x7fffffffu;
 
 struct Tile {
   int sys, tx, ty, pad;
@@ -124,7 +134,11 @@ struct KParams {
   double *partial;         // [S][ntiles]
   double *fpart;           // [2][ntiles] assembly partials
   double *hist;
-  unsigned *bar;           // [0] count, [1] generation, [2] systems done, [3] its snapshot
+  int *act;                // per system, its tiles with interior cells, in index order
+                           // (stored at the system's tile range)
+  unsigned long long *claim;  // per system: generation << 32 | next tile to hand out
+  unsigned *arrive;        // per system: tiles finished in the current generation
+  unsigned *bar;           // control words, kBarWords of them
   int *err;
   unsigned long long budget_ns;
   int S;                   // sweeps per step of this launch

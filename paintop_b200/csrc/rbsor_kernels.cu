@@ -44,41 +44,6 @@ __device__ __forceinline__ long long plane_index(const SysDesc &d, int c, int y,
   return d.off + (long long)c * d.plane + (long long)y * d.pw + i;
 }
 
-// Bounded grid barrier over a cooperative launch (all blocks co-resident).
-// Returns false if an error was raised anywhere or the wait gave up.
-__device__ bool grid_sync(unsigned *bar, int *err) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    const unsigned gen = ld_acquire(bar + 1);
-    __threadfence();
-    const unsigned prev = atomicAdd(bar, 1u);
-    if (prev == gridDim.x - 1) {
-      // every block has arrived: snapshot the done counter for this step (a
-      // block that leaves the barrier early may already bump bar[2] in the next
-      // step, so blocks must not read bar[2] itself to decide to exit)
-      atomicExch(bar + 3, atomicAdd(bar + 2, 0u));
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      // A step is at most milliseconds; 20 s without a release means something
-      // is wrong: record it and leave instead of waiting forever.
-      const unsigned long long give_up = gtimer() + 20ull * 1000000000ull;
-      while (ld_acquire(bar + 1) == gen) {
-        if (ld_vol(err) != 0) { ok = 0; break; }
-        if (gtimer() > give_up) { atomicCAS(err, 0, KERR_BARRIER_TIMEOUT); ok = 0; break; }
-        __nanosleep(40);
-      }
-    }
-    __threadfence();
-    s_ok = ok && (ld_vol(err) == 0);
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
 // ----------------------------------------------------------------------------
 // geometry of one tile configuration
 // ----------------------------------------------------------------------------
@@ -233,8 +198,8 @@ __global__ void k_init(KParams P) {
   SysState s;
   s.mode = M_SWEEP; s.s = 0; s.iterations = 0; s.cur = 0;
   s.pending = P_NONE; s.status = -1; s.refinements = 0; s.since = 0;
-  s.isince = 0; s.nact = n; s.out_anchor = 0; s.pad = 0;
-  s.arrive = 0; s.pad2 = 0;
+  s.isince = 0; s.nact = n; s.out_anchor = 0; s.steps = 0;
+  s.pad0 = 0; s.pad1 = 0;
   s.r0 = sqrt(sa); s.outer = sqrt(su);
   s.best = INFINITY; s.ibest = INFINITY; s.last = 1.0; s.ibase = s.outer;
   // poisson.rs:172-189: no unknowns or a satisfied system -> 0 iterations, converged.
@@ -249,6 +214,37 @@ __global__ void k_init(KParams P) {
     s.s = d.max_it < P.S ? d.max_it : P.S;
   }
   P.st[sys] = s;
+  P.arrive[sys] = 0;
+  P.claim[sys] = s.mode == M_DONE ? (unsigned long long)kClaimDone : 0ull;
+}
+
+// Per system, the tiles with interior cells in index order (one block per
+// system; a block-wide exclusive scan keeps the order fixed).
+__global__ void k_compact(KParams P) {
+  __shared__ int sw[32];
+  __shared__ int s_base;
+  const SysDesc d = P.sys[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  for (int k0 = 0; k0 < d.ntiles; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    const int flag = (k < d.ntiles && P.tcount[d.tile0 + k] > 0) ? 1 : 0;
+    const unsigned m = __ballot_sync(0xffffffffu, flag);
+    const int before = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) sw[warp] = __popc(m);
+    __syncthreads();
+    int off = s_base;
+    for (int w = 0; w < warp; ++w) off += sw[w];
+    if (flag) P.act[d.tile0 + off + before] = d.tile0 + k;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int w = 0; w < nw; ++w) tot += sw[w];
+      s_base += tot;
+    }
+    __syncthreads();
+  }
 }
 
 // Interleave the result: interior cells take (float)u (the reference's `as f32`,
@@ -312,56 +308,96 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
   const int pl = Y0 & 1;  // colour parity of loaded row 0 (column 0 is even)
   const float w = d.omega, inv = d.inv_denom;
   const double dd = 4.0 + d.lambda;
-  for (int j = 0; j < s; ++j) {
+  constexpr int OX0 = G::HX, OX1 = G::HX + G::TW;  // owned loaded columns
+  constexpr int OY0 = G::H, OY1 = G::H + TH;       // owned loaded rows
+  constexpr int RW = kPWL / 2;                      // float2 per plane row (one per lane)
+  // Each lane owns the aligned pair of plane indices (2 lane, 2 lane + 1) of a
+  // row; a warp owns whole rows. The residual of a state is assembled from the
+  // passes that already hold its values: black cells' residual of state j right
+  // after their update in sweep j, red cells' residual of state j just before
+  // their update in sweep j+1 (or in a last pass after the final sweep).
+  double acc[S];
+#pragma unroll
+  for (int j = 0; j < S; ++j) acc[j] = 0.0;
+
+  auto resid = [&](float l, float r, float u, float dn, float e, float g) -> double {
+    const double ns = (((double)l + (double)r) + (double)u) + (double)dn;
+    const double rr = fma(-dd, (double)e, ns) - (double)g;
+    return rr * rr;
+  };
+
+#pragma unroll
+  for (int j = 0; j < S; ++j) {
+    if (j >= s) break;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int tt = 2 * j + h + 1;  // half-sweep number: valid window shrinks by tt
-      float *Ec = sE + h * G::PLANE;
-      const float *Eo = sE + (1 - h) * G::PLANE;
-      const float *Gc = sG + h * G::PLANE;
-      const uint8_t *Cc = sC + h * G::PLANE;
+      float2 *Ec = reinterpret_cast<float2 *>(sE + h * G::PLANE);
+      const float2 *Eo = reinterpret_cast<const float2 *>(sE + (1 - h) * G::PLANE);
+      const float2 *Gc = reinterpret_cast<const float2 *>(sG + h * G::PLANE);
+      const uint16_t *Cc = reinterpret_cast<const uint16_t *>(sC + h * G::PLANE);
       const int yhi = G::LH - 1 - tt;
       const int xlo = G::XOFF + tt, xhi = kLW - 1 - G::XOFF - tt;
+      const bool duty = (h == 1) || (j > 0);  // residual of black state j / red state j-1
+      double part = 0.0;
       for (int ly = tt + warp; ly <= yhi; ly += kWarps) {
         const int q = (h + ly + pl) & 1;
-        const int ilo = (xlo - q + 1) >> 1, ihi = (xhi - q) >> 1;
-        const int rb = ly * kPWL;
-        for (int i = ilo + lane; i <= ihi; i += 32) {
-          const int o = rb + i;
-          if (Cc[o]) {
-            const float ns = ((Eo[o - 1 + q] + Eo[o + q]) + Eo[o - kPWL]) + Eo[o + kPWL];
-            const float tg = (ns - Gc[o]) * inv;
-            const float e = Ec[o];
-            Ec[o] = fmaf(w, tg - e, e);
-          }
+        const int r2 = ly * RW + lane;
+        const float2 up = Eo[r2 - RW], dn = Eo[r2 + RW], ct = Eo[r2];
+        const float2 gc = Gc[r2];
+        const float2 ec = Ec[r2];
+        const unsigned cc = Cc[r2];
+        const float far = q ? __shfl_down_sync(0xffffffffu, ct.x, 1)
+                            : __shfl_up_sync(0xffffffffu, ct.y, 1);
+        const float l0 = q ? ct.x : far, r0 = q ? ct.y : ct.x;
+        const float l1 = q ? ct.y : ct.x, r1 = q ? far : ct.y;
+        const int x0 = 4 * lane + q, x1 = x0 + 2;  // loaded columns of the pair
+        const bool a0 = (cc & 0xffu) && x0 >= xlo && x0 <= xhi;
+        const bool a1 = (cc & 0xff00u) && x1 >= xlo && x1 <= xhi;
+        float n0 = ec.x, n1 = ec.y;
+        if (a0) n0 = fmaf(w, (((l0 + r0) + up.x) + dn.x - gc.x) * inv - ec.x, ec.x);
+        if (a1) n1 = fmaf(w, (((l1 + r1) + up.y) + dn.y - gc.y) * inv - ec.y, ec.y);
+        if (duty && ly >= OY0 && ly < OY1) {
+          if (a0 && x0 >= OX0 && x0 < OX1) part += resid(l0, r0, up.x, dn.x, h ? n0 : ec.x, gc.x);
+          if (a1 && x1 >= OX0 && x1 < OX1) part += resid(l1, r1, up.y, dn.y, h ? n1 : ec.y, gc.y);
         }
+        Ec[r2] = make_float2(n0, n1);
       }
+      if (h == 1) acc[j] += part;
+      else if (j > 0) acc[j - 1] += part;
       __syncthreads();
     }
-    // FP64 residual of the owned cells after sweep j.
-    double acc = 0.0;
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const float *Ec = sE + c * G::PLANE;
-      const float *Eo = sE + (1 - c) * G::PLANE;
-      const float *Gc = sG + c * G::PLANE;
-      const uint8_t *Cc = sC + c * G::PLANE;
-      for (int ly = G::H + warp; ly < G::H + TH; ly += kWarps) {
-        const int q = (c + ly + pl) & 1;
-        const int rb = ly * kPWL;
-        for (int i = G::HX / 2 + lane; i < G::HX / 2 + G::TW / 2; i += 32) {
-          const int o = rb + i;
-          if (Cc[o]) {
-            const double ns = (((double)Eo[o - 1 + q] + (double)Eo[o + q]) + (double)Eo[o - kPWL]) +
-                              (double)Eo[o + kPWL];
-            const double r = fma(-dd, (double)Ec[o], ns) - (double)Gc[o];
-            acc = fma(r, r, acc);
-          }
-        }
-      }
+  }
+  // red cells' residual of the final state
+  {
+    const float2 *Er = reinterpret_cast<const float2 *>(sE);
+    const float2 *Eb = reinterpret_cast<const float2 *>(sE + G::PLANE);
+    const float2 *Gr = reinterpret_cast<const float2 *>(sG);
+    const uint16_t *Cr = reinterpret_cast<const uint16_t *>(sC);
+    double part = 0.0;
+    for (int ly = OY0 + warp; ly < OY1; ly += kWarps) {
+      const int q = (ly + pl) & 1;
+      const int r2 = ly * RW + lane;
+      const float2 up = Eb[r2 - RW], dn = Eb[r2 + RW], ct = Eb[r2];
+      const float2 gc = Gr[r2], ec = Er[r2];
+      const unsigned cc = Cr[r2];
+      const float far = q ? __shfl_down_sync(0xffffffffu, ct.x, 1)
+                          : __shfl_up_sync(0xffffffffu, ct.y, 1);
+      const float l0 = q ? ct.x : far, r0 = q ? ct.y : ct.x;
+      const float l1 = q ? ct.y : ct.x, r1 = q ? far : ct.y;
+      const int x0 = 4 * lane + q, x1 = x0 + 2;
+      if ((cc & 0xffu) && x0 >= OX0 && x0 < OX1) part += resid(l0, r0, up.x, dn.x, ec.x, gc.x);
+      if ((cc & 0xff00u) && x1 >= OX0 && x1 < OX1) part += resid(l1, r1, up.y, dn.y, ec.y, gc.y);
     }
-    acc = block_sum(acc, sred);
-    if (tid == 0) P.partial[(long long)j * P.ntiles + t] = acc;
+#pragma unroll
+    for (int j = 0; j < S; ++j)
+      if (j == s - 1) acc[j] += part;
+  }
+#pragma unroll
+  for (int j = 0; j < S; ++j) {
+    if (j >= s) break;
+    const double tot = block_sum(acc[j], sred);
+    if (tid == 0) P.partial[(long long)j * P.ntiles + t] = tot;
   }
 
   // ---- write the owned cells
@@ -536,9 +572,53 @@ __device__ void advance(const KParams &P, const SysDesc &d, SysState *stp, int m
     default:
       break;
   }
-  s.arrive = 0;
+  s.steps += 1;
   *stp = s;
-  __threadfence();
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Thread 0: claim the next open tile of any system, starting at system `rot`.
+// Returns the system (or -1 when every system is done, an error was raised or
+// the wait for work exceeded its bound) and sets *idx, *gen.
+__device__ int claim_tile(const KParams &P, int rot, int *idx, unsigned *gen,
+                          unsigned long long t_start) {
+  unsigned long long idle_from = 0;
+  for (;;) {
+    // an error anywhere or the wall budget ends every block at its next claim
+    if (ld_vol(P.err) != 0) return -1;
+    if (gtimer() - t_start > P.budget_ns) {
+      atomicCAS(P.err, 0, KERR_DEADLINE);
+      return -1;
+    }
+    for (int k = 0; k < P.nsys; ++k) {
+      int c = rot + k;
+      if (c >= P.nsys) c -= P.nsys;
+      const unsigned nact = (unsigned)__ldcg(&P.st[c].nact);
+      if ((unsigned)ld_acquire_u64(P.claim + c) >= nact) continue;  // step fully handed out
+      const unsigned long long cw = atomicAdd(P.claim + c, 1ull);
+      if ((unsigned)cw < nact) {
+        *idx = (int)(unsigned)cw;
+        *gen = (unsigned)(cw >> 32);
+        __threadfence();  // the claimed generation's state was published before its claim word
+        return c;
+      }
+    }
+    if (ld_acquire(P.bar + 2) >= (unsigned)P.nsys) return -1;
+    const unsigned long long now = gtimer();
+    // every open step is handed out and being finished by other blocks; a
+    // step takes milliseconds at most, so 20 s without work is a fault
+    if (!idle_from) idle_from = now;
+    else if (now - idle_from > 20ull * 1000000000ull) {
+      atomicCAS(P.err, 0, KERR_STALLED);
+      return -1;
+    }
+    __nanosleep(64);
+  }
 }
 
 template <int S, int TH>
@@ -549,60 +629,75 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
   float *sG = sE + 2 * G::PLANE;
   uint8_t *sC = reinterpret_cast<uint8_t *>(sG + 2 * G::PLANE);
   double *sred = reinterpret_cast<double *>(sC + 2 * G::PLANE);
-  __shared__ int s_last;
+  __shared__ int s_last, s_sys, s_idx;
+  __shared__ unsigned s_gen;
   const unsigned long long t_start = gtimer();
+  int rot = P.nsys > 0 ? (int)(blockIdx.x % (unsigned)P.nsys) : 0;
 
   for (;;) {
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-      if (__ldg(P.tcount + t) == 0) continue;
-      const Tile tl = P.tiles[t];
-      SysState *stp = P.st + tl.sys;
-      const int mode = __ldcg(&stp->mode);
-      if (mode == M_DONE) continue;
-      const int s = __ldcg(&stp->s);
-      const int cur = __ldcg(&stp->cur);
-      const SysDesc d = P.sys[tl.sys];
-      if (mode == M_SWEEP || mode == M_REDO) {
-        sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
-      } else if (mode == M_FOLD) {
-        fold_tile<S, TH>(P, d, tl, cur);
-      } else {
-        resid_tile<S, TH>(P, d, t, tl, sred);
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned a = atomicAdd(&stp->arrive, 1u);
-        s_last = (a == (unsigned)__ldcg(&stp->nact) - 1u);
-        __threadfence();
-      }
-      __syncthreads();
-      if (s_last) {
-        // this block finished the system's step last: reduce in tile order
-        double part[S];
+    if (threadIdx.x == 0) {
+      int idx = 0;
+      unsigned gen = 0;
+      const int sys = claim_tile(P, rot, &idx, &gen, t_start);
+      s_sys = sys;
+      s_idx = idx;
+      s_gen = gen;
+    }
+    __syncthreads();
+    const int sys = s_sys, idx = s_idx;
+    const unsigned gen = s_gen;
+    __syncthreads();
+    if (sys < 0) break;
+    rot = sys;
+    const SysDesc d = P.sys[sys];
+    const int t = __ldcg(P.act + d.tile0 + idx);
+    const Tile tl = P.tiles[t];
+    SysState *stp = P.st + sys;
+    const int mode = __ldcg(&stp->mode);
+    const int s = __ldcg(&stp->s);
+    const int cur = __ldcg(&stp->cur);
+    if (mode == M_SWEEP || mode == M_REDO) {
+      sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
+    } else if (mode == M_FOLD) {
+      fold_tile<S, TH>(P, d, tl, cur);
+    } else {
+      resid_tile<S, TH>(P, d, t, tl, sred);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned a = atomicAdd(P.arrive + sys, 1u);
+      s_last = (a == (unsigned)__ldcg(&stp->nact) - 1u);
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_last) {
+      // the system's step is complete: reduce its partials in tile order,
+      // advance its state machine and open its next step
+      double part[S];
 #pragma unroll
-        for (int j = 0; j < S; ++j) part[j] = 0.0;
-        const int nsum = (mode == M_SWEEP) ? s : (mode == M_RESID ? 1 : 0);
-        if (nsum > 0) {
-          for (int k = d.tile0 + threadIdx.x; k < d.tile0 + d.ntiles; k += kThreads) {
-            if (__ldg(P.tcount + k) == 0) continue;
-#pragma unroll
-            for (int j = 0; j < S; ++j)
-              if (j < nsum) part[j] += __ldcg(P.partial + (long long)j * P.ntiles + k);
-          }
+      for (int j = 0; j < S; ++j) part[j] = 0.0;
+      const int nsum = (mode == M_SWEEP) ? s : (mode == M_RESID ? 1 : 0);
+      const int nact = __ldcg(&stp->nact);
+      if (nsum > 0) {
+        for (int k = threadIdx.x; k < nact; k += kThreads) {
+          const int tk = __ldcg(P.act + d.tile0 + k);
 #pragma unroll
           for (int j = 0; j < S; ++j)
-            if (j < nsum) part[j] = block_sum(part[j], sred);
+            if (j < nsum) part[j] += __ldcg(P.partial + (long long)j * P.ntiles + tk);
         }
-        if (threadIdx.x == 0) advance(P, d, stp, mode, part);
-        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < S; ++j)
+          if (j < nsum) part[j] = block_sum(part[j], sred);
       }
-    }
-    if (!grid_sync(P.bar, P.err)) break;
-    if (__ldcg(P.bar + 3) >= (unsigned)P.nsys) break;
-    if (gtimer() - t_start > P.budget_ns) {
-      atomicCAS(P.err, 0, KERR_DEADLINE);
-      break;
+      if (threadIdx.x == 0) {
+        advance(P, d, stp, mode, part);
+        P.arrive[sys] = 0;
+        __threadfence();
+        const unsigned long long next = (unsigned long long)(gen + 1u) << 32;
+        atomicExch(P.claim + sys, __ldcg(&stp->mode) == M_DONE ? (next | kClaimDone) : next);
+      }
+      __syncthreads();
     }
   }
 }
@@ -625,9 +720,10 @@ static cudaError_t launch_solve_t(const KParams &P, int sms, cudaStream_t stream
   *grid_out = grid;
   KParams Pc = P;
   Pc.S = S;
-  void *args[] = {&Pc};
-  return cudaLaunchCooperativeKernel((const void *)k_solve<S, TH>, dim3(grid), dim3(kThreads),
-                                     args, G::kSmem, stream);
+  // No block waits for a particular other block (work is claimed, never
+  // assigned), so an ordinary launch suffices; the grid fills the GPU once.
+  k_solve<S, TH><<<grid, kThreads, G::kSmem, stream>>>(Pc);
+  return cudaGetLastError();
 }
 
 int tile_config_count() { return 4; }
@@ -653,6 +749,7 @@ size_t tile_config_smem(int idx) {
 cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream) {
   if (P.ntiles <= 0) return cudaSuccess;
   k_tile_count<<<P.ntiles, 256, 0, stream>>>(P, tc.tw, tc.th);
+  k_compact<<<P.nsys, 256, 0, stream>>>(P);
   k_assemble<<<P.ntiles, kThreads, 0, stream>>>(P, tc.tw, tc.th);
   k_init<<<P.nsys, 256, 0, stream>>>(P);
   return cudaGetLastError();

@@ -118,8 +118,8 @@ struct Plan {
 
 // Arena layout (byte offsets) for one call.
 struct Layout {
-  size_t sys, st, tiles, tcount, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in, mask,
-      out, total;
+  size_t sys, st, claim, arrive, tiles, tcount, act, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in,
+      mask, out, total;
 };
 
 Layout layout(const Plan &pl, bool stage) {
@@ -129,8 +129,11 @@ Layout layout(const Plan &pl, bool stage) {
   const size_t nt = pl.tiles.size(), ns = pl.sys.size();
   L.sys = take(ns * sizeof(SysDesc));
   L.st = take(ns * sizeof(SysState));
+  L.claim = take(ns * sizeof(unsigned long long));
+  L.arrive = take(ns * sizeof(unsigned));
   L.tiles = take(nt * sizeof(Tile));
   L.tcount = take(nt * sizeof(int));
+  L.act = take(nt * sizeof(int));
   L.e0 = take(pl.cells * sizeof(float));
   L.e1 = take(pl.cells * sizeof(float));
   L.g = take(pl.cells * sizeof(float));
@@ -140,7 +143,7 @@ Layout layout(const Plan &pl, bool stage) {
   L.partial = take((size_t)pl.tc.S * nt * sizeof(double));
   L.fpart = take(2 * nt * sizeof(double));
   L.hist = take(pl.hist * sizeof(double));
-  L.bar = take(4 * sizeof(unsigned));
+  L.bar = take(kBarWords * sizeof(unsigned));
   L.err = take(sizeof(int));
   L.in = stage ? take(pl.in_floats * sizeof(float)) : 0;
   L.mask = stage ? take(pl.mask_floats * sizeof(float)) : 0;
@@ -284,7 +287,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(base + L.tiles, pl.tiles.data(), pl.tiles.size() * sizeof(Tile),
                          cudaMemcpyHostToDevice, st);
-  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.bar, 0, 4 * sizeof(unsigned), st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.bar, 0, kBarWords * sizeof(unsigned), st);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.err, 0, sizeof(int), st);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "plan upload");
 
@@ -293,6 +296,9 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   P.st = reinterpret_cast<SysState *>(base + L.st);
   P.tiles = reinterpret_cast<const Tile *>(base + L.tiles);
   P.tcount = reinterpret_cast<int *>(base + L.tcount);
+  P.act = reinterpret_cast<int *>(base + L.act);
+  P.claim = reinterpret_cast<unsigned long long *>(base + L.claim);
+  P.arrive = reinterpret_cast<unsigned *>(base + L.arrive);
   P.ntiles = (int)pl.tiles.size();
   P.nsys = nsys;
   P.e0 = reinterpret_cast<float *>(base + L.e0);
@@ -365,7 +371,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   }
   if (kerr != KERR_NONE)
     return fail(ctx, PT_TIMEOUT, kerr == KERR_DEADLINE ? "solve exceeded its wall budget"
-                                                       : "grid barrier wait gave up");
+                                                       : "wait for work gave up (no progress)");
 
   // ---- reports
   for (uint32_t i = 0; i < n; ++i) {
