@@ -25,6 +25,24 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 
 __device__ __forceinline__ int ld_vol(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
+// Asynchronous global -> shared copies (Ampere+ cp.async). `in == false` copies
+// no bytes and zero-fills the destination.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src, bool in) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem_src),
+               "r"(in ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src, bool in) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(gmem_src),
+               "r"(in ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Deterministic block sum: fixed xor-butterfly inside each warp, then warps in
 // index order. The total is valid in thread 0. Uses sred[0 .. blockDim.x/32).
 __device__ __forceinline__ double block_sum(double v, double *sred) {
@@ -60,7 +78,7 @@ struct Geo {
   static constexpr size_t kSmem = (size_t)2 * PLANE * sizeof(float)   // e
                                   + (size_t)2 * PLANE * sizeof(float) // g
                                   + (size_t)2 * PLANE                 // cell
-                                  + 64 * sizeof(double);              // reduction scratch
+                                  + kWarps * sizeof(double);          // reduction scratch
 };
 
 // ----------------------------------------------------------------------------
@@ -283,26 +301,23 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
   const float *__restrict__ ein = cur ? P.e1 : P.e0;
   float *__restrict__ eout = cur ? P.e0 : P.e1;
 
-  // ---- load tile + halo (16-byte vectors; outside the image reads as boundary 0)
+  // ---- load tile + halo straight into shared memory with cp.async (L2 only:
+  // other blocks wrote these planes). Outside the image the copy reads nothing
+  // and zero-fills, which is exactly a boundary cell (e = 0, g = 0, cell = 0).
   constexpr int V = kPWL / 4;
   for (int k = tid; k < 2 * G::LH * V; k += kThreads) {
     const int c = k / (G::LH * V);
     const int r = k - c * (G::LH * V);
     const int ly = r / V, v = r - ly * V;
     const int gy = Y0 + ly, gi = gi0 + 4 * v;
-    float4 ev = make_float4(0.f, 0.f, 0.f, 0.f), gv = ev;
-    uint32_t cv = 0;
-    if (gy >= 0 && gy < d.H && gi >= 0 && gi < d.pw) {
-      const long long o = plane_index(d, c, gy, gi);
-      ev = __ldcg(reinterpret_cast<const float4 *>(ein + o));
-      gv = __ldcg(reinterpret_cast<const float4 *>(P.g + o));
-      cv = __ldg(reinterpret_cast<const uint32_t *>(P.cell + o));
-    }
+    const bool in = gy >= 0 && gy < d.H && gi >= 0 && gi < d.pw;
+    const long long o = in ? plane_index(d, c, gy, gi) : d.off;  // a valid address either way
     const int so = c * G::PLANE + ly * kPWL + 4 * v;
-    *reinterpret_cast<float4 *>(sE + so) = ev;
-    *reinterpret_cast<float4 *>(sG + so) = gv;
-    *reinterpret_cast<uint32_t *>(sC + so) = cv;
+    cp_async16(sE + so, ein + o, in);
+    cp_async16(sG + so, P.g + o, in);
+    cp_async4(sC + so, P.cell + o, in);
   }
+  cp_async_wait_all();
   __syncthreads();
 
   const int pl = Y0 & 1;  // colour parity of loaded row 0 (column 0 is even)
@@ -310,12 +325,17 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
   const double dd = 4.0 + d.lambda;
   constexpr int OX0 = G::HX, OX1 = G::HX + G::TW;  // owned loaded columns
   constexpr int OY0 = G::H, OY1 = G::H + TH;       // owned loaded rows
-  constexpr int RW = kPWL / 2;                      // float2 per plane row (one per lane)
-  // Each lane owns the aligned pair of plane indices (2 lane, 2 lane + 1) of a
-  // row; a warp owns whole rows. The residual of a state is assembled from the
-  // passes that already hold its values: black cells' residual of state j right
-  // after their update in sweep j, red cells' residual of state j just before
-  // their update in sweep j+1 (or in a last pass after the final sweep).
+  constexpr int RQ = kPWL / 4;                      // float4 per plane row (16 lanes)
+  static_assert((G::LH - 2) % 32 == 0, "rows 1..LH-2 must split evenly over the warps");
+  static_assert(TH % 4 == 0, "owned rows come in groups of four");
+  constexpr int kRowPairs = (G::LH - 2) / 2;
+  // Each lane owns four consecutive plane entries (four cells of one colour) of
+  // a row; the two half-warps take rows two apart, so both rows of a warp have
+  // the same colour parity. Every half-sweep relaxes all rows 1..LH-2 and all
+  // columns: cells outside the window that a whole-grid sweep would reproduce
+  // get values nobody reads (they never reach the owned region before the tile
+  // is written back), which keeps the work of every warp identical.
+  const int hw = lane >> 4, l16 = lane & 15;
   double acc[S];
 #pragma unroll
   for (int j = 0; j < S; ++j) acc[j] = 0.0;
@@ -331,37 +351,43 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
     if (j >= s) break;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int tt = 2 * j + h + 1;  // half-sweep number: valid window shrinks by tt
-      float2 *Ec = reinterpret_cast<float2 *>(sE + h * G::PLANE);
-      const float2 *Eo = reinterpret_cast<const float2 *>(sE + (1 - h) * G::PLANE);
-      const float2 *Gc = reinterpret_cast<const float2 *>(sG + h * G::PLANE);
-      const uint16_t *Cc = reinterpret_cast<const uint16_t *>(sC + h * G::PLANE);
-      const int yhi = G::LH - 1 - tt;
-      const int xlo = G::XOFF + tt, xhi = kLW - 1 - G::XOFF - tt;
+      float4 *Ec = reinterpret_cast<float4 *>(sE + h * G::PLANE);
+      const float4 *Eo = reinterpret_cast<const float4 *>(sE + (1 - h) * G::PLANE);
+      const float4 *Gc = reinterpret_cast<const float4 *>(sG + h * G::PLANE);
+      const uint32_t *Cc = reinterpret_cast<const uint32_t *>(sC + h * G::PLANE);
       const bool duty = (h == 1) || (j > 0);  // residual of black state j / red state j-1
       double part = 0.0;
-      for (int ly = tt + warp; ly <= yhi; ly += kWarps) {
-        const int q = (h + ly + pl) & 1;
-        const int r2 = ly * RW + lane;
-        const float2 up = Eo[r2 - RW], dn = Eo[r2 + RW], ct = Eo[r2];
-        const float2 gc = Gc[r2];
-        const float2 ec = Ec[r2];
-        const unsigned cc = Cc[r2];
-        const float far = q ? __shfl_down_sync(0xffffffffu, ct.x, 1)
-                            : __shfl_up_sync(0xffffffffu, ct.y, 1);
-        const float l0 = q ? ct.x : far, r0 = q ? ct.y : ct.x;
-        const float l1 = q ? ct.y : ct.x, r1 = q ? far : ct.y;
-        const int x0 = 4 * lane + q, x1 = x0 + 2;  // loaded columns of the pair
-        const bool a0 = (cc & 0xffu) && x0 >= xlo && x0 <= xhi;
-        const bool a1 = (cc & 0xff00u) && x1 >= xlo && x1 <= xhi;
-        float n0 = ec.x, n1 = ec.y;
-        if (a0) n0 = fmaf(w, (((l0 + r0) + up.x) + dn.x - gc.x) * inv - ec.x, ec.x);
-        if (a1) n1 = fmaf(w, (((l1 + r1) + up.y) + dn.y - gc.y) * inv - ec.y, ec.y);
-        if (duty && ly >= OY0 && ly < OY1) {
-          if (a0 && x0 >= OX0 && x0 < OX1) part += resid(l0, r0, up.x, dn.x, h ? n0 : ec.x, gc.x);
-          if (a1 && x1 >= OX0 && x1 < OX1) part += resid(l1, r1, up.y, dn.y, h ? n1 : ec.y, gc.y);
+      for (int rp = warp; rp < kRowPairs; rp += kWarps) {
+        const int base = 1 + 4 * (rp >> 1) + (rp & 1);
+        const int ly = base + 2 * hw;
+        const int q = (h + base + pl) & 1;  // same for both rows of the warp
+        const int r4 = ly * RQ + l16;
+        const float4 up = Eo[r4 - RQ], dn = Eo[r4 + RQ], ct = Eo[r4];
+        const float4 gc = Gc[r4];
+        const float4 ec = Ec[r4];
+        const uint32_t cc = Cc[r4];
+        const float prev = __shfl_up_sync(0xffffffffu, ct.w, 1, 16);
+        const float next = __shfl_down_sync(0xffffffffu, ct.x, 1, 16);
+        float L0, R0, L1, R1, L2, R2, L3, R3;
+        if (q == 0) {
+          L0 = prev; R0 = ct.x; L1 = ct.x; R1 = ct.y; L2 = ct.y; R2 = ct.z; L3 = ct.z; R3 = ct.w;
+        } else {
+          L0 = ct.x; R0 = ct.y; L1 = ct.y; R1 = ct.z; L2 = ct.z; R2 = ct.w; L3 = ct.w; R3 = next;
         }
-        Ec[r2] = make_float2(n0, n1);
+        float4 ne = ec;
+        if (cc & 0xffu) ne.x = fmaf(w, ((((L0 + R0) + up.x) + dn.x) - gc.x) * inv - ec.x, ec.x);
+        if (cc & 0xff00u) ne.y = fmaf(w, ((((L1 + R1) + up.y) + dn.y) - gc.y) * inv - ec.y, ec.y);
+        if (cc & 0xff0000u) ne.z = fmaf(w, ((((L2 + R2) + up.z) + dn.z) - gc.z) * inv - ec.z, ec.z);
+        if (cc & 0xff000000u) ne.w = fmaf(w, ((((L3 + R3) + up.w) + dn.w) - gc.w) * inv - ec.w, ec.w);
+        if (duty && ly >= OY0 && ly < OY1) {
+          const int x0 = 8 * l16 + q;  // loaded column of the lane's first cell
+          const float4 ee = h ? ne : ec;  // black: state j after its update; red: state j-1
+          if ((cc & 0xffu) && x0 >= OX0 && x0 < OX1) part += resid(L0, R0, up.x, dn.x, ee.x, gc.x);
+          if ((cc & 0xff00u) && x0 + 2 >= OX0 && x0 + 2 < OX1) part += resid(L1, R1, up.y, dn.y, ee.y, gc.y);
+          if ((cc & 0xff0000u) && x0 + 4 >= OX0 && x0 + 4 < OX1) part += resid(L2, R2, up.z, dn.z, ee.z, gc.z);
+          if ((cc & 0xff000000u) && x0 + 6 >= OX0 && x0 + 6 < OX1) part += resid(L3, R3, up.w, dn.w, ee.w, gc.w);
+        }
+        Ec[r4] = ne;
       }
       if (h == 1) acc[j] += part;
       else if (j > 0) acc[j - 1] += part;
@@ -370,24 +396,32 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
   }
   // red cells' residual of the final state
   {
-    const float2 *Er = reinterpret_cast<const float2 *>(sE);
-    const float2 *Eb = reinterpret_cast<const float2 *>(sE + G::PLANE);
-    const float2 *Gr = reinterpret_cast<const float2 *>(sG);
-    const uint16_t *Cr = reinterpret_cast<const uint16_t *>(sC);
+    const float4 *Er = reinterpret_cast<const float4 *>(sE);
+    const float4 *Eb = reinterpret_cast<const float4 *>(sE + G::PLANE);
+    const float4 *Gr = reinterpret_cast<const float4 *>(sG);
+    const uint32_t *Cr = reinterpret_cast<const uint32_t *>(sC);
     double part = 0.0;
-    for (int ly = OY0 + warp; ly < OY1; ly += kWarps) {
-      const int q = (ly + pl) & 1;
-      const int r2 = ly * RW + lane;
-      const float2 up = Eb[r2 - RW], dn = Eb[r2 + RW], ct = Eb[r2];
-      const float2 gc = Gr[r2], ec = Er[r2];
-      const unsigned cc = Cr[r2];
-      const float far = q ? __shfl_down_sync(0xffffffffu, ct.x, 1)
-                          : __shfl_up_sync(0xffffffffu, ct.y, 1);
-      const float l0 = q ? ct.x : far, r0 = q ? ct.y : ct.x;
-      const float l1 = q ? ct.y : ct.x, r1 = q ? far : ct.y;
-      const int x0 = 4 * lane + q, x1 = x0 + 2;
-      if ((cc & 0xffu) && x0 >= OX0 && x0 < OX1) part += resid(l0, r0, up.x, dn.x, ec.x, gc.x);
-      if ((cc & 0xff00u) && x1 >= OX0 && x1 < OX1) part += resid(l1, r1, up.y, dn.y, ec.y, gc.y);
+    for (int rp = warp; rp < TH / 2; rp += kWarps) {
+      const int base = OY0 + 4 * (rp >> 1) + (rp & 1);
+      const int ly = base + 2 * hw;
+      const int q = (base + pl) & 1;
+      const int r4 = ly * RQ + l16;
+      const float4 up = Eb[r4 - RQ], dn = Eb[r4 + RQ], ct = Eb[r4];
+      const float4 gc = Gr[r4], ec = Er[r4];
+      const uint32_t cc = Cr[r4];
+      const float prev = __shfl_up_sync(0xffffffffu, ct.w, 1, 16);
+      const float next = __shfl_down_sync(0xffffffffu, ct.x, 1, 16);
+      float L0, R0, L1, R1, L2, R2, L3, R3;
+      if (q == 0) {
+        L0 = prev; R0 = ct.x; L1 = ct.x; R1 = ct.y; L2 = ct.y; R2 = ct.z; L3 = ct.z; R3 = ct.w;
+      } else {
+        L0 = ct.x; R0 = ct.y; L1 = ct.y; R1 = ct.z; L2 = ct.z; R2 = ct.w; L3 = ct.w; R3 = next;
+      }
+      const int x0 = 8 * l16 + q;
+      if ((cc & 0xffu) && x0 >= OX0 && x0 < OX1) part += resid(L0, R0, up.x, dn.x, ec.x, gc.x);
+      if ((cc & 0xff00u) && x0 + 2 >= OX0 && x0 + 2 < OX1) part += resid(L1, R1, up.y, dn.y, ec.y, gc.y);
+      if ((cc & 0xff0000u) && x0 + 4 >= OX0 && x0 + 4 < OX1) part += resid(L2, R2, up.z, dn.z, ec.z, gc.z);
+      if ((cc & 0xff000000u) && x0 + 6 >= OX0 && x0 + 6 < OX1) part += resid(L3, R3, up.w, dn.w, ec.w, gc.w);
     }
 #pragma unroll
     for (int j = 0; j < S; ++j)
@@ -726,23 +760,27 @@ static cudaError_t launch_solve_t(const KParams &P, int sms, cudaStream_t stream
   return cudaGetLastError();
 }
 
-int tile_config_count() { return 4; }
+int tile_config_count() { return 5; }
 
+// (sweeps per step S, owned tile height TH); every loaded height TH + 2(2S+1)
+// leaves rows 1..LH-2 a multiple of 32.
 TileConfig tile_config(int idx) {
   switch (idx) {
-    case 0: return {1, 64, tile_w(1)};
-    case 1: return {2, 64, tile_w(2)};
-    case 2: return {3, 64, tile_w(3)};
-    default: return {3, 32, tile_w(3)};
+    case 0: return {1, 60, tile_w(1)};
+    case 1: return {2, 88, tile_w(2)};
+    case 2: return {3, 84, tile_w(3)};
+    case 3: return {3, 52, tile_w(3)};
+    default: return {4, 80, tile_w(4)};
   }
 }
 
 size_t tile_config_smem(int idx) {
   switch (idx) {
-    case 0: return Geo<1, 64>::kSmem;
-    case 1: return Geo<2, 64>::kSmem;
-    case 2: return Geo<3, 64>::kSmem;
-    default: return Geo<3, 32>::kSmem;
+    case 0: return Geo<1, 60>::kSmem;
+    case 1: return Geo<2, 88>::kSmem;
+    case 2: return Geo<3, 84>::kSmem;
+    case 3: return Geo<3, 52>::kSmem;
+    default: return Geo<4, 80>::kSmem;
   }
 }
 
@@ -757,10 +795,11 @@ cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t
 
 cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid) {
   switch (cfg) {
-    case 0: return launch_solve_t<1, 64>(P, sms, stream, grid);
-    case 1: return launch_solve_t<2, 64>(P, sms, stream, grid);
-    case 2: return launch_solve_t<3, 64>(P, sms, stream, grid);
-    default: return launch_solve_t<3, 32>(P, sms, stream, grid);
+    case 0: return launch_solve_t<1, 60>(P, sms, stream, grid);
+    case 1: return launch_solve_t<2, 88>(P, sms, stream, grid);
+    case 2: return launch_solve_t<3, 84>(P, sms, stream, grid);
+    case 3: return launch_solve_t<3, 52>(P, sms, stream, grid);
+    default: return launch_solve_t<4, 80>(P, sms, stream, grid);
   }
 }
 
