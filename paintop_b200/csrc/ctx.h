@@ -23,11 +23,16 @@ struct pt_ctx {
   double last_solve_ms = 0.0;  // persistent kernel, CUDA events on `stream`
   double last_call_ms = 0.0;   // whole call from first upload to last download
   long long last_launches = 0; // kernels launched by the last call
+  bool graphs = true;          // capture device-pointer solves into a CUDA graph
+  cudaGraphExec_t gexec = nullptr;
+  std::string gkey;            // the plan the cached graph was captured for
 
   bool reserve(size_t bytes) {
     if (bytes <= arena_cap) return true;
     if (arena) {
       cudaStreamSynchronize(stream);
+      if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }  // it points into the arena
+      gkey.clear();
       cudaFree(arena);
       arena = nullptr;
       arena_cap = 0;
@@ -48,6 +53,8 @@ struct pt_ctx {
   }
 
   void release() {
+    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+    gkey.clear();
     for (auto &e : ev)
       if (e) { cudaEventDestroy(e); e = nullptr; }
     if (arena) cudaFree(arena);

@@ -100,7 +100,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   const long long ntiles = tps * C;
   const long long plane = (long long)H * pw;
   const long long cells = 2 * plane * C;
-  size_t o = 0, sys_o, st_o, claim_o, arrive_o, tiles_o, tc_o, act_o, e0_o, e1_o, g_o, cell_o, u_o, bp_o, part_o, fpart_o,
+  size_t o = 0, sys_o, st_o, claim_o, arrive_o, tiles_o, tc_o, tbox_o, act_o, e0_o, e1_o, g_o, cell_o, u_o, bp_o, part_o, fpart_o,
          hist_o, bar_o, err_o;
   auto take = [&](size_t bytes) { size_t r = o; o = aup(o + (bytes ? bytes : 1)); return r; };
   sys_o = take(C * sizeof(SysDesc));
@@ -109,6 +109,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   arrive_o = take(C * sizeof(unsigned));
   tiles_o = take(ntiles * sizeof(Tile));
   tc_o = take(ntiles * sizeof(int));
+  tbox_o = take(ntiles * sizeof(int4));
   act_o = take(ntiles * sizeof(int));
   e0_o = take(cells * sizeof(float));
   e1_o = take(cells * sizeof(float));
@@ -124,6 +125,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   if (o > (size_t)PT_NOALLOC_SCRATCH_BYTES) return PT_OOM;  // does not fit the fixed array
 
   std::lock_guard<std::mutex> lock(g_mu);
+  cudaGetLastError();  // an earlier, unrelated runtime error must not fail this call's checks
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PT_NO_DEVICE;
   if (!g_scratch_dev[dev]) {
@@ -162,6 +164,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   P.st = reinterpret_cast<SysState *>(base + st_o);
   P.tiles = reinterpret_cast<const Tile *>(base + tiles_o);
   P.tcount = reinterpret_cast<int *>(base + tc_o);
+  P.tbox = reinterpret_cast<int4 *>(base + tbox_o);
   P.act = reinterpret_cast<int *>(base + act_o);
   P.claim = reinterpret_cast<unsigned long long *>(base + claim_o);
   P.arrive = reinterpret_cast<unsigned *>(base + arrive_o);
@@ -217,7 +220,7 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
     r.tolerance = p->tolerance;
     r.final_residual = s.last;
     r.history_len = r.iterations;
-    r.omega_used = descs[c].omega;
+    r.omega_used = s.omega;
     r.refinements = (uint32_t)s.refinements;
     r.channel = (int)c;
     r.initial_residual = s.r0;

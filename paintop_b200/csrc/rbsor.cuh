@@ -96,7 +96,7 @@ struct SysDesc {
   const float *mask;       // coverage mask (W*H)
   float *out;              // interleaved candidate (W*H*C)
   long long hist_off;      // offset of this system's history
-  float omega, inv_denom;  // SOR factor, 1 / (4 + lambda) in f32
+  float omega, inv_denom;  // SOR factor (negative: choose it on device), 1 / (4 + lambda)
   double lambda;
   double tol;
   int max_it;
@@ -109,6 +109,7 @@ struct SysState {
   int isince, nact, out_anchor, steps;
   int pad0, pad1;
   double r0, outer, best, ibest, last, ibase;
+  double omega;            // the SOR factor the sweeps use (chosen on device when automatic)
 };
 
 // Control words of the persistent kernel: [2] systems done. The host zeroes
@@ -127,6 +128,7 @@ struct KParams {
   SysState *st;
   const Tile *tiles;
   int *tcount;             // interior cells per tile
+  int4 *tbox;              // per tile: interior bounding box (min x, min y, max x, max y)
   int ntiles, nsys;
   float *e0, *e1, *g;
   uint8_t *cell;

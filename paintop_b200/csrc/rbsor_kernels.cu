@@ -90,24 +90,35 @@ __device__ __forceinline__ bool interior_at(const SysDesc &d, int x, int y) {
   return d.mask[(long long)y * d.W + x] > 0.5f;           // poisson.rs:349 (strict >)
 }
 
-// Interior cells per tile (owned region only).
+// Interior cells per tile (owned region only) and their bounding box. min/max
+// are order-independent, so the box is deterministic.
 __global__ void k_tile_count(KParams P, int TW, int TH) {
   const Tile tl = P.tiles[blockIdx.x];
   const SysDesc d = P.sys[tl.sys];
-  int n = 0;
+  __shared__ int s[32];
+  __shared__ int sb[4];
+  if (threadIdx.x < 4) sb[threadIdx.x] = (threadIdx.x < 2) ? 0x7fffffff : -1;
+  __syncthreads();
+  int n = 0, x0m = 0x7fffffff, y0m = 0x7fffffff, x1m = -1, y1m = -1;
   const int x0 = tl.tx * TW, y0 = tl.ty * TH;
   for (int k = threadIdx.x; k < TW * TH; k += blockDim.x) {
     const int x = x0 + k % TW, y = y0 + k / TW;
-    if (x < d.W && y < d.H && interior_at(d, x, y)) ++n;
+    if (x < d.W && y < d.H && interior_at(d, x, y)) {
+      ++n;
+      x0m = min(x0m, x); y0m = min(y0m, y); x1m = max(x1m, x); y1m = max(y1m, y);
+    }
   }
-  __shared__ int s[32];
   for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
   if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = n;
+  if (x1m >= 0) {
+    atomicMin(&sb[0], x0m); atomicMin(&sb[1], y0m); atomicMax(&sb[2], x1m); atomicMax(&sb[3], y1m);
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     int t = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
     P.tcount[blockIdx.x] = t;
+    P.tbox[blockIdx.x] = make_int4(sb[0], sb[1], sb[2], sb[3]);
   }
 }
 
@@ -220,6 +231,29 @@ __global__ void k_init(KParams P) {
   s.pad0 = 0; s.pad1 = 0;
   s.r0 = sqrt(sa); s.outer = sqrt(su);
   s.best = INFINITY; s.ibest = INFINITY; s.last = 1.0; s.ibase = s.outer;
+  s.omega = d.omega;
+  if (d.omega < 0.0f) {
+    // automatic SOR factor: Young's optimum for red-black SOR with the Jacobi
+    // spectral radius of (4+lambda)I - N on the region's bounding box (a x b
+    // cells including the boundary ring): (2cos(pi/a) + 2cos(pi/b)) / (4+lambda)
+    int bx0 = 0x7fffffff, by0 = 0x7fffffff, bx1 = -1, by1 = -1;
+    for (int k = 0; k < d.ntiles; ++k) {
+      const int t = d.tile0 + k;
+      if (P.tcount[t] == 0) continue;
+      const int4 b = P.tbox[t];
+      bx0 = min(bx0, b.x); by0 = min(by0, b.y); bx1 = max(bx1, b.z); by1 = max(by1, b.w);
+    }
+    double om = 1.0;
+    if (bx1 >= 0) {
+      const double a = (double)(bx1 - bx0 + 2), b = (double)(by1 - by0 + 2);
+      const double pi = 3.141592653589793;
+      double rho = (2.0 * cos(pi / a) + 2.0 * cos(pi / b)) / (4.0 + d.lambda);
+      rho = fmin(fmax(rho, 0.0), 1.0 - 1e-15);
+      om = 2.0 / (1.0 + sqrt(1.0 - rho * rho));
+    }
+    s.omega = om;
+    const_cast<SysDesc *>(P.sys)[sys].omega = (float)om;
+  }
   // poisson.rs:172-189: no unknowns or a satisfied system -> 0 iterations, converged.
   if (n == 0 || s.r0 == 0.0) {
     s.mode = M_DONE; s.status = STOP_CONVERGED; s.last = 0.0; s.out_anchor = 1;
@@ -740,7 +774,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
 // launch entry points (host)
 // ----------------------------------------------------------------------------
 template <int S, int TH>
-static cudaError_t launch_solve_t(const KParams &P, int sms, cudaStream_t stream, int *grid_out) {
+static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
   using G = Geo<S, TH>;
   cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)G::kSmem);
@@ -752,6 +786,12 @@ static cudaError_t launch_solve_t(const KParams &P, int sms, cudaStream_t stream
   int grid = per_sm * sms;
   if (grid > P.ntiles) grid = P.ntiles > 0 ? P.ntiles : 1;
   *grid_out = grid;
+  return cudaSuccess;
+}
+
+template <int S, int TH>
+static cudaError_t launch_prepared_t(const KParams &P, int grid, cudaStream_t stream) {
+  using G = Geo<S, TH>;
   KParams Pc = P;
   Pc.S = S;
   // No block waits for a particular other block (work is claimed, never
@@ -793,14 +833,30 @@ cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t
   return cudaGetLastError();
 }
 
-cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid) {
+cudaError_t prepare_solve(const KParams &P, int cfg, int sms, int *grid) {
   switch (cfg) {
-    case 0: return launch_solve_t<1, 60>(P, sms, stream, grid);
-    case 1: return launch_solve_t<2, 88>(P, sms, stream, grid);
-    case 2: return launch_solve_t<3, 84>(P, sms, stream, grid);
-    case 3: return launch_solve_t<3, 52>(P, sms, stream, grid);
-    default: return launch_solve_t<4, 80>(P, sms, stream, grid);
+    case 0: return prepare_solve_t<1, 60>(P, sms, grid);
+    case 1: return prepare_solve_t<2, 88>(P, sms, grid);
+    case 2: return prepare_solve_t<3, 84>(P, sms, grid);
+    case 3: return prepare_solve_t<3, 52>(P, sms, grid);
+    default: return prepare_solve_t<4, 80>(P, sms, grid);
   }
+}
+
+cudaError_t launch_prepared(const KParams &P, int cfg, int grid, cudaStream_t stream) {
+  switch (cfg) {
+    case 0: return launch_prepared_t<1, 60>(P, grid, stream);
+    case 1: return launch_prepared_t<2, 88>(P, grid, stream);
+    case 2: return launch_prepared_t<3, 84>(P, grid, stream);
+    case 3: return launch_prepared_t<3, 52>(P, grid, stream);
+    default: return launch_prepared_t<4, 80>(P, grid, stream);
+  }
+}
+
+cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid) {
+  cudaError_t e = prepare_solve(P, cfg, sms, grid);
+  if (e != cudaSuccess) return e;
+  return launch_prepared(P, cfg, *grid, stream);
 }
 
 cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,

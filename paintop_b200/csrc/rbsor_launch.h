@@ -18,8 +18,12 @@ size_t tile_config_smem(int idx);
 
 // k_tile_count + k_assemble + k_init on the stream.
 cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream);
-// The persistent cooperative solve; *grid receives the block count used.
+// The persistent solve; *grid receives the block count used.
 cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid);
+// The same in two halves: set the kernel's attributes and size its grid (not a
+// stream operation, so it stays outside a stream capture), then launch.
+cudaError_t prepare_solve(const KParams &P, int cfg, int sms, int *grid);
+cudaError_t launch_prepared(const KParams &P, int cfg, int grid, cudaStream_t stream);
 // Interleave one image's channels sys0 .. sys0+C-1 into its output.
 cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,
                         cudaStream_t stream);

@@ -75,35 +75,6 @@ pt_status validate(pt_ctx *ctx, const pt_problem &p) {
   return PT_OK;
 }
 
-// Red-black SOR optimum for the discrete operator of a region: the Jacobi
-// spectral radius of (4+lambda)I - N is (4 - mu_min)/(4 + lambda) with mu_min the
-// smallest Dirichlet eigenvalue of the 5-point Laplacian on the region; for a
-// region spanning a box of a x b cells mu_min ~ pi^2 (1/a^2 + 1/b^2) (a
-// rectangle's value; other shapes of that extent are close to it). Young's
-// formula then gives omega = 2 / (1 + sqrt(1 - rho^2)).
-double auto_omega(double lambda, double a, double b) {
-  a = std::max(a, 1.0);
-  b = std::max(b, 1.0);
-  const double pi2 = 9.869604401089358;
-  const double mu = pi2 * (1.0 / (a * a) + 1.0 / (b * b));
-  const double rho = std::min(std::max((4.0 - mu) / (4.0 + lambda), 0.0), 1.0 - 1e-15);
-  return 2.0 / (1.0 + std::sqrt(1.0 - rho * rho));
-}
-
-// Span of the interior cells of a mask (host side, for PT_FLAG_OMEGA_AUTO).
-void interior_span(const pt_problem &p, double *a, double *b) {
-  long long x0 = p.width, x1 = -1, y0 = p.height, y1 = -1;
-  if (p.width >= 3 && p.height >= 3)
-    for (uint32_t y = 1; y + 1 < p.height; ++y)
-      for (uint32_t x = 1; x + 1 < p.width; ++x)
-        if (p.mask[(size_t)y * p.width + x] > 0.5f) {
-          x0 = std::min<long long>(x0, x); x1 = std::max<long long>(x1, x);
-          y0 = std::min<long long>(y0, y); y1 = std::max<long long>(y1, y);
-        }
-  *a = x1 >= x0 ? double(x1 - x0 + 2) : 1.0;
-  *b = y1 >= y0 ? double(y1 - y0 + 2) : 1.0;
-}
-
 struct Plan {
   int cfg;
   TileConfig tc;
@@ -118,7 +89,7 @@ struct Plan {
 
 // Arena layout (byte offsets) for one call.
 struct Layout {
-  size_t sys, st, claim, arrive, tiles, tcount, act, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in,
+  size_t sys, st, claim, arrive, tiles, tcount, tbox, act, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in,
       mask, out, total;
 };
 
@@ -133,6 +104,7 @@ Layout layout(const Plan &pl, bool stage) {
   L.arrive = take(ns * sizeof(unsigned));
   L.tiles = take(nt * sizeof(Tile));
   L.tcount = take(nt * sizeof(int));
+  L.tbox = take(nt * sizeof(int4));
   L.act = take(nt * sizeof(int));
   L.e0 = take(pl.cells * sizeof(float));
   L.e1 = take(pl.cells * sizeof(float));
@@ -190,13 +162,8 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     const int W = (int)p.width, H = (int)p.height, C = (int)p.channels;
     const int pw = (int)align_up((size_t)(W + 1) / 2, 4);
     const int ntx = (W + pl.tc.tw - 1) / pl.tc.tw, nty = (H + pl.tc.th - 1) / pl.tc.th;
-    double omega = p.omega;
-    if (p.flags & PT_FLAG_OMEGA_AUTO) {
-      double a = 1, b = 1;
-      if (!devptr) interior_span(p, &a, &b);
-      else { a = W; b = H; }
-      omega = auto_omega(p.lambda, a, b);
-    }
+    // automatic omega is chosen on the device from the region's extent
+    const double omega = (p.flags & PT_FLAG_OMEGA_AUTO) ? -1.0 : p.omega;
     const long long img = (long long)W * H;
     for (int c = 0; c < C; ++c) {
       SysDesc d{};
@@ -287,8 +254,6 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(base + L.tiles, pl.tiles.data(), pl.tiles.size() * sizeof(Tile),
                          cudaMemcpyHostToDevice, st);
-  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.bar, 0, kBarWords * sizeof(unsigned), st);
-  if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.err, 0, sizeof(int), st);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "plan upload");
 
   KParams P{};
@@ -296,6 +261,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   P.st = reinterpret_cast<SysState *>(base + L.st);
   P.tiles = reinterpret_cast<const Tile *>(base + L.tiles);
   P.tcount = reinterpret_cast<int *>(base + L.tcount);
+  P.tbox = reinterpret_cast<int4 *>(base + L.tbox);
   P.act = reinterpret_cast<int *>(base + L.act);
   P.claim = reinterpret_cast<unsigned long long *>(base + L.claim);
   P.arrive = reinterpret_cast<unsigned *>(base + L.arrive);
@@ -315,21 +281,68 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   P.budget_ns = (unsigned long long)(ctx->budget_s * 1e9);
   P.S = pl.tc.S;
 
-  ce = launch_assembly(P, pl.tc, st);
-  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "assembly launch");
   int grid = 0;
-  cudaEventRecord(ctx->ev[1], st);
-  ce = launch_solve(P, pl.cfg, ctx->sms, st, &grid);
-  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "solve launch");
-  cudaEventRecord(ctx->ev[2], st);
-  long long launches = 4;  // tile count, assembly, init, solve
+  ce = prepare_solve(P, pl.cfg, ctx->sms, &grid);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "solve prepare");
   ctx->last_grid = grid;
   ctx->last_cfg = pl.cfg;
-  for (uint32_t i = 0; i < n; ++i) {
-    if (ps[i].channels == 0) continue;
-    ce = launch_emit(P, sys0[i], pl.tc, (long long)ps[i].width * ps[i].height, st);
-    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "emit launch");
-    ++launches;
+  long long launches = 5;  // tile count, compaction, assembly, init, solve
+  for (uint32_t i = 0; i < n; ++i) launches += ps[i].channels > 0 ? 1 : 0;  // emits
+
+  // Everything from here to the results is stream work on the device: with
+  // device pointers it is captured once into a CUDA graph and replayed while
+  // the plan (descriptors, pointers, arena, configuration) stays the same.
+  auto record = [&](cudaEvent_t ev, bool capturing) {
+    // inside a capture an external record node still times the launch; the
+    // flag is only valid while capturing
+    return capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
+  };
+  auto enqueue = [&](bool capturing) -> cudaError_t {
+    cudaError_t e = cudaMemsetAsync(base + L.bar, 0, kBarWords * sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + L.err, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = launch_assembly(P, pl.tc, st);
+    if (e == cudaSuccess) e = record(ctx->ev[1], capturing);
+    if (e == cudaSuccess) e = launch_prepared(P, pl.cfg, grid, st);
+    if (e == cudaSuccess) e = record(ctx->ev[2], capturing);
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i)
+      if (ps[i].channels > 0)
+        e = launch_emit(P, sys0[i], pl.tc, (long long)ps[i].width * ps[i].height, st);
+    if (devptr && histories)
+      for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) {
+        if (!histories[i] || !ps[i].max_iterations) continue;
+        for (uint32_t c = 0; c < ps[i].channels && e == cudaSuccess; ++c)
+          e = cudaMemcpyAsync(histories[i] + (size_t)c * ps[i].max_iterations,
+                              reinterpret_cast<double *>(base + L.hist) + pl.sys[sys0[i] + c].hist_off,
+                              ps[i].max_iterations * sizeof(double), cudaMemcpyDeviceToDevice, st);
+      }
+    return e;
+  };
+  if (devptr && ctx->graphs) {
+    std::string key(reinterpret_cast<const char *>(pl.sys.data()), pl.sys.size() * sizeof(SysDesc));
+    const long long extra[6] = {pl.cfg, grid, (long long)(uintptr_t)base, (long long)L.total,
+                                (long long)pl.tiles.size(), (long long)(histories != nullptr)};
+    key.append(reinterpret_cast<const char *>(extra), sizeof(extra));
+    if (histories)
+      for (uint32_t i = 0; i < n; ++i) key.append(reinterpret_cast<const char *>(&histories[i]), sizeof(void *));
+    if (!ctx->gexec || key != ctx->gkey) {
+      if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+      cudaGraph_t g = nullptr;
+      ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+      if (ce == cudaSuccess) {
+        const cudaError_t e1 = enqueue(true);
+        ce = cudaStreamEndCapture(st, &g);
+        if (e1 != cudaSuccess) ce = e1;
+      }
+      if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ctx->gexec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (ce != cudaSuccess) { ctx->gexec = nullptr; return cuda_fail(ctx, ce, "graph capture"); }
+      ctx->gkey = key;
+    }
+    ce = cudaGraphLaunch(ctx->gexec, st);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "graph launch");
+  } else {
+    ce = enqueue(false);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "launch");
   }
 
   // ---- download
@@ -344,7 +357,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       ce = cudaMemcpyAsync(outs[i], pl.sys[sys0[i]].out, nf * sizeof(float), cudaMemcpyDeviceToHost, st);
     }
   }
-  if (histories && ce == cudaSuccess) {
+  if (histories && !devptr && ce == cudaSuccess) {
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
       if (!histories[i]) continue;
       for (uint32_t c = 0; c < ps[i].channels && ce == cudaSuccess; ++c) {
@@ -353,7 +366,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
         if (!cnt) continue;
         ce = cudaMemcpyAsync(histories[i] + (size_t)c * cnt,
                              reinterpret_cast<double *>(base + L.hist) + d.hist_off, cnt * sizeof(double),
-                             devptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st);
+                             cudaMemcpyDeviceToHost, st);
       }
     }
   }
@@ -363,8 +376,9 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "stream synchronize");
   {
     float a = 0.f, b = 0.f;
-    cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
-    cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+    if (cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]) != cudaSuccess) a = -1.f;
+    if (cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]) != cudaSuccess) b = -1.f;
+    cudaGetLastError();  // a failed timing query must not leak into later error checks
     ctx->last_solve_ms = a;
     ctx->last_call_ms = b;
     ctx->last_launches = launches;
@@ -386,7 +400,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       r.tolerance = p.tolerance;
       r.final_residual = s.last;
       r.history_len = r.iterations;
-      r.omega_used = pl.sys[sys0[i] + c].omega;
+      r.omega_used = s.omega;
       r.refinements = (uint32_t)s.refinements;
       r.channel = (int)c;
       r.initial_residual = s.r0;
@@ -433,6 +447,7 @@ pt_status pt_ctx_create(int device, pt_ctx **out) {
   if (!c) return PT_OOM;
   c->device = device;
   c->sms = prop.multiProcessorCount;
+  if (const char *g = std::getenv("PAINTOP_CUDA_GRAPHS")) c->graphs = std::strcmp(g, "0") != 0;
   e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {

@@ -361,3 +361,49 @@ def test_screened_star_512_within_bounded_tier(ctx, oracle):
     ref, rworst, _ = oracle.blend_channels(src, tgt, mask, 4, 512, 512, 2000, 1e-6, 0.01, 1.8)
     d = out.astype(np.float64) - ref
     assert np.abs(d).max() <= BOUNDED_MAX_ABS and np.sqrt(np.mean(d ** 2)) <= BOUNDED_RMS
+
+
+# ---- automatic omega, device pointers and graph replay --------------------------------
+
+def test_auto_omega_converges_faster_on_pure_poisson(ctx):
+    w, h, c = 300, 220, 1
+    src, tgt, mask = random_problem(41, w, h, c)
+    _, fixed, _ = ctx.solve(src, tgt, mask, w, h, c, max_iterations=20000, tolerance=1e-6,
+                            omega=1.8)
+    from paintop_b200 import _lib
+    out, auto, _ = ctx.solve(src, tgt, mask, w, h, c, max_iterations=20000, tolerance=1e-6,
+                             flags=_lib.PT_FLAG_OMEGA_AUTO)
+    assert 1.8 < auto[0]["omega_used"] < 2.0
+    assert auto[0]["converged"] and auto[0]["iterations"] < fixed[0]["iterations"]
+
+
+def test_device_pointers_graph_replay_matches_host_path(ctx):
+    import torch
+    from paintop_b200 import _lib
+    import ctypes as C
+    dev = torch.device("cuda", 0)
+    w, h, ch = 333, 201, 3
+    L = _lib.lib()
+    outs = []
+    for seed in (60, 60, 61, 60):  # replay, replay, new inputs (recapture), back again
+        src, tgt, mask = random_problem(seed, w, h, ch)
+        ref, rper, _ = ctx.solve(src, tgt, mask, w, h, ch, lam=0.02, max_iterations=800,
+                                 tolerance=1e-8)
+        ds, dt, dm = (torch.from_numpy(a).to(dev) for a in (src, tgt, mask))
+        out = torch.empty(w * h * ch, device=dev)
+        hist = torch.zeros(ch * 800, dtype=torch.float64, device=dev)
+        p = _lib.PtProblem(w, h, ch, ds.data_ptr(), dt.data_ptr(), dm.data_ptr(), 0.02, 800, 1e-8,
+                           1.8, _lib.PT_FLAG_DEVICE_POINTERS, None)
+        reps = (_lib.PtReport * (ch + 1))()
+        for _ in range(2):
+            assert L.pt_poisson_solve(ctx.h, C.byref(p), out.data_ptr(), reps,
+                                      hist.data_ptr()) == _lib.PT_OK
+            got = out.cpu().numpy()
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+            hh = hist.cpu().numpy()
+            for k in range(ch):
+                n = reps[k].history_len
+                assert n == rper[k]["iterations"]
+                assert hh[k * 800: k * 800 + n].tolist() == rper[k]["residual_history"]
+        outs.append(got)
+    assert np.array_equal(outs[0], outs[3])
