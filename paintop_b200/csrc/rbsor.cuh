@@ -110,6 +110,8 @@ struct SysState {
   int pad0, pad1;
   double r0, outer, best, ibest, last, ibase;
   double omega;            // the SOR factor the sweeps use (chosen on device when automatic)
+  int stall_window;        // sweeps without a new best that end the solve as stalled
+  int pad2;
 };
 
 // Control words of the persistent kernel: [2] systems done. The host zeroes

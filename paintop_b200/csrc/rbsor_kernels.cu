@@ -232,6 +232,8 @@ __global__ void k_init(KParams P) {
   s.r0 = sqrt(sa); s.outer = sqrt(su);
   s.best = INFINITY; s.ibest = INFINITY; s.last = 1.0; s.ibase = s.outer;
   s.omega = d.omega;
+  s.stall_window = (int)kStallWindow;  // poisson.rs:80
+  s.pad2 = 0;
   if (d.omega < 0.0f) {
     // automatic SOR factor: Young's optimum for red-black SOR with the Jacobi
     // spectral radius of (4+lambda)I - N on the region's bounding box (a x b
@@ -253,6 +255,11 @@ __global__ void k_init(KParams P) {
     }
     s.omega = om;
     const_cast<SysDesc *>(P.sys)[sys].omega = (float)om;
+    // Near the optimum the residual norm of red-black SOR rises and falls on a
+    // time scale of 1/(2 - omega) sweeps (its asymptotic decay time) before it
+    // settles; a window of twice that many sweeps keeps the stall rule a test
+    // for lost progress rather than for that transient.
+    s.stall_window = max((int)kStallWindow, (int)ceil(2.0 / fmax(2.0 - om, 1e-6)));
   }
   // poisson.rs:172-189: no unknowns or a satisfied system -> 0 iterations, converged.
   if (n == 0 || s.r0 == 0.0) {
@@ -541,13 +548,13 @@ __device__ void resid_tile(const KParams &P, const SysDesc &d, int t, const Tile
 }
 
 __device__ __forceinline__ void apply_stall(SysState &s, double rel, int &done) {
-  // poisson.rs:219-228
+  // poisson.rs:219-228 (window 16 for a given omega; see k_init for automatic omega)
   if (rel < s.best * (1.0 - kStallImprovement)) {
     s.best = rel;
     s.since = 0;
   } else {
     s.since += 1;
-    if ((unsigned)s.since >= kStallWindow) done = 1;
+    if (s.since >= s.stall_window) done = 1;
   }
 }
 
