@@ -248,6 +248,58 @@ pt_status pt_autotune(pt_ctx *ctx, const pt_problem *ps, uint32_t n, uint32_t re
 pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_candidate, pt_report *reports,
                                    double *history, void *stream);
 
+/* ---- learned warm start (no counterpart in the reference) ----------------
+ *
+ * A small U-Net (4 levels of 16-32-64-128 channels, two 3x3 convolutions +
+ * ReLU per level, 2x2 average pooling, bilinear x2 upsampling, skip
+ * concatenation, 1x1 head) that predicts a solve's result from four per-pixel
+ * features; its prediction seeds pt_poisson_solve through PT_FLAG_WARM_START.
+ * Convolutions run on the tensor cores in bf16 with fp32 accumulation; the
+ * parameters are fp32 masters trained with Adam (beta1 0.9, beta2 0.999, eps
+ * 1e-8). Training steps are deterministic (fixed-order reductions).
+ * All image buffers of these calls are DEVICE pointers: batch x h x w f32
+ * (features: batch x h x w x 4). h and w must be multiples of 8. Calls on a
+ * network take its context's lock and run on the context's stream. */
+typedef struct pt_unet pt_unet;
+
+/* He-normal initialisation from a SplitMix64 stream seeded with `seed`. */
+pt_status pt_unet_create(pt_ctx *ctx, uint64_t seed, pt_unet **out);
+pt_status pt_unet_destroy(pt_unet *net);
+/* Number of fp32 parameters: per 3x3 layer W[cout][3][3][cin] then b[cout]
+ * (the first layer's cin is 16, of which 4 are real inputs), then the head's
+ * w[16] and b[1]. */
+uint64_t pt_unet_param_count(const pt_unet *net);
+pt_status pt_unet_get_params(pt_unet *net, float *host);
+pt_status pt_unet_set_params(pt_unet *net, const float *host);
+/* Features of single-channel images: 0 the guidance Laplacian at interior
+ * cells (0 elsewhere), 1 anchor - guidance outside the interior (0 inside), 2
+ * the interior mask, 3 the distance to the nearest non-interior cell along the
+ * row and column, divided by 32 and clipped at 1 (0 outside). Interior = mask >
+ * 0.5 and not on the image border (the reference's rule, poisson.rs:86-103).
+ * The network predicts the correction u - guidance (harmonic inside the
+ * interior for Poisson blending, with boundary values feature 1); the warm
+ * start is guidance + prediction. */
+pt_status pt_unet_features(pt_unet *net, const float *guidance, const float *anchor,
+                           const float *mask, uint32_t batch, uint32_t h, uint32_t w,
+                           float *features);
+/* pred = network(features). */
+pt_status pt_unet_forward(pt_unet *net, const float *features, uint32_t batch, uint32_t h,
+                          uint32_t w, float *pred);
+/* The masked mean squared error over pixels with loss_mask > 0.5 and, when
+ * grad_host is not NULL, its gradient with respect to every parameter (host
+ * array of pt_unet_param_count floats). Does not update the parameters. */
+pt_status pt_unet_loss_grad(pt_unet *net, const float *features, const float *target,
+                            const float *loss_mask, uint32_t batch, uint32_t h, uint32_t w,
+                            double *loss, float *grad_host);
+/* One Adam step on the masked mean squared error; *loss receives the loss of
+ * the parameters before the step. */
+pt_status pt_unet_train_step(pt_unet *net, const float *features, const float *target,
+                             const float *loss_mask, uint32_t batch, uint32_t h, uint32_t w,
+                             float lr, double *loss);
+/* Parameters and Adam moments to / from a file (little-endian, versioned). */
+pt_status pt_unet_save(pt_unet *net, const char *path);
+pt_status pt_unet_load(pt_unet *net, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -27,6 +28,9 @@ EXPORTED = (
     "pt_op_compute", "pt_status_str", "pt_ctx_last_error", "pt_tile_config_count",
     "pt_tile_config_info", "pt_ctx_set_config", "pt_ctx_last_config", "pt_autotune",
     "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_poisson_solve_noalloc",
+    "pt_unet_create", "pt_unet_destroy", "pt_unet_param_count", "pt_unet_get_params",
+    "pt_unet_set_params", "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad",
+    "pt_unet_train_step", "pt_unet_save", "pt_unet_load",
 )
 PT_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
@@ -134,6 +138,23 @@ def lib():
     L.pt_ctx_last_timing.restype = C.c_int
     L.pt_poisson_solve_noalloc.argtypes = [C.POINTER(PtProblem), vp, C.POINTER(PtReport), vp, vp]
     L.pt_poisson_solve_noalloc.restype = C.c_int
+    u64, f32 = C.c_uint64, C.c_float
+    L.pt_unet_create.argtypes = [vp, u64, C.POINTER(vp)]
+    L.pt_unet_destroy.argtypes = [vp]
+    L.pt_unet_param_count.argtypes = [vp]
+    L.pt_unet_param_count.restype = u64
+    L.pt_unet_get_params.argtypes = [vp, vp]
+    L.pt_unet_set_params.argtypes = [vp, vp]
+    L.pt_unet_features.argtypes = [vp, vp, vp, vp, u32, u32, u32, vp]
+    L.pt_unet_forward.argtypes = [vp, vp, u32, u32, u32, vp]
+    L.pt_unet_loss_grad.argtypes = [vp, vp, vp, vp, u32, u32, u32, C.POINTER(C.c_double), vp]
+    L.pt_unet_train_step.argtypes = [vp, vp, vp, vp, u32, u32, u32, f32, C.POINTER(C.c_double)]
+    L.pt_unet_save.argtypes = [vp, C.c_char_p]
+    L.pt_unet_load.argtypes = [vp, C.c_char_p]
+    for name in ("pt_unet_create", "pt_unet_destroy", "pt_unet_get_params", "pt_unet_set_params",
+                 "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad", "pt_unet_train_step",
+                 "pt_unet_save", "pt_unet_load"):
+        getattr(L, name).restype = C.c_int
     _lib = L
     return L
 
@@ -162,9 +183,16 @@ class Context:
         if st != PT_OK:
             raise CudaError(st, "pt_ctx_create")
         self.h = h
+        self._children = weakref.WeakSet()  # objects whose C handles point into this context
+
+    def adopt(self, child) -> None:
+        """Register an object with a close() that must run before the context is destroyed."""
+        self._children.add(child)
 
     def close(self):
         if getattr(self, "h", None):
+            for child in list(self._children):
+                child.close()
             lib().pt_ctx_destroy(self.h)
             self.h = None
 

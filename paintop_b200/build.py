@@ -21,7 +21,8 @@ LIB = os.path.join(HERE, "libpaintop_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                    "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["rbsor_kernels.cu", "solver_host.cu", "op_host.cpp", "autotune.cpp", "noalloc.cu"]
+SOURCES = ["rbsor_kernels.cu", "solver_host.cu", "op_host.cpp", "autotune.cpp", "noalloc.cu",
+           "unet/unet_kernels.cu", "unet/unet.cu"]
 
 
 def nvcc() -> str:
@@ -40,13 +41,14 @@ def _stale(obj: str, deps: list[str]) -> bool:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers = [os.path.join(d, f) for d in (CSRC, os.path.join(CSRC, "unet")) for f in os.listdir(d)
+               if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "paintop_cuda.h"))
     objs = []
     changed = force
     for src in SOURCES:
         path = os.path.join(CSRC, src)
-        obj = os.path.join(OBJ, src + ".o")
+        obj = os.path.join(OBJ, src.replace("/", "_") + ".o")
         objs.append(obj)
         if force or verbose or _stale(obj, [path] + headers):
             cmd = [nvcc()] + CU_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", path, "-o", obj]

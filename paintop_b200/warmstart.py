@@ -1,0 +1,341 @@
+"""Learned warm start for the Poisson solve: a small U-Net behind ``pt_unet_*``.
+
+The network (``csrc/unet``) runs and trains on the GPU through the library's
+own tensor-core kernels; PyTorch only holds device buffers and generates the
+seeded synthetic training images on the device (the same distributions as
+:mod:`paintop_b200.synth`). Training data are solves of the plain method
+itself: each 256x256 instance is solved by the library's red-black SOR to a
+relative residual of 1e-7 and the network learns to predict the correction
+u - g (solution minus guidance) from four per-pixel features
+(``pt_unet_features``). For Poisson blending that correction is harmonic in
+the interior with boundary values anchor - g, so it is smooth where g is not.
+
+At inference the guess seeds ``pt_poisson_solve`` through PT_FLAG_WARM_START;
+SOR with FP64 refinement then drives the solve to the same tolerance, measured
+against the same anchor-based normalisation as the plain solve. For images
+larger than the training size the problem is pooled by an integer factor, the
+network predicts the coarse correction, and the guess is the fine guidance plus
+the upsampled correction, so the fine detail of g is kept and only the smooth
+part comes from the network.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+PT_OK = 0
+
+
+def _torch():
+    import torch  # device buffers only
+    return torch
+
+
+def _dptr(t) -> int:
+    assert t.is_cuda and t.is_contiguous() and t.dtype == _torch().float32, (t.device, t.dtype)
+    return t.data_ptr()
+
+
+class UNet:
+    """A network on one library context. Buffers are float32 CUDA tensors."""
+
+    def __init__(self, ctx: "_lib.Context", seed: int = 0):
+        self.ctx = ctx
+        h = C.c_void_p()
+        st = _lib.lib().pt_unet_create(ctx.h, C.c_uint64(seed), C.byref(h))
+        if st != PT_OK:
+            raise _lib.CudaError(st, ctx.last_error())
+        self.h = h
+        ctx.adopt(self)
+
+    def close(self):
+        """Free the network; the context closes its networks before itself."""
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
+            _lib.lib().pt_unet_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != PT_OK:
+            raise _lib.CudaError(st, f"{what}: {self.ctx.last_error()}")
+
+    @property
+    def param_count(self) -> int:
+        return int(_lib.lib().pt_unet_param_count(self.h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.param_count, dtype=np.float32)
+        self._check(_lib.lib().pt_unet_get_params(self.h, out.ctypes.data), "get_params")
+        return out
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.param_count
+        self._check(_lib.lib().pt_unet_set_params(self.h, p.ctypes.data), "set_params")
+
+    def save(self, path: str) -> None:
+        self._check(_lib.lib().pt_unet_save(self.h, os.fsencode(path)), "save")
+
+    def load(self, path: str) -> None:
+        self._check(_lib.lib().pt_unet_load(self.h, os.fsencode(path)), "load")
+
+    def features(self, guidance, anchor, mask):
+        """(B, H, W) float32 CUDA tensors -> (B, H, W, 4) features."""
+        torch = _torch()
+        B, H, W = guidance.shape
+        f = torch.empty((B, H, W, 4), device=guidance.device, dtype=torch.float32)
+        torch.cuda.synchronize()
+        self._check(_lib.lib().pt_unet_features(self.h, _dptr(guidance), _dptr(anchor), _dptr(mask),
+                                                B, H, W, _dptr(f)), "features")
+        return f
+
+    def forward(self, feats):
+        torch = _torch()
+        B, H, W, _ = feats.shape
+        pred = torch.empty((B, H, W), device=feats.device, dtype=torch.float32)
+        torch.cuda.synchronize()
+        self._check(_lib.lib().pt_unet_forward(self.h, _dptr(feats), B, H, W, _dptr(pred)), "forward")
+        return pred
+
+    def loss_grad(self, feats, target, loss_mask, want_grad=True):
+        B, H, W, _ = feats.shape
+        loss = C.c_double()
+        g = np.empty(self.param_count, dtype=np.float32) if want_grad else None
+        _torch().cuda.synchronize()
+        self._check(_lib.lib().pt_unet_loss_grad(self.h, _dptr(feats), _dptr(target), _dptr(loss_mask),
+                                                 B, H, W, C.byref(loss),
+                                                 g.ctypes.data if g is not None else None), "loss_grad")
+        return loss.value, g
+
+    def train_step(self, feats, target, loss_mask, lr: float = 1e-3) -> float:
+        B, H, W, _ = feats.shape
+        loss = C.c_double()
+        _torch().cuda.synchronize()
+        self._check(_lib.lib().pt_unet_train_step(self.h, _dptr(feats), _dptr(target), _dptr(loss_mask),
+                                                  B, H, W, C.c_float(lr), C.byref(loss)), "train_step")
+        return loss.value
+
+
+# ---------------------------------------------------------------------------
+# seeded synthetic training instances on the device
+# ---------------------------------------------------------------------------
+def _sinusoids(gen, rng: np.random.Generator, B: int, size: int, device):
+    """B single-channel images of 8 random sinusoids + 0.5 + N(0, 0.02^2), clamped."""
+    torch = _torch()
+    f = rng.uniform(1.0, 16.0, (B, 8))
+    th = rng.uniform(0.0, 2 * math.pi, (B, 8))
+    ph = rng.uniform(0.0, 2 * math.pi, (B, 8))
+    a = rng.uniform(0.05, 0.2, (B, 8))
+    kx = torch.tensor(2 * math.pi * f * np.cos(th), device=device, dtype=torch.float32)
+    ky = torch.tensor(2 * math.pi * f * np.sin(th), device=device, dtype=torch.float32)
+    ph = torch.tensor(ph, device=device, dtype=torch.float32)
+    a = torch.tensor(a, device=device, dtype=torch.float32)
+    c = (torch.arange(size, device=device, dtype=torch.float32) + 0.5) / size
+    x = c.view(1, 1, 1, size)
+    y = c.view(1, 1, size, 1)
+    arg = kx.view(B, 8, 1, 1) * x + ky.view(B, 8, 1, 1) * y + ph.view(B, 8, 1, 1)
+    img = 0.5 + (a.view(B, 8, 1, 1) * torch.sin(arg)).sum(1)
+    img = img + 0.02 * torch.randn((B, size, size), generator=gen, device=device)
+    return img.clamp_(0.0, 1.0).contiguous()
+
+
+def _masks(rng: np.random.Generator, B: int, size: int, device):
+    """Random ellipse (pixel-centre test) or blob polygon (4x4 supersampled,
+    nonzero rule) masks, as in synth.train_instance."""
+    torch = _torch()
+    out = torch.empty((B, size, size), device=device, dtype=torch.float32)
+    c = torch.arange(size, device=device, dtype=torch.float64) + 0.5
+    S = 4
+    sub = (torch.arange(size * S, device=device, dtype=torch.float64) + 0.5) / S
+    for b in range(B):
+        if rng.uniform() < 0.5:
+            rx, ry = rng.uniform(0.15, 0.4) * size, rng.uniform(0.15, 0.4) * size
+            cx = size / 2 + rng.uniform(-0.08, 0.08) * size
+            cy = size / 2 + rng.uniform(-0.08, 0.08) * size
+            ang = rng.uniform(0, math.pi)
+            X = c.view(1, -1) - cx
+            Y = c.view(-1, 1) - cy
+            u = X * math.cos(ang) + Y * math.sin(ang)
+            v = -X * math.sin(ang) + Y * math.cos(ang)
+            out[b] = ((u / rx) ** 2 + (v / ry) ** 2 <= 1.0).float()
+        else:
+            nv = int(rng.integers(5, 13))
+            mean_r = rng.uniform(0.2, 0.38) * size
+            angles = np.sort(rng.uniform(0, 2 * math.pi, nv))
+            radii = mean_r * (1.0 + rng.uniform(-0.25, 0.25, nv))
+            px = size / 2 + radii * np.cos(angles)
+            py = size / 2 + radii * np.sin(angles)
+            X = sub.view(1, -1)
+            Y = sub.view(-1, 1)
+            wind = torch.zeros((size * S, size * S), device=device, dtype=torch.int32)
+            for k in range(nv):
+                ax, ay, bx, by = px[k], py[k], px[(k + 1) % nv], py[(k + 1) % nv]
+                straddle = (ay <= Y) != (by <= Y)
+                if ay == by:
+                    continue
+                xc = ax + (Y - ay) * (bx - ax) / (by - ay)
+                d = 1 if by > ay else -1
+                wind += (straddle & (xc > X)).int() * d
+            cov = (wind != 0).float().view(size, S, size, S).sum((1, 3)) / (S * S)
+            out[b] = cov
+    return out
+
+
+def make_instances(n: int, size: int = 256, seed: int = 0, device="cuda"):
+    """n seeded training instances: (guidance, anchor, mask), each (n, size, size)."""
+    torch = _torch()
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    g = _sinusoids(gen, rng, n, size, device)
+    a = _sinusoids(gen, rng, n, size, device)
+    m = _masks(rng, n, size, device)
+    return g, a, m
+
+
+def solve_batch_device(ctx, guidance, anchor, mask, *, tol=1e-7, max_iterations=100000,
+                       omega_auto=True, omega=1.8, guess=None):
+    """Solve B single-channel Poisson-blend problems held in device tensors with
+    one pt_poisson_solve_batch call. Returns (out (B, H, W), reports)."""
+    torch = _torch()
+    B, H, W = guidance.shape
+    out = torch.empty_like(guidance)
+    arr = (_lib.PtProblem * B)()
+    outs = (C.c_void_p * B)()
+    reps = [(_lib.PtReport * 2)() for _ in range(B)]
+    rep_ptrs = (C.POINTER(_lib.PtReport) * B)()
+    flags = _lib.PT_FLAG_DEVICE_POINTERS | (_lib.PT_FLAG_OMEGA_AUTO if omega_auto else 0)
+    img = H * W * 4
+    for i in range(B):
+        arr[i] = _lib.PtProblem(W, H, 1, guidance.data_ptr() + i * img, anchor.data_ptr() + i * img,
+                                mask.data_ptr() + i * img, 0.0, max_iterations, tol, omega,
+                                flags | (_lib.PT_FLAG_WARM_START if guess is not None else 0),
+                                (guess.data_ptr() + i * img) if guess is not None else None)
+        outs[i] = out.data_ptr() + i * img
+        rep_ptrs[i] = C.cast(reps[i], C.POINTER(_lib.PtReport))
+    torch.cuda.synchronize()
+    st = _lib.lib().pt_poisson_solve_batch(ctx.h, arr, B, outs, rep_ptrs, None)
+    if st != PT_OK:
+        raise _lib.CudaError(st, ctx.last_error())
+    return out, [r[1].as_dict() for r in reps]
+
+
+def interior_mask(mask):
+    """mask > 0.5 away from the image border (the solver's interior rule)."""
+    m = (mask > 0.5).float()
+    m[:, 0, :] = 0
+    m[:, -1, :] = 0
+    m[:, :, 0] = 0
+    m[:, :, -1] = 0
+    return m.contiguous()
+
+
+@dataclass
+class Dataset:
+    guidance: object
+    anchor: object
+    mask: object
+    solution: object
+    sweeps: np.ndarray
+    gen_s: float
+    solve_s: float
+
+
+def build_dataset(ctx, n: int = 20000, size: int = 256, seed: int = 0, chunk: int = 512,
+                  tol: float = 1e-7) -> Dataset:
+    """Generate and solve n training instances on the device (solves by the plain method)."""
+    torch = _torch()
+    gs, an, ms, us, sw = [], [], [], [], []
+    t_gen = t_solve = 0.0
+    for c0 in range(0, n, chunk):
+        k = min(chunk, n - c0)
+        t0 = time.perf_counter()
+        g, a, m = make_instances(k, size, seed * 1000003 + c0)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        u, reps = solve_batch_device(ctx, g, a, m, tol=tol)
+        t2 = time.perf_counter()
+        t_gen += t1 - t0
+        t_solve += t2 - t1
+        gs.append(g); an.append(a); ms.append(m); us.append(u)
+        sw += [r["iterations"] for r in reps]
+        bad = [r for r in reps if not r["converged"]]
+        if bad:
+            raise RuntimeError(f"{len(bad)} training solves did not converge: {bad[0]}")
+    return Dataset(torch.cat(gs), torch.cat(an), torch.cat(ms), torch.cat(us), np.asarray(sw),
+                   t_gen, t_solve)
+
+
+def train(net: UNet, data: Dataset, *, epochs: int = 4, batch: int = 64, lr: float = 1e-3,
+          seed: int = 0, log=None, max_steps=None):
+    """Adam on the masked L2 loss over interior pixels; returns the per-step losses
+    and the device time of the training steps."""
+    torch = _torch()
+    n = data.guidance.shape[0]
+    rng = np.random.default_rng(seed)
+    losses = []
+    step_s = 0.0
+    steps = 0
+    for ep in range(epochs):
+        order = rng.permutation(n)
+        for b0 in range(0, n - batch + 1, batch):
+            idx = torch.as_tensor(order[b0:b0 + batch], device=data.guidance.device)
+            g = data.guidance[idx].contiguous()
+            a = data.anchor[idx].contiguous()
+            m = data.mask[idx].contiguous()
+            u = (data.solution[idx] - g).contiguous()  # the correction u - g
+            f = net.features(g, a, m)
+            lm = interior_mask(m)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            losses.append(net.train_step(f, u, lm, lr))
+            torch.cuda.synchronize()
+            step_s += time.perf_counter() - t0
+            steps += 1
+            if log and steps % 50 == 0:
+                log(f"epoch {ep} step {steps} loss {np.mean(losses[-50:]):.3e}")
+            if max_steps and steps >= max_steps:
+                return np.asarray(losses), step_s
+    return np.asarray(losses), step_s
+
+
+def train_flops_per_pixel() -> float:
+    """Algorithmic FLOPs of one training step per input pixel: forward, backward-data
+    and backward-weights of every 3x3 convolution (2 FLOPs per multiply-add, padded
+    channel counts as executed; the first layer has no backward-data)."""
+    from_level = [0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0]
+    layers = [(16, 16), (16, 16), (32, 16), (32, 32), (64, 32), (64, 64), (128, 64), (128, 128),
+              (64, 192), (64, 64), (32, 96), (32, 32), (16, 48), (16, 16)]
+    total = 0.0
+    for l, ((co, ci), lev) in enumerate(zip(layers, from_level)):
+        mac = 9.0 * co * ci / (4 ** lev)
+        total += 2 * mac * (3 if l > 0 else 2)
+    return total
+
+
+def predict_guess(net: UNet, guidance, anchor, mask, scale: int = 1):
+    """Warm-start guess for single-channel problems (B, H, W): guidance + the
+    predicted correction. With scale > 1 the network runs on the problem pooled
+    by `scale` (area average) and its correction is upsampled bilinearly."""
+    torch = _torch()
+    import torch.nn.functional as F  # resampling of the guess only (not the solve)
+    if scale == 1:
+        return (guidance + net.forward(net.features(guidance, anchor, mask))).contiguous()
+    G = F.avg_pool2d(guidance[:, None], scale)[:, 0].contiguous()
+    A = F.avg_pool2d(anchor[:, None], scale)[:, 0].contiguous()
+    M = F.avg_pool2d(mask[:, None], scale)[:, 0].contiguous()
+    corr = net.forward(net.features(G, A, M))
+    corr = F.interpolate(corr[:, None], scale_factor=scale, mode="bilinear", align_corners=False)[:, 0]
+    return (guidance + corr).contiguous()
