@@ -100,6 +100,9 @@ typedef struct pt_report {
   uint32_t refinements; /* FP64 residual-correction steps (incl. the final check) */
   int32_t channel;      /* the channel index (for the worst entry: which channel) */
   double initial_residual; /* ||r(anchor)||, the FP64 normaliser of every relative residual */
+  int32_t warm_start;   /* 1: the sweeps started from initial_guess; 0: from the anchor
+                           (no guess, or a guess whose FP64 residual norm was not below
+                           ||r(anchor)||, which falls back to the plain start) */
 } pt_report;
 
 pt_status pt_ctx_create(int device, pt_ctx **out);
@@ -296,6 +299,17 @@ pt_status pt_unet_loss_grad(pt_unet *net, const float *features, const float *ta
 pt_status pt_unet_train_step(pt_unet *net, const float *features, const float *target,
                              const float *loss_mask, uint32_t batch, uint32_t h, uint32_t w,
                              float lr, double *loss);
+/* The warm start of one pt_poisson_solve problem (device pointers; images
+ * width x height x channels interleaved, mask width x height): every channel
+ * is pooled by `scale` (area average, 1 = full resolution), the network
+ * predicts each channel's correction at that resolution, and
+ *   guess = guidance + bilinear upsampling of the correction
+ * is written to `guess` (width x height x channels), ready for
+ * PT_FLAG_WARM_START. Pooling brings large regions to the size the network was
+ * trained on (its receptive field is about 100 pixels). */
+pt_status pt_unet_guess(pt_unet *net, const float *guidance, const float *anchor,
+                        const float *mask, uint32_t width, uint32_t height, uint32_t channels,
+                        uint32_t scale, float *guess);
 /* Parameters and Adam moments to / from a file (little-endian, versioned). */
 pt_status pt_unet_save(pt_unet *net, const char *path);
 pt_status pt_unet_load(pt_unet *net, const char *path);

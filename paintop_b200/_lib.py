@@ -30,7 +30,7 @@ EXPORTED = (
     "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_poisson_solve_noalloc",
     "pt_unet_create", "pt_unet_destroy", "pt_unet_param_count", "pt_unet_get_params",
     "pt_unet_set_params", "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad",
-    "pt_unet_train_step", "pt_unet_save", "pt_unet_load",
+    "pt_unet_train_step", "pt_unet_save", "pt_unet_load", "pt_unet_guess",
 )
 PT_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
@@ -50,7 +50,7 @@ class PtReport(C.Structure):
         ("iterations", C.c_uint32), ("converged", C.c_int32), ("stop_reason", C.c_int32),
         ("tolerance", C.c_double), ("final_residual", C.c_double), ("history_len", C.c_uint32),
         ("omega_used", C.c_double), ("refinements", C.c_uint32), ("channel", C.c_int32),
-        ("initial_residual", C.c_double),
+        ("initial_residual", C.c_double), ("warm_start", C.c_int32),
     ]
 
     def as_dict(self, history=None):
@@ -59,7 +59,8 @@ class PtReport(C.Structure):
                  tolerance=float(self.tolerance), final_residual=float(self.final_residual),
                  history_len=int(self.history_len), omega_used=float(self.omega_used),
                  refinements=int(self.refinements), channel=int(self.channel),
-                 initial_residual=float(self.initial_residual))
+                 initial_residual=float(self.initial_residual),
+                 warm_start=bool(self.warm_start))
         if history is not None:
             d["residual_history"] = history
         return d
@@ -149,11 +150,12 @@ def lib():
     L.pt_unet_forward.argtypes = [vp, vp, u32, u32, u32, vp]
     L.pt_unet_loss_grad.argtypes = [vp, vp, vp, vp, u32, u32, u32, C.POINTER(C.c_double), vp]
     L.pt_unet_train_step.argtypes = [vp, vp, vp, vp, u32, u32, u32, f32, C.POINTER(C.c_double)]
+    L.pt_unet_guess.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, vp]
     L.pt_unet_save.argtypes = [vp, C.c_char_p]
     L.pt_unet_load.argtypes = [vp, C.c_char_p]
     for name in ("pt_unet_create", "pt_unet_destroy", "pt_unet_get_params", "pt_unet_set_params",
                  "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad", "pt_unet_train_step",
-                 "pt_unet_save", "pt_unet_load"):
+                 "pt_unet_save", "pt_unet_load", "pt_unet_guess"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

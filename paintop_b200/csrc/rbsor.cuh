@@ -107,7 +107,8 @@ struct SysState {
   int mode, s, iterations, cur;
   int pending, status, refinements, since;
   int isince, nact, out_anchor, steps;
-  int pad0, pad1;
+  int warm_used;           // 1: the sweeps start from the caller's guess
+  int pad1;
   double r0, outer, best, ibest, last, ibase;
   double omega;            // the SOR factor the sweeps use (chosen on device when automatic)
   int stall_window;        // sweeps without a new best that end the solve as stalled

@@ -132,6 +132,15 @@ __device__ __forceinline__ bool tile_support(const KParams &P, const SysDesc &d,
   return false;
 }
 
+// r(anchor) at an interior pixel: (4 + lambda) a - (sum of the four anchor
+// neighbours) against b' (poisson.rs:315-321), in this operand order.
+__device__ __forceinline__ double anchor_residual(const SysDesc &d, long long px, double a, double bp) {
+  const int C = d.C, ch = d.chan;
+  const double na = (((double)d.tgt[(px - 1) * C + ch] + (double)d.tgt[(px + 1) * C + ch]) +
+                     (double)d.tgt[(px - d.W) * C + ch]) + (double)d.tgt[(px + d.W) * C + ch];
+  return fma(d.lambda + 4.0, -a, na) - bp;
+}
+
 // Assemble one tile of one system (owned cells only). Writes cell, bp, u, g and
 // zeroes e0/e1; accumulates ||r(anchor)||^2 and ||r(u_init)||^2 partials.
 // Arithmetic of b and r follows poisson.rs:364-373 (guidance_laplacian) and
@@ -173,9 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_assemble(KParams P, int TW, int TH
                        (double)d.src[pu * C + ch]) + (double)d.src[pd * C + ch];
     const double b = fma(4.0, -sc, ns);
     const double bp = fma(lam, -a, b);
-    const double na = (((double)d.tgt[pl * C + ch] + (double)d.tgt[pr * C + ch]) +
-                       (double)d.tgt[pu * C + ch]) + (double)d.tgt[pd * C + ch];
-    const double ra = fma(lam + 4.0, -a, na) - bp;
+    const double ra = anchor_residual(d, px, a, bp);
     acc_a = fma(ra, ra, acc_a);
     double uc = a, ru = ra;
     if (d.warm) {
@@ -228,8 +235,14 @@ __global__ void k_init(KParams P) {
   s.mode = M_SWEEP; s.s = 0; s.iterations = 0; s.cur = 0;
   s.pending = P_NONE; s.status = -1; s.refinements = 0; s.since = 0;
   s.isince = 0; s.nact = n; s.out_anchor = 0; s.steps = 0;
-  s.pad0 = 0; s.pad1 = 0;
+  s.warm_used = 0; s.pad1 = 0;
   s.r0 = sqrt(sa); s.outer = sqrt(su);
+  if (d.warm) {
+    // The plain start is the fallback: a guess whose residual is not below the
+    // anchor's (or not finite) is replaced by the anchor (k_warm_fallback).
+    if (s.outer < s.r0) s.warm_used = 1;
+    else s.outer = s.r0;
+  }
   s.best = INFINITY; s.ibest = INFINITY; s.last = 1.0; s.ibase = s.outer;
   s.omega = d.omega;
   s.stall_window = (int)kStallWindow;  // poisson.rs:80
@@ -275,6 +288,30 @@ __global__ void k_init(KParams P) {
   P.st[sys] = s;
   P.arrive[sys] = 0;
   P.claim[sys] = s.mode == M_DONE ? (unsigned long long)kClaimDone : 0ull;
+}
+
+// Restore the anchor start (u = anchor, g = -r(anchor), as k_assemble writes
+// without a guess) in the systems whose guess k_init rejected.
+__global__ void __launch_bounds__(kThreads) k_warm_fallback(KParams P, int TW, int TH) {
+  const int t = blockIdx.x;
+  const Tile tl = P.tiles[t];
+  const SysDesc d = P.sys[tl.sys];
+  if (!d.warm || P.st[tl.sys].warm_used || !tile_support(P, d, tl.tx, tl.ty)) return;
+  const int half = TW / 2;
+  for (int k = threadIdx.x; k < 2 * TH * half; k += blockDim.x) {
+    const int c = k / (TH * half);
+    const int r = k - c * (TH * half);
+    const int y = tl.ty * TH + r / half;
+    const int i = tl.tx * half + r % half;
+    if (y >= d.H || i >= d.pw) continue;
+    const int x = 2 * i + ((c + y) & 1);
+    if (x >= d.W || !interior_at(d, x, y)) continue;
+    const long long o = plane_index(d, c, y, i);
+    const long long px = (long long)y * d.W + x;
+    const double a = (double)d.tgt[px * d.C + d.chan];
+    P.u[o] = a;
+    P.g[o] = (float)(-anchor_residual(d, px, a, P.bp[o]));
+  }
 }
 
 // Per system, the tiles with interior cells in index order (one block per
@@ -831,12 +868,13 @@ size_t tile_config_smem(int idx) {
   }
 }
 
-cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream) {
+cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream, bool any_warm) {
   if (P.ntiles <= 0) return cudaSuccess;
   k_tile_count<<<P.ntiles, 256, 0, stream>>>(P, tc.tw, tc.th);
   k_compact<<<P.nsys, 256, 0, stream>>>(P);
   k_assemble<<<P.ntiles, kThreads, 0, stream>>>(P, tc.tw, tc.th);
   k_init<<<P.nsys, 256, 0, stream>>>(P);
+  if (any_warm) k_warm_fallback<<<P.ntiles, kThreads, 0, stream>>>(P, tc.tw, tc.th);
   return cudaGetLastError();
 }
 

@@ -17,7 +17,9 @@ TileConfig tile_config(int idx);
 size_t tile_config_smem(int idx);
 
 // k_tile_count + k_assemble + k_init on the stream.
-cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream);
+// any_warm: some system has PT_FLAG_WARM_START (adds the guess-rejection pass)
+cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream,
+                            bool any_warm = false);
 // The persistent solve; *grid receives the block count used.
 cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream, int *grid);
 // The same in two halves: set the kernel's attributes and size its grid (not a

@@ -297,10 +297,12 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     // flag is only valid while capturing
     return capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
   };
+  bool any_warm = false;
+  for (uint32_t i = 0; i < n; ++i) any_warm |= (ps[i].flags & PT_FLAG_WARM_START) != 0;
   auto enqueue = [&](bool capturing) -> cudaError_t {
     cudaError_t e = cudaMemsetAsync(base + L.bar, 0, kBarWords * sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.err, 0, sizeof(int), st);
-    if (e == cudaSuccess) e = launch_assembly(P, pl.tc, st);
+    if (e == cudaSuccess) e = launch_assembly(P, pl.tc, st, any_warm);
     if (e == cudaSuccess) e = record(ctx->ev[1], capturing);
     if (e == cudaSuccess) e = launch_prepared(P, pl.cfg, grid, st);
     if (e == cudaSuccess) e = record(ctx->ev[2], capturing);
@@ -404,6 +406,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       r.refinements = (uint32_t)s.refinements;
       r.channel = (int)c;
       r.initial_residual = s.r0;
+      r.warm_start = s.warm_used;
       reports[i][c] = r;
       // worse_of (poisson_blend.rs:240-246)
       if (worst < 0) worst = (int)c;

@@ -67,6 +67,8 @@ struct pt_unet {
   float *pred = nullptr, *dpred = nullptr, *wpart = nullptr, *cpart = nullptr, *count = nullptr;
   double *lpart = nullptr;
   int *err = nullptr;
+  float *gmem = nullptr;  // scratch of pt_unet_guess, grown to a high-water mark
+  size_t gmem_bytes = 0;
   std::mutex mu;
 };
 
@@ -382,6 +384,7 @@ pt_status pt_unet_destroy(pt_unet *n) {
     cudaStreamSynchronize(n->ctx->stream);
     cudaFree(n->params); cudaFree(n->m); cudaFree(n->v); cudaFree(n->grad); cudaFree(n->wbf);
     cudaFree(n->act_mem);
+    cudaFree(n->gmem);
   }
   delete n;
   return PT_OK;
@@ -456,6 +459,42 @@ pt_status pt_unet_train_step(pt_unet *n, const float *features, const float *tar
      "adam");
   RET(refresh_weights(n));
   return PT_OK;
+}
+
+pt_status pt_unet_guess(pt_unet *n, const float *guidance, const float *anchor, const float *mask,
+                        uint32_t width, uint32_t height, uint32_t channels, uint32_t scale, float *guess) {
+  if (!n || !guidance || !anchor || !mask || !guess || !width || !height || !channels || !scale)
+    return PT_INVALID_ARG;
+  if (scale > 64 || channels > 64) return PT_INVALID_ARG;
+  const int W = (int)width, H = (int)height, C = (int)channels, s = (int)scale;
+  const int hv = (H + s - 1) / s, wv = (W + s - 1) / s;
+  const int Hc = (std::max(hv, 8) + 7) / 8 * 8, Wc = (std::max(wv, 8) + 7) / 8 * 8;
+  RET(check_shape((uint32_t)C, (uint32_t)Hc, (uint32_t)Wc));
+  std::lock_guard<std::mutex> lock(n->ctx->mu);
+  cudaSetDevice(n->ctx->device);
+  const size_t cells = (size_t)C * Hc * Wc, need = cells * 7 * sizeof(float);
+  if (need > n->gmem_bytes) {
+    cudaFree(n->gmem);
+    n->gmem = nullptr;
+    n->gmem_bytes = 0;
+    if (cudaMalloc(&n->gmem, need) != cudaSuccess) {
+      cudaGetLastError();
+      n->gmem = nullptr;
+      return PT_OOM;
+    }
+    n->gmem_bytes = need;
+  }
+  float *cg = n->gmem, *ca = cg + cells, *cm = ca + cells, *feat = cm + cells;
+  cudaStream_t st = n->ctx->stream;
+  CK(launch_pool_inputs(guidance, anchor, mask, W, H, C, s, Wc, Hc, cg, ca, cm, st), "pool inputs");
+  CK(launch_features(cg, ca, cm, C, Hc, Wc, feat, st), "features");
+  RET(ensure_acts(n, C, Hc, Wc));
+  RET(forward(n, feat));
+  CK(launch_compose_guess(guidance, n->pred, W, H, C, s, Wc, Hc, guess, st), "compose guess");
+  int kerr = 0;
+  CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, st), "err copy");
+  CK(cudaStreamSynchronize(st), "sync");
+  return kerr ? PT_TIMEOUT : PT_OK;
 }
 
 pt_status pt_unet_save(pt_unet *n, const char *path) {

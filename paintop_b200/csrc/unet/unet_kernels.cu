@@ -361,20 +361,45 @@ __global__ void k_colsum_reduce(const float *part, int nparts, int c, float *out
 // ----------------------------------------------------------------------------
 // pooling, upsampling, masks
 // ----------------------------------------------------------------------------
-// 2x2 average pooling: out (H/2 x W/2 x c, ld_out) from in (H x W x c at ldi, off)
+// The elementwise kernels below move 8 channels (16 bytes) per thread: every
+// channel count, pitch and slice offset of the network is a multiple of 8.
+__device__ __forceinline__ void ld8(const __nv_bfloat16 *p, float (&v)[8]) {
+  const uint4 q = *reinterpret_cast<const uint4 *>(p);
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float2 f = __bfloat1622float2(h[j]);
+    v[2 * j] = f.x;
+    v[2 * j + 1] = f.y;
+  }
+}
+__device__ __forceinline__ void st8(__nv_bfloat16 *p, const float (&v)[8]) {
+  uint4 q;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&q);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+  *reinterpret_cast<uint4 *>(p) = q;
+}
+
+// 2x2 average pooling: out (H/2 x W/2 x c at ldo, ooff) from in (H x W x c at ldi, ioff)
 __global__ void k_avgpool2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bfloat16 *out, int ldo, int ooff,
                            int B, int H, int W, int c) {
-  const int Ho = H / 2, Wo = W / 2;
-  const long long total = (long long)B * Ho * Wo * c;
+  const int Ho = H / 2, Wo = W / 2, c8 = c / 8;
+  const long long total = (long long)B * Ho * Wo * c8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    const long long q = i / c;
+    const int ch = (int)(i % c8) * 8;
+    const long long q = i / c8;
     const int x = (int)(q % Wo), y = (int)((q / Wo) % Ho), b = (int)(q / ((long long)Wo * Ho));
     const long long r0 = ((long long)b * H + 2 * y) * W + 2 * x;
-    const float s = bf2f(in[r0 * ldi + ioff + ch]) + bf2f(in[(r0 + 1) * ldi + ioff + ch]) +
-                    bf2f(in[(r0 + W) * ldi + ioff + ch]) + bf2f(in[(r0 + W + 1) * ldi + ioff + ch]);
-    out[q * ldo + ooff + ch] = __float2bfloat16_rn(0.25f * s);
+    float v00[8], v01[8], v10[8], v11[8], o[8];
+    ld8(in + r0 * ldi + ioff + ch, v00);
+    ld8(in + (r0 + 1) * ldi + ioff + ch, v01);
+    ld8(in + (r0 + W) * ldi + ioff + ch, v10);
+    ld8(in + (r0 + W + 1) * ldi + ioff + ch, v11);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) o[j] = 0.25f * (((v00[j] + v01[j]) + v10[j]) + v11[j]);
+    st8(out + q * ldo + ooff + ch, o);
   }
 }
 
@@ -383,16 +408,21 @@ __global__ void k_avgpool2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bflo
 __global__ void k_unpool_add_mask(const __nv_bfloat16 *dskip, int lds, int soff, const __nv_bfloat16 *dpool,
                                   int ldp, int poff, const __nv_bfloat16 *act, int lda, int aoff,
                                   __nv_bfloat16 *out, int ldo, int ooff, int B, int H, int W, int c) {
-  const long long total = (long long)B * H * W * c;
+  const int c8 = c / 8;
+  const long long total = (long long)B * H * W * c8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    const long long q = i / c;
+    const int ch = (int)(i % c8) * 8;
+    const long long q = i / c8;
     const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((long long)W * H));
     const long long pq = ((long long)b * (H / 2) + y / 2) * (W / 2) + x / 2;
-    float g = bf2f(dskip[q * lds + soff + ch]) + 0.25f * bf2f(dpool[pq * ldp + poff + ch]);
-    if (!(bf2f(act[q * lda + aoff + ch]) > 0.0f)) g = 0.0f;
-    out[q * ldo + ooff + ch] = __float2bfloat16_rn(g);
+    float ds[8], dp[8], av[8], o[8];
+    ld8(dskip + q * lds + soff + ch, ds);
+    ld8(dpool + pq * ldp + poff + ch, dp);
+    ld8(act + q * lda + aoff + ch, av);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) o[j] = av[j] > 0.0f ? ds[j] + 0.25f * dp[j] : 0.0f;
+    st8(out + q * ldo + ooff + ch, o);
   }
 }
 
@@ -407,38 +437,45 @@ __device__ __forceinline__ void up_taps(int o, int n, int &i0, int &i1, float &w
 }
 __global__ void k_upsample2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bfloat16 *out, int ldo, int ooff,
                             int B, int Hi, int Wi, int c) {
-  const int Ho = 2 * Hi, Wo = 2 * Wi;
-  const long long total = (long long)B * Ho * Wo * c;
+  const int Ho = 2 * Hi, Wo = 2 * Wi, c8 = c / 8;
+  const long long total = (long long)B * Ho * Wo * c8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    const long long q = i / c;
+    const int ch = (int)(i % c8) * 8;
+    const long long q = i / c8;
     const int x = (int)(q % Wo), y = (int)((q / Wo) % Ho), b = (int)(q / ((long long)Wo * Ho));
     int y0, y1, x0, x1;
     float wy0, wy1, wx0, wx1;
     up_taps(y, Hi, y0, y1, wy0, wy1);
     up_taps(x, Wi, x0, x1, wx0, wx1);
-    auto at = [&](int yy, int xx) { return bf2f(in[(((long long)b * Hi + yy) * Wi + xx) * ldi + ioff + ch]); };
-    const float v = wy0 * (wx0 * at(y0, x0) + wx1 * at(y0, x1)) + wy1 * (wx0 * at(y1, x0) + wx1 * at(y1, x1));
-    out[q * ldo + ooff + ch] = __float2bfloat16_rn(v);
+    const __nv_bfloat16 *base = in + ioff + ch;
+    float a00[8], a01[8], a10[8], a11[8], o[8];
+    ld8(base + (((long long)b * Hi + y0) * Wi + x0) * ldi, a00);
+    ld8(base + (((long long)b * Hi + y0) * Wi + x1) * ldi, a01);
+    ld8(base + (((long long)b * Hi + y1) * Wi + x0) * ldi, a10);
+    ld8(base + (((long long)b * Hi + y1) * Wi + x1) * ldi, a11);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      o[j] = wy0 * (wx0 * a00[j] + wx1 * a01[j]) + wy1 * (wx0 * a10[j] + wx1 * a11[j]);
+    st8(out + q * ldo + ooff + ch, o);
   }
 }
 // Adjoint of k_upsample2 (a gather over the outputs that read each input),
 // times the ReLU mask of the upsampled activation.
 __global__ void k_upsample2_bwd(const __nv_bfloat16 *dout, int ldd, int doff, const __nv_bfloat16 *act, int lda,
                                 int aoff, __nv_bfloat16 *din, int ldo, int ooff, int B, int Hi, int Wi, int c) {
-  const int Ho = 2 * Hi, Wo = 2 * Wi;
-  const long long total = (long long)B * Hi * Wi * c;
+  const int Ho = 2 * Hi, Wo = 2 * Wi, c8 = c / 8;
+  const long long total = (long long)B * Hi * Wi * c8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    const long long q = i / c;
+    const int ch = (int)(i % c8) * 8;
+    const long long q = i / c8;
     const int x = (int)(q % Wi), y = (int)((q / Wi) % Hi), b = (int)(q / ((long long)Wi * Hi));
     // output rows that read input row y: 2y, 2y+1 (weight 0.75), 2y-1 and 2y+2
     // (weight 0.25), plus the clamped border rows
-    float wyv[4];
-    int oy[4];
-    int ny = 0;
+    float wyv[4], wxv[4];
+    int oy[4], ox[4];
+    int ny = 0, nx = 0;
     for (int o = max(2 * y - 1, 0); o <= min(2 * y + 2, Ho - 1); ++o) {
       int i0, i1;
       float w0, w1;
@@ -446,9 +483,6 @@ __global__ void k_upsample2_bwd(const __nv_bfloat16 *dout, int ldd, int doff, co
       const float wgt = (i0 == y ? w0 : 0.0f) + (i1 == y ? w1 : 0.0f);
       if (wgt != 0.0f) { oy[ny] = o; wyv[ny] = wgt; ++ny; }
     }
-    float wxv[4];
-    int ox[4];
-    int nx = 0;
     for (int o = max(2 * x - 1, 0); o <= min(2 * x + 2, Wo - 1); ++o) {
       int i0, i1;
       float w0, w1;
@@ -456,12 +490,19 @@ __global__ void k_upsample2_bwd(const __nv_bfloat16 *dout, int ldd, int doff, co
       const float wgt = (i0 == x ? w0 : 0.0f) + (i1 == x ? w1 : 0.0f);
       if (wgt != 0.0f) { ox[nx] = o; wxv[nx] = wgt; ++nx; }
     }
-    float s = 0.0f;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0}, v[8], av[8];
     for (int a1 = 0; a1 < ny; ++a1)
-      for (int a2 = 0; a2 < nx; ++a2)
-        s += wyv[a1] * wxv[a2] * bf2f(dout[(((long long)b * Ho + oy[a1]) * Wo + ox[a2]) * ldd + doff + ch]);
-    if (!(bf2f(act[q * lda + aoff + ch]) > 0.0f)) s = 0.0f;
-    din[q * ldo + ooff + ch] = __float2bfloat16_rn(s);
+      for (int a2 = 0; a2 < nx; ++a2) {
+        ld8(dout + (((long long)b * Ho + oy[a1]) * Wo + ox[a2]) * ldd + doff + ch, v);
+        const float wgt = wyv[a1] * wxv[a2];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] += wgt * v[j];
+      }
+    ld8(act + q * lda + aoff + ch, av);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (!(av[j] > 0.0f)) s[j] = 0.0f;
+    st8(din + q * ldo + ooff + ch, s);
   }
 }
 
@@ -623,6 +664,61 @@ __global__ void k_features(const float *guid, const float *anchor, const float *
 }
 
 // ----------------------------------------------------------------------------
+// warm-start guess at another resolution
+// ----------------------------------------------------------------------------
+// Pool channel ch of interleaved (H x W x C) guidance and anchor, and the mask,
+// by `s` (area average over the block's in-image pixels) into image ch of a
+// (C x Hc x Wc) batch; coarse cells with no in-image pixel get 0.
+__global__ void k_pool_inputs(const float *g, const float *a, const float *m, int W, int H, int C, int s, int Wc,
+                              int Hc, float *cg, float *ca, float *cm) {
+  const long long total = (long long)C * Hc * Wc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ch = (int)(i / ((long long)Hc * Wc));
+    const int r = (int)(i - (long long)ch * Hc * Wc), cy = r / Wc, cx = r - cy * Wc;
+    const int y0 = cy * s, x0 = cx * s, y1 = min(y0 + s, H), x1 = min(x0 + s, W);
+    float sg = 0.0f, sa = 0.0f, sm = 0.0f;
+    int cnt = 0;
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) {
+        const long long px = (long long)y * W + x;
+        sg += g[px * C + ch];
+        sa += a[px * C + ch];
+        sm += m[px];
+        ++cnt;
+      }
+    const float inv = cnt ? 1.0f / (float)cnt : 0.0f;
+    cg[i] = sg * inv;
+    ca[i] = sa * inv;
+    cm[i] = sm * inv;
+  }
+}
+
+// guess = guidance + the coarse correction upsampled bilinearly (half-pixel
+// centres, clamped to the coarse cells that cover the image).
+__global__ void k_compose_guess(const float *g, const float *corr, int W, int H, int C, int s, int Wc, int Hc,
+                                float *guess) {
+  const int hv = (H + s - 1) / s, wv = (W + s - 1) / s;  // coarse cells that touch the image
+  const long long total = (long long)W * H * C;
+  const float inv = 1.0f / (float)s;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ch = (int)(i % C);
+    const long long px = i / C;
+    const int y = (int)(px / W), x = (int)(px - (long long)y * W);
+    const float fy = fminf(fmaxf(((float)y + 0.5f) * inv - 0.5f, 0.0f), (float)(hv - 1));
+    const float fx = fminf(fmaxf(((float)x + 0.5f) * inv - 0.5f, 0.0f), (float)(wv - 1));
+    const int iy = min((int)fy, hv - 1), ix = min((int)fx, wv - 1);
+    const int jy = min(iy + 1, hv - 1), jx = min(ix + 1, wv - 1);
+    const float wy = fy - (float)iy, wx = fx - (float)ix;
+    const float *c = corr + (long long)ch * Hc * Wc;
+    const float top = c[(long long)iy * Wc + ix] + wx * (c[(long long)iy * Wc + jx] - c[(long long)iy * Wc + ix]);
+    const float bot = c[(long long)jy * Wc + ix] + wx * (c[(long long)jy * Wc + jx] - c[(long long)jy * Wc + ix]);
+    guess[i] = g[i] + (top + wy * (bot - top));
+  }
+}
+
+// ----------------------------------------------------------------------------
 // launchers
 // ----------------------------------------------------------------------------
 template <int N>
@@ -714,7 +810,8 @@ int colsum_parts(long long P) { return (int)((P + kColsumChunk - 1) / kColsumChu
 
 cudaError_t launch_avgpool2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bfloat16 *out, int ldo, int ooff,
                             int B, int H, int W, int c, cudaStream_t st) {
-  k_avgpool2<<<blocks_for((long long)B * H * W * c / 4, 256), 256, 0, st>>>(in, ldi, ioff, out, ldo, ooff, B, H,
+  if (c % 8 || ldi % 8 || ioff % 8 || ldo % 8 || ooff % 8) return cudaErrorInvalidValue;
+  k_avgpool2<<<blocks_for((long long)B * H * W * c / 32, 256), 256, 0, st>>>(in, ldi, ioff, out, ldo, ooff, B, H,
                                                                            W, c);
   return cudaGetLastError();
 }
@@ -722,20 +819,24 @@ cudaError_t launch_unpool_add_mask(const __nv_bfloat16 *dskip, int lds, int soff
                                    int ldp, int poff, const __nv_bfloat16 *act, int lda, int aoff,
                                    __nv_bfloat16 *out, int ldo, int ooff, int B, int H, int W, int c,
                                    cudaStream_t st) {
-  k_unpool_add_mask<<<blocks_for((long long)B * H * W * c, 256), 256, 0, st>>>(
+  if (c % 8 || lds % 8 || soff % 8 || ldp % 8 || poff % 8 || lda % 8 || aoff % 8 || ldo % 8 || ooff % 8)
+    return cudaErrorInvalidValue;
+  k_unpool_add_mask<<<blocks_for((long long)B * H * W * c / 8, 256), 256, 0, st>>>(
       dskip, lds, soff, dpool, ldp, poff, act, lda, aoff, out, ldo, ooff, B, H, W, c);
   return cudaGetLastError();
 }
 cudaError_t launch_upsample2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bfloat16 *out, int ldo, int ooff,
                              int B, int Hi, int Wi, int c, cudaStream_t st) {
-  k_upsample2<<<blocks_for((long long)B * Hi * Wi * 4 * c, 256), 256, 0, st>>>(in, ldi, ioff, out, ldo, ooff, B,
+  if (c % 8 || ldi % 8 || ioff % 8 || ldo % 8 || ooff % 8) return cudaErrorInvalidValue;
+  k_upsample2<<<blocks_for((long long)B * Hi * Wi * 4 * c / 8, 256), 256, 0, st>>>(in, ldi, ioff, out, ldo, ooff, B,
                                                                                Hi, Wi, c);
   return cudaGetLastError();
 }
 cudaError_t launch_upsample2_bwd(const __nv_bfloat16 *dout, int ldd, int doff, const __nv_bfloat16 *act, int lda,
                                  int aoff, __nv_bfloat16 *din, int ldo, int ooff, int B, int Hi, int Wi, int c,
                                  cudaStream_t st) {
-  k_upsample2_bwd<<<blocks_for((long long)B * Hi * Wi * c, 256), 256, 0, st>>>(dout, ldd, doff, act, lda, aoff,
+  if (c % 8 || ldd % 8 || doff % 8 || lda % 8 || aoff % 8 || ldo % 8 || ooff % 8) return cudaErrorInvalidValue;
+  k_upsample2_bwd<<<blocks_for((long long)B * Hi * Wi * c / 8, 256), 256, 0, st>>>(dout, ldd, doff, act, lda, aoff,
                                                                                din, ldo, ooff, B, Hi, Wi, c);
   return cudaGetLastError();
 }
@@ -781,6 +882,17 @@ cudaError_t launch_features_to_input(const float *f, __nv_bfloat16 *x, long long
 cudaError_t launch_features(const float *guid, const float *anchor, const float *mask, int B, int H, int W,
                             float *f, cudaStream_t st) {
   k_features<<<blocks_for((long long)B * H * W, 256), 256, 0, st>>>(guid, anchor, mask, B, H, W, f);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pool_inputs(const float *g, const float *a, const float *m, int W, int H, int C, int s, int Wc,
+                               int Hc, float *cg, float *ca, float *cm, cudaStream_t st) {
+  k_pool_inputs<<<blocks_for((long long)C * Hc * Wc, 256), 256, 0, st>>>(g, a, m, W, H, C, s, Wc, Hc, cg, ca, cm);
+  return cudaGetLastError();
+}
+cudaError_t launch_compose_guess(const float *g, const float *corr, int W, int H, int C, int s, int Wc, int Hc,
+                                 float *guess, cudaStream_t st) {
+  k_compose_guess<<<blocks_for((long long)W * H * C, 256), 256, 0, st>>>(g, corr, W, H, C, s, Wc, Hc, guess);
   return cudaGetLastError();
 }
 

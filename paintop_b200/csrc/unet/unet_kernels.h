@@ -80,5 +80,12 @@ cudaError_t launch_prep_weights(const float *w, int cout, int cin, __nv_bfloat16
 cudaError_t launch_features_to_input(const float *f, __nv_bfloat16 *x, long long P, cudaStream_t st);
 cudaError_t launch_features(const float *guid, const float *anchor, const float *mask, int B, int H, int W,
                             float *f, cudaStream_t st);
+// Warm start at another resolution: pool interleaved inputs by s into a
+// (C x Hc x Wc) batch; compose guess = guidance + bilinear upsampling of the
+// (C x Hc x Wc) correction.
+cudaError_t launch_pool_inputs(const float *g, const float *a, const float *m, int W, int H, int C, int s, int Wc,
+                               int Hc, float *cg, float *ca, float *cm, cudaStream_t st);
+cudaError_t launch_compose_guess(const float *g, const float *corr, int W, int H, int C, int s, int Wc, int Hc,
+                                 float *guess, cudaStream_t st);
 
 }  // namespace unet

@@ -21,6 +21,7 @@ part comes from the network.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import math
 import os
 import time
@@ -278,37 +279,84 @@ def build_dataset(ctx, n: int = 20000, size: int = 256, seed: int = 0, chunk: in
                    t_gen, t_solve)
 
 
+class Trainer:
+    """Adam on the masked L2 loss over interior pixels, one shuffled pass per epoch.
+
+    The state that decides every later step is the network (parameters, Adam
+    moments, step count: ``pt_unet_save``) plus the epoch, the position in the
+    current permutation, that permutation and the shuffling generator's state;
+    :meth:`save` and :meth:`load` carry all of it, so a resumed run repeats an
+    uninterrupted one bit for bit."""
+
+    def __init__(self, net: UNet, data: Dataset, *, batch: int = 64, lr: float = 1e-3, seed: int = 0):
+        self.net, self.data, self.batch, self.lr = net, data, batch, lr
+        self.n = data.guidance.shape[0]
+        if self.n < batch:
+            raise ValueError("the dataset is smaller than one batch")
+        self.rng = np.random.default_rng(seed)
+        self.epoch, self.pos, self.steps = 0, 0, 0
+        self.order = self.rng.permutation(self.n)
+        self.step_s = 0.0
+
+    def _next_indices(self):
+        if self.pos + self.batch > self.n:
+            self.epoch += 1
+            self.pos = 0
+            self.order = self.rng.permutation(self.n)
+        idx = self.order[self.pos:self.pos + self.batch]
+        self.pos += self.batch
+        return idx
+
+    def step(self) -> float:
+        torch = _torch()
+        d = self.data
+        idx = torch.as_tensor(self._next_indices(), device=d.guidance.device)
+        g = d.guidance[idx].contiguous()
+        a = d.anchor[idx].contiguous()
+        m = d.mask[idx].contiguous()
+        target = (d.solution[idx] - g).contiguous()  # the correction u - g
+        f = self.net.features(g, a, m)
+        lm = interior_mask(m)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = self.net.train_step(f, target, lm, self.lr)
+        torch.cuda.synchronize()
+        self.step_s += time.perf_counter() - t0
+        self.steps += 1
+        return loss
+
+    def save(self, path: str) -> None:
+        self.net.save(path)
+        state = dict(epoch=self.epoch, pos=self.pos, steps=self.steps, batch=self.batch, lr=self.lr,
+                     n=self.n, rng=self.rng.bit_generator.state)
+        np.savez(path + ".trainer.npz", order=self.order, state=json.dumps(state))
+
+    def load(self, path: str) -> None:
+        self.net.load(path)
+        z = np.load(path + ".trainer.npz")
+        state = json.loads(str(z["state"]))
+        if state["n"] != self.n or state["batch"] != self.batch:
+            raise ValueError("checkpoint was written for another dataset size or batch")
+        self.epoch, self.pos, self.steps = state["epoch"], state["pos"], state["steps"]
+        self.lr = state["lr"]
+        self.rng.bit_generator.state = state["rng"]
+        self.order = z["order"]
+
+
 def train(net: UNet, data: Dataset, *, epochs: int = 4, batch: int = 64, lr: float = 1e-3,
           seed: int = 0, log=None, max_steps=None):
-    """Adam on the masked L2 loss over interior pixels; returns the per-step losses
-    and the device time of the training steps."""
-    torch = _torch()
-    n = data.guidance.shape[0]
-    rng = np.random.default_rng(seed)
+    """Run `epochs` passes (or `max_steps` steps); returns the per-step losses and
+    the host-timed duration of the training steps."""
+    tr = Trainer(net, data, batch=batch, lr=lr, seed=seed)
+    total = epochs * (tr.n // batch)
+    if max_steps:
+        total = min(total, max_steps)
     losses = []
-    step_s = 0.0
-    steps = 0
-    for ep in range(epochs):
-        order = rng.permutation(n)
-        for b0 in range(0, n - batch + 1, batch):
-            idx = torch.as_tensor(order[b0:b0 + batch], device=data.guidance.device)
-            g = data.guidance[idx].contiguous()
-            a = data.anchor[idx].contiguous()
-            m = data.mask[idx].contiguous()
-            u = (data.solution[idx] - g).contiguous()  # the correction u - g
-            f = net.features(g, a, m)
-            lm = interior_mask(m)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            losses.append(net.train_step(f, u, lm, lr))
-            torch.cuda.synchronize()
-            step_s += time.perf_counter() - t0
-            steps += 1
-            if log and steps % 50 == 0:
-                log(f"epoch {ep} step {steps} loss {np.mean(losses[-50:]):.3e}")
-            if max_steps and steps >= max_steps:
-                return np.asarray(losses), step_s
-    return np.asarray(losses), step_s
+    for k in range(total):
+        losses.append(tr.step())
+        if log and (k + 1) % 50 == 0:
+            log(f"epoch {tr.epoch} step {k + 1} loss {np.mean(losses[-50:]):.3e}")
+    return np.asarray(losses), tr.step_s
 
 
 def train_flops_per_pixel() -> float:
@@ -326,16 +374,50 @@ def train_flops_per_pixel() -> float:
 
 
 def predict_guess(net: UNet, guidance, anchor, mask, scale: int = 1):
-    """Warm-start guess for single-channel problems (B, H, W): guidance + the
-    predicted correction. With scale > 1 the network runs on the problem pooled
-    by `scale` (area average) and its correction is upsampled bilinearly."""
+    """Warm-start guess for single-channel problems (B, H, W) through
+    ``pt_unet_guess``: guidance + the predicted correction, the network run on
+    the problem pooled by `scale` and its correction upsampled bilinearly."""
     torch = _torch()
-    import torch.nn.functional as F  # resampling of the guess only (not the solve)
+    B, H, W = guidance.shape
+    out = torch.empty_like(guidance)
+    torch.cuda.synchronize()
+    img = H * W * 4
+    for b in range(B) if scale > 1 else []:
+        net._check(_lib.lib().pt_unet_guess(net.h, guidance.data_ptr() + b * img, anchor.data_ptr() + b * img,
+                                            mask.data_ptr() + b * img, W, H, 1, scale,
+                                            out.data_ptr() + b * img), "guess")
     if scale == 1:
-        return (guidance + net.forward(net.features(guidance, anchor, mask))).contiguous()
-    G = F.avg_pool2d(guidance[:, None], scale)[:, 0].contiguous()
-    A = F.avg_pool2d(anchor[:, None], scale)[:, 0].contiguous()
-    M = F.avg_pool2d(mask[:, None], scale)[:, 0].contiguous()
-    corr = net.forward(net.features(G, A, M))
-    corr = F.interpolate(corr[:, None], scale_factor=scale, mode="bilinear", align_corners=False)[:, 0]
-    return (guidance + corr).contiguous()
+        # the batch as channels of one image would share one mask: run the
+        # network on the batch directly instead
+        out = (guidance + net.forward(net.features(guidance, anchor, mask))).contiguous()
+    return out
+
+
+def guess_image(net: UNet, guidance, anchor, mask, scale: int):
+    """pt_unet_guess on one interleaved (H, W, C) problem held in device tensors."""
+    torch = _torch()
+    H, W, Ch = guidance.shape
+    out = torch.empty_like(guidance)
+    torch.cuda.synchronize()
+    net._check(_lib.lib().pt_unet_guess(net.h, _dptr(guidance), _dptr(anchor), _dptr(mask), W, H, Ch, scale,
+                                        _dptr(out)), "guess")
+    return out
+
+
+def save_params(net: UNet, path: str) -> None:
+    """The network's fp32 parameters (no optimiser state) as a small file."""
+    p = net.get_params()
+    with open(path, "wb") as f:
+        f.write(b"PTUNETP1")
+        f.write(np.array([p.size], dtype="<u8").tobytes())
+        f.write(p.astype("<f4").tobytes())
+
+
+def load_params(net: UNet, path: str) -> None:
+    with open(path, "rb") as f:
+        if f.read(8) != b"PTUNETP1":
+            raise ValueError(f"{path}: not a parameter file")
+        n = int(np.frombuffer(f.read(8), dtype="<u8")[0])
+        if n != net.param_count:
+            raise ValueError(f"{path}: {n} parameters, the network has {net.param_count}")
+        net.set_params(np.frombuffer(f.read(4 * n), dtype="<f4"))
