@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark: Poisson solves/s at relative residual 1e-6 on the screened 2048^2 workload.
+"""Benchmark: Poisson solves/s at relative residual 1e-6 on the screened 2048^2 workload,
+plus the learned warm start against the plain solve on 4096^2 RGB inputs.
 
 Workload (one "step" = one solve): 2048x2048 RGBA f32 screened-Poisson,
 lambda = 0.01, a random 12-vertex star mask covering 30% (+-2%), relative
@@ -11,6 +12,8 @@ Arms:
                      HBM (device pointers); `e2e`: solves/s through the C ABI with
                      pinned host buffers, host<->device copies inside the timed
                      region.
+  learned_warm_start (N=1) solves/s of U-Net guess + SOR vs plain SOR on the
+                     same 4096x4096 RGB, 8-polygon inputs (``learned_leg``).
   --impl reference   the reference op's CPU algorithm (the oracle restatement of
                      crates/paintop-cpu/src/poisson.rs) on the host cores, one
                      channel solve per step as a bounded sample.
@@ -323,6 +326,10 @@ def gpu_arm(args):
     peak, peak_kind = _peaks()
     traffic = _profile_traffic()
 
+    learned = None
+    if ws == 1 and not args.no_learned and not args.device_only:
+        learned = learned_leg(ctx, dev)  # reported apart; outside the timed region above
+
     line = None
     if rank == 0:
         cpu = cpu_baseline_sample(inst) if (ws == 1 and not args.no_cpu_baseline and
@@ -350,6 +357,7 @@ def gpu_arm(args):
             "clocks": clocks,
             "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
                        "converged": converged, "worst_final_residual": worst_res},
+            "learned_warm_start": learned,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -504,6 +512,73 @@ def batch_arm(args):
     return 0
 
 
+LEARNED_PARAMS = os.path.join(ROOT, "paintop_b200", "weights", "warmstart_unet_256.params")
+
+
+def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8):
+    """Learned warm start vs plain SOR on the same inputs: 4096x4096 RGB, 8
+    polygons (3-10% of the area each), relative residual 1e-6, automatic omega
+    for both, inputs resident in HBM. The network (trained by
+    paintop_b200.train_warmstart on 20,000 256x256 solves) runs on the inputs
+    pooled by `scale`; its upsampled correction plus the guidance seeds the
+    solve. Time per solve = guess + solve (CUDA events on the context stream)."""
+    import ctypes as Ct
+    import torch
+    from paintop_b200 import _lib, synth, warmstart
+    if not os.path.exists(LEARNED_PARAMS):
+        return {"unavailable": "no trained parameters at paintop_b200/weights"}
+    inst = synth.multi_4096(1)
+    W, H, C = inst.width, inst.height, inst.channels
+    g = torch.as_tensor(inst.source, device=dev).contiguous()
+    a = torch.as_tensor(inst.target, device=dev).contiguous()
+    m = torch.as_tensor(inst.mask, device=dev).contiguous()
+    out = torch.empty_like(g)
+    guess = torch.empty_like(g)
+    net = warmstart.UNet(ctx, seed=0)
+    warmstart.load_params(net, LEARNED_PARAMS)
+    L = _lib.lib()
+    reps = (_lib.PtReport * (C + 1))()
+    flags = _lib.PT_FLAG_DEVICE_POINTERS | _lib.PT_FLAG_OMEGA_AUTO
+    p_plain = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), 0.0, 100000, 1e-6, 1.8,
+                             flags, None)
+    p_warm = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), 0.0, 100000, 1e-6, 1.8,
+                            flags | _lib.PT_FLAG_WARM_START, guess.data_ptr())
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    torch.cuda.synchronize(dev)
+
+    def run(learned: bool):
+        if learned:
+            st = L.pt_unet_guess(net.h, g.data_ptr(), a.data_ptr(), m.data_ptr(), W, H, C, scale, guess.data_ptr())
+            if st != _lib.PT_OK:
+                raise _lib.CudaError(st, ctx.last_error())
+        st = L.pt_poisson_solve(ctx.h, Ct.byref(p_warm if learned else p_plain), out.data_ptr(), reps, None)
+        if st != _lib.PT_OK:
+            raise _lib.CudaError(st, ctx.last_error())
+        return [int(reps[c].iterations) for c in range(C)], all(reps[c].converged for c in range(C)), \
+            [bool(reps[c].warm_start) for c in range(C)]
+
+    res = {}
+    for learned in (False, True):
+        for _ in range(warmup):
+            run(learned)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            sweeps, conv, used = run(learned)
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / steps
+        res["learned" if learned else "plain"] = dict(solves_per_s=1.0 / sec, ms_per_solve=sec * 1e3,
+                                                      sweeps=sweeps, converged=conv,
+                                                      **({"guess_used": used} if learned else {}))
+    net.close()
+    return {"workload": "multi_4096: 4096x4096 RGB, 8 polygons 3-10% each, rel-res 1e-6, automatic omega",
+            "model": "U-Net 16-32-64-128, bf16, trained on 20,000 256x256 solves; inference pooled x%d" % scale,
+            "steps": steps, **res,
+            "speedup": res["learned"]["solves_per_s"] / res["plain"]["solves_per_s"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,6 +590,8 @@ def main():
                     help="time only the device-resident arm (for profiler runs)")
     ap.add_argument("--workload", default="screened_2048", choices=["screened_2048", "batch_uneven"])
     ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-warm-start leg (4096x4096 RGB, learned vs plain)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "cuda":
         args.warmup = 3

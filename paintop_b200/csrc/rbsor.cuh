@@ -101,6 +101,17 @@ struct SysDesc {
   double tol;
   int max_it;
   int warm;                // 1 if an initial guess is staged
+  int region1;             // 1 + index of the image's RegionDesc (automatic omega), 0: none
+  int pad;
+};
+
+// Connected interior regions of one image, for the automatic SOR factor. The
+// channels of an image share its mask, so each image is labelled once.
+struct RegionDesc {
+  long long lab_off;       // offset of the image's pixels in the label / size arrays
+  int W, H;
+  int sys0;                // the image's first system (its mask and extent)
+  int pad;
 };
 
 struct SysState {
@@ -147,6 +158,13 @@ struct KParams {
   int *err;
   unsigned long long budget_ns;
   int S;                   // sweeps per step of this launch
+  // connected regions (automatic omega); nregions = 0 skips the labelling
+  const RegionDesc *regions;
+  int nregions;
+  long long rpix;          // pixels of all labelled images
+  int *label;              // per pixel: region root (local pixel index) or -1
+  int *rsize;              // per pixel: region size, at the root
+  int *rmax;               // per RegionDesc: largest region size
 };
 
 }  // namespace ptk

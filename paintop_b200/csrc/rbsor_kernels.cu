@@ -208,6 +208,84 @@ __global__ void __launch_bounds__(kThreads) k_assemble(KParams P, int TW, int TH
   }
 }
 
+// ---- connected interior regions (automatic omega) --------------------------
+// A union-find over the pixels of each labelled image (4-neighbour
+// connectivity): every label points at itself (a root) or at a smaller index
+// of the same region, so a root search walks strictly decreasing indices and
+// ends; unions lower a root with atomicMin, so each retry sees a smaller
+// label and ends too. The final labels are the regions' smallest pixel
+// indices whatever the order of the unions, so the result is deterministic.
+__device__ __forceinline__ int region_of(const KParams &P, long long gp) {
+  int lo = 0, hi = P.nregions - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (P.regions[mid].lab_off <= gp) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ int label_root(int *L, int x) {
+  const volatile int *vl = L;
+  const int x0 = x;
+  for (int k = x; k >= 0; --k) {  // at most x + 1 steps: labels only decrease
+    const int y = vl[x];
+    if (y == x) break;
+    x = y;
+  }
+  if (x != x0) atomicMin(&L[x0], x);  // shorten the chain; never raises a label
+  return x;
+}
+__device__ void label_unite(int *L, int a, int b) {
+  for (int k = a + b + 2; k > 0; --k) {  // each retry lowers a or b
+    a = label_root(L, a);
+    b = label_root(L, b);
+    if (a == b) return;
+    if (a < b) {
+      const int old = atomicMin(&L[b], a);
+      if (old == b) return;
+      b = old;
+    } else {
+      const int old = atomicMin(&L[a], b);
+      if (old == a) return;
+      a = old;
+    }
+  }
+}
+__global__ void k_label_init(KParams P) {
+  for (long long gp = blockIdx.x * (long long)blockDim.x + threadIdx.x; gp < P.rpix;
+       gp += (long long)gridDim.x * blockDim.x) {
+    const RegionDesc r = P.regions[region_of(P, gp)];
+    const int p = (int)(gp - r.lab_off), y = p / r.W, x = p - y * r.W;
+    P.label[gp] = interior_at(P.sys[r.sys0], x, y) ? p : -1;
+  }
+}
+__global__ void k_label_link(KParams P) {
+  for (long long gp = blockIdx.x * (long long)blockDim.x + threadIdx.x; gp < P.rpix;
+       gp += (long long)gridDim.x * blockDim.x) {
+    if (P.label[gp] < 0) continue;
+    const RegionDesc r = P.regions[region_of(P, gp)];
+    int *L = P.label + r.lab_off;
+    const int p = (int)(gp - r.lab_off), y = p / r.W, x = p - y * r.W;
+    if (x > 0 && L[p - 1] >= 0) label_unite(L, p, p - 1);
+    if (y > 0 && L[p - r.W] >= 0) label_unite(L, p, p - r.W);
+  }
+}
+__global__ void k_label_count(KParams P) {
+  for (long long gp = blockIdx.x * (long long)blockDim.x + threadIdx.x; gp < P.rpix;
+       gp += (long long)gridDim.x * blockDim.x) {
+    if (P.label[gp] < 0) continue;
+    const RegionDesc r = P.regions[region_of(P, gp)];
+    const int root = label_root(P.label + r.lab_off, (int)(gp - r.lab_off));
+    atomicAdd(&P.rsize[r.lab_off + root], 1);
+  }
+}
+__global__ void k_label_max(KParams P) {
+  for (long long gp = blockIdx.x * (long long)blockDim.x + threadIdx.x; gp < P.rpix;
+       gp += (long long)gridDim.x * blockDim.x) {
+    const int n = P.rsize[gp];
+    if (n > 0) atomicMax(&P.rmax[region_of(P, gp)], n);
+  }
+}
+
 // Per-system initial state from the assembly partials (tile order).
 __global__ void k_init(KParams P) {
   __shared__ double sred[kWarps];
@@ -263,6 +341,20 @@ __global__ void k_init(KParams P) {
       const double a = (double)(bx1 - bx0 + 2), b = (double)(by1 - by0 + 2);
       const double pi = 3.141592653589793;
       double rho = (2.0 * cos(pi / a) + 2.0 * cos(pi / b)) / (4.0 + d.lambda);
+      // Several regions share one box: bound the largest region's smallest
+      // eigenvalue from its area instead (Faber-Krahn: no region of that area
+      // has a smaller one than the disk, pi j0^2 / area), with the area grown
+      // to (sqrt(n) + 1)^2 for the half-cell margin of the discrete boundary.
+      // Both are upper bounds on the Jacobi spectral radius; take the smaller.
+      if (d.region1 > 0) {
+        const int nmax = P.rmax[d.region1 - 1];
+        if (nmax > 0) {
+          const double area = (sqrt((double)nmax) + 1.0) * (sqrt((double)nmax) + 1.0);
+          const double j0 = 2.404825557695773;  // first zero of the Bessel function J0
+          const double pij0sq = 3.141592653589793 * (j0 * j0);
+          rho = fmin(rho, (4.0 - pij0sq / area) / (4.0 + d.lambda));
+        }
+      }
       rho = fmin(fmax(rho, 0.0), 1.0 - 1e-15);
       om = 2.0 / (1.0 + sqrt(1.0 - rho * rho));
     }
@@ -870,6 +962,17 @@ size_t tile_config_smem(int idx) {
 
 cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t stream, bool any_warm) {
   if (P.ntiles <= 0) return cudaSuccess;
+  if (P.nregions > 0) {
+    cudaError_t e = cudaMemsetAsync(P.rsize, 0, P.rpix * sizeof(int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P.rmax, 0, P.nregions * sizeof(int), stream);
+    if (e != cudaSuccess) return e;
+    long long nb = (P.rpix + 255) / 256;
+    const unsigned blocks = (unsigned)(nb > 148 * 16 ? 148 * 16 : (nb < 1 ? 1 : nb));
+    k_label_init<<<blocks, 256, 0, stream>>>(P);
+    k_label_link<<<blocks, 256, 0, stream>>>(P);
+    k_label_count<<<blocks, 256, 0, stream>>>(P);
+    k_label_max<<<blocks, 256, 0, stream>>>(P);
+  }
   k_tile_count<<<P.ntiles, 256, 0, stream>>>(P, tc.tw, tc.th);
   k_compact<<<P.nsys, 256, 0, stream>>>(P);
   k_assemble<<<P.ntiles, kThreads, 0, stream>>>(P, tc.tw, tc.th);

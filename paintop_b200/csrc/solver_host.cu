@@ -85,12 +85,14 @@ struct Plan {
   long long in_floats = 0; // staged input floats (images + guesses)
   long long mask_floats = 0;
   long long out_floats = 0;
+  std::vector<RegionDesc> regions;  // images labelled for the automatic omega
+  long long rpix = 0;               // their pixels
 };
 
 // Arena layout (byte offsets) for one call.
 struct Layout {
   size_t sys, st, claim, arrive, tiles, tcount, tbox, act, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in,
-      mask, out, total;
+      mask, out, regions, label, rsize, rmax, total;
 };
 
 Layout layout(const Plan &pl, bool stage) {
@@ -120,6 +122,10 @@ Layout layout(const Plan &pl, bool stage) {
   L.in = stage ? take(pl.in_floats * sizeof(float)) : 0;
   L.mask = stage ? take(pl.mask_floats * sizeof(float)) : 0;
   L.out = stage ? take(pl.out_floats * sizeof(float)) : 0;
+  L.regions = take(pl.regions.size() * sizeof(RegionDesc));
+  L.label = take((size_t)pl.rpix * sizeof(int));
+  L.rsize = take((size_t)pl.rpix * sizeof(int));
+  L.rmax = take(pl.regions.size() * sizeof(int));
   L.total = o;
   return L;
 }
@@ -165,6 +171,12 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     // automatic omega is chosen on the device from the region's extent
     const double omega = (p.flags & PT_FLAG_OMEGA_AUTO) ? -1.0 : p.omega;
     const long long img = (long long)W * H;
+    int region1 = 0;
+    if ((p.flags & PT_FLAG_OMEGA_AUTO) && C > 0 && img > 0) {
+      pl.regions.push_back(RegionDesc{pl.rpix, W, H, (int)pl.sys.size(), 0});
+      pl.rpix += img;
+      region1 = (int)pl.regions.size();
+    }
     for (int c = 0; c < C; ++c) {
       SysDesc d{};
       d.inst = (int)i; d.chan = c; d.W = W; d.H = H; d.C = C; d.pw = pw;
@@ -184,6 +196,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       d.tol = p.tolerance;
       d.max_it = (int)p.max_iterations;
       d.warm = (p.flags & PT_FLAG_WARM_START) ? 1 : 0;
+      d.region1 = region1;
       pl.sys.push_back(d);
     }
     if (C > 0) {
@@ -254,6 +267,9 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(base + L.tiles, pl.tiles.data(), pl.tiles.size() * sizeof(Tile),
                          cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess && !pl.regions.empty())
+    ce = cudaMemcpyAsync(base + L.regions, pl.regions.data(), pl.regions.size() * sizeof(RegionDesc),
+                         cudaMemcpyHostToDevice, st);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "plan upload");
 
   KParams P{};
@@ -280,6 +296,12 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   P.err = reinterpret_cast<int *>(base + L.err);
   P.budget_ns = (unsigned long long)(ctx->budget_s * 1e9);
   P.S = pl.tc.S;
+  P.regions = reinterpret_cast<const RegionDesc *>(base + L.regions);
+  P.nregions = (int)pl.regions.size();
+  P.rpix = pl.rpix;
+  P.label = reinterpret_cast<int *>(base + L.label);
+  P.rsize = reinterpret_cast<int *>(base + L.rsize);
+  P.rmax = reinterpret_cast<int *>(base + L.rmax);
 
   int grid = 0;
   ce = prepare_solve(P, pl.cfg, ctx->sms, &grid);
