@@ -113,6 +113,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint3
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+// Arrive and add `bytes` to the transaction count the phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// ---- TMA (tensor copies; never multicast) -----------------------------------
+// One box of a 4-D tensor map into shared memory; completion is reported to
+// `mbar` as transaction bytes. Coordinates are element indices, innermost
+// first; out-of-range elements read as zero.
+__device__ __forceinline__ void tma_load_4d(void *smem_dst, const void *tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t *mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(smem_dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // ---- cp.async ---------------------------------------------------------------
 __device__ __forceinline__ void cp16(void *smem_dst, const void *gmem_src, bool in) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src),

@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -122,7 +123,8 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
   size_t maxch = 0;
   for (int l = 0; l < 14; ++l) {
     const int lev = (l <= 1 || l >= 12) ? 0 : (l <= 3 || l >= 10) ? 1 : (l <= 5 || l >= 8) ? 2 : 3;
-    const int ch = wgrad_chunks(B, H >> lev, W >> lev);
+    int ch = wgrad_chunks(B, H >> lev, W >> lev);
+    if ((W >> lev) % 128 == 0) ch = std::max(ch, wgrad_tma_chunks(B, H >> lev, W >> lev));
     const size_t need = (size_t)ch * 9 * kLayers[l].cout * kLayers[l].cin;
     if (need > maxch) maxch = need;
   }
@@ -151,6 +153,21 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
   return cudaMemset(n->err, 0, sizeof(int)) == cudaSuccess ? PT_OK : PT_LAUNCH_FAILED;
 }
 
+// The TMA halo kernels serve layers whose width is a multiple of 128;
+// PAINTOP_UNET_TMA=0 routes every layer through the gather kernels instead.
+bool tma_enabled() {
+  const char *e = std::getenv("PAINTOP_UNET_TMA");
+  return !(e && e[0] == '0');
+}
+
+cudaError_t launch_conv_any(const ConvArgs &a, int n, cudaStream_t st) {
+  if (tma_enabled() && conv_tma_ok(a, n)) {
+    const cudaError_t e = launch_conv_tma(a, n, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  return launch_conv3x3(a, n, st);
+}
+
 pt_status conv(pt_unet *n, int l, const Act &x, int x_off, const Act &y, int y_off, bool relu) {
   ConvArgs a{};
   a.x = x.p; a.ldx = x.c; a.x_off = x_off; a.cin = kLayers[l].cin;
@@ -158,7 +175,7 @@ pt_status conv(pt_unet *n, int l, const Act &x, int x_off, const Act &y, int y_o
   a.bias = n->params + n->b_off[l];
   a.y = y.p; a.ldy = y.c; a.y_off = y_off; a.relu = relu ? 1 : 0;
   a.B = n->B; a.H = n->H >> x.level; a.W = n->W >> x.level; a.err = n->err;
-  CK(launch_conv3x3(a, kLayers[l].cout, n->ctx->stream), "conv forward");
+  CK(launch_conv_any(a, kLayers[l].cout, n->ctx->stream), "conv forward");
   return PT_OK;
 }
 
@@ -171,7 +188,7 @@ pt_status dgrad(pt_unet *n, int l, const Act &dy, const Act &dx, int dx_off, con
   a.y = dx.p; a.ldy = dx.c; a.y_off = dx_off; a.relu = 0;
   if (mask) { a.mask = mask->p; a.ldm = mask->c; a.m_off = m_off; }
   a.B = n->B; a.H = n->H >> dy.level; a.W = n->W >> dy.level; a.err = n->err;
-  CK(launch_conv3x3(a, kLayers[l].cin, n->ctx->stream), "conv backward-data");
+  CK(launch_conv_any(a, kLayers[l].cin, n->ctx->stream), "conv backward-data");
   return PT_OK;
 }
 
@@ -182,7 +199,18 @@ pt_status wgrad(pt_unet *n, int l, const Act &dy, const Act &x, int x_off) {
   a.x = x.p; a.ldx = x.c; a.x_off = x_off;
   a.B = n->B; a.H = n->H >> dy.level; a.W = n->W >> dy.level;
   a.part = n->wpart; a.dw = n->grad + n->w_off[l]; a.err = n->err;
-  CK(launch_wgrad(a, kLayers[l].cin, n->ctx->stream), "conv backward-weights");
+  bool done = false;
+  if (tma_enabled() && wgrad_tma_ok(a, kLayers[l].cin)) {
+    int chunks = 0;
+    const cudaError_t e = launch_wgrad_tma(a, kLayers[l].cin, n->ctx->stream, &chunks);
+    if (e == cudaSuccess) {
+      CK(launch_wgrad_reduce(a.part, chunks, a.cout, kLayers[l].cin, a.dw, n->ctx->stream), "weight reduce");
+      done = true;
+    } else if (e != cudaErrorNotSupported) {
+      return cfail(n, e, "conv backward-weights");
+    }
+  }
+  if (!done) CK(launch_wgrad(a, kLayers[l].cin, n->ctx->stream), "conv backward-weights");
   CK(launch_colsum(dy.p, dy.c, 0, kLayers[l].cout, npix(n, dy.level), n->cpart, n->grad + n->b_off[l],
                    n->ctx->stream),
      "bias gradient");

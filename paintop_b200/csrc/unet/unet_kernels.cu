@@ -786,6 +786,11 @@ cudaError_t launch_wgrad(const WgradArgs &a, int cin, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st) {
+  k_wgrad_reduce<<<256, 256, 0, st>>>(part, nchunks, cout, cin, dw);
+  return cudaGetLastError();
+}
+
 static unsigned blocks_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b > 148 * 32) b = 148 * 32;

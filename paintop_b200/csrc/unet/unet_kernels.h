@@ -46,6 +46,14 @@ struct WgradArgs {
 };
 
 cudaError_t launch_conv3x3(const ConvArgs &a, int n, cudaStream_t st);
+// TMA halo path (conv_tma.cu) for widths that are multiples of 128; the
+// launchers return cudaErrorNotSupported when a tensor map cannot be built.
+bool conv_tma_ok(const ConvArgs &a, int n);
+cudaError_t launch_conv_tma(const ConvArgs &a, int n, cudaStream_t st);
+bool wgrad_tma_ok(const WgradArgs &a, int cin);
+int wgrad_tma_chunks(int B, int H, int W);
+cudaError_t launch_wgrad_tma(const WgradArgs &a, int cin, cudaStream_t st, int *chunks);
+cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st);
 int wgrad_chunks(int B, int H, int W);
 cudaError_t launch_wgrad(const WgradArgs &a, int cin, cudaStream_t st);
 int colsum_parts(long long P);

@@ -3,6 +3,7 @@
   python -m paintop_b200.train_warmstart train --instances 20000 --epochs 8 --out DIR
   python -m paintop_b200.train_warmstart eval256 --params FILE --instances 256
   python -m paintop_b200.train_warmstart multi4096 --params FILE --scale 8
+  python -m paintop_b200.train_warmstart steps --batch 64 --steps 10
 
 ``train`` generates the seeded 256x256 single-channel instances on the device,
 solves each with the library's own red-black SOR + FP64 refinement to a
@@ -199,6 +200,30 @@ def cmd_multi4096(args):
     ctx.close()
 
 
+def cmd_steps(args):
+    """Training steps on seeded instances without solving them (the target is
+    the anchor's correction): a fixed workload for timing and profiling."""
+    torch = ws._torch()
+    ctx = _lib.Context(0)
+    net = ws.UNet(ctx, seed=0)
+    g, a, m = ws.make_instances(args.batch, args.size, seed=3)
+    f = net.features(g, a, m)
+    lm = ws.interior_mask(m)
+    t = (a - g).contiguous()
+    for _ in range(args.warmup):
+        net.train_step(f, t, lm, 1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.train_step(f, t, lm, 1e-3)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    flops = ws.train_flops_per_pixel() * args.batch * args.size * args.size
+    print(json.dumps(dict(batch=args.batch, size=args.size, steps=args.steps, step_ms=dt * 1e3,
+                          tflops=flops / dt / 1e12)))
+    ctx.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m paintop_b200.train_warmstart")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -216,8 +241,13 @@ def main(argv=None):
     c.add_argument("--params", required=True)
     c.add_argument("--scale", type=int, default=8)
     c.add_argument("--seed", type=int, default=1)
+    p = sub.add_parser("steps")
+    p.add_argument("--batch", type=int, default=64)
+    p.add_argument("--size", type=int, default=256)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
     args = ap.parse_args(argv)
-    {"train": cmd_train, "eval256": cmd_eval256, "multi4096": cmd_multi4096}[args.cmd](args)
+    {"train": cmd_train, "eval256": cmd_eval256, "multi4096": cmd_multi4096, "steps": cmd_steps}[args.cmd](args)
 
 
 if __name__ == "__main__":

@@ -50,7 +50,12 @@ def test_features_bit_exact(ctx, ws, torch_cuda):
     assert np.array_equal(f.view(np.uint32), ref.view(np.uint32))
 
 
-@pytest.mark.parametrize("B,H,W", [(2, 32, 32), (1, 24, 40), (2, 64, 64)])
+# widths that are multiples of 128 run the TMA halo kernels on their first
+# levels; the others the gather kernels
+SHAPES = [(2, 32, 32), (1, 24, 40), (2, 64, 64), (1, 64, 256), (2, 40, 128)]
+
+
+@pytest.mark.parametrize("B,H,W", SHAPES)
 def test_forward_matches_oracle(ctx, ws, torch_cuda, B, H, W):
     torch = torch_cuda
     net = ws.UNet(ctx, seed=2)
@@ -64,7 +69,7 @@ def test_forward_matches_oracle(ctx, ws, torch_cuda, B, H, W):
     assert _rel(pred, ref) < 1e-2
 
 
-@pytest.mark.parametrize("B,H,W", [(2, 32, 32), (1, 24, 40), (2, 64, 64)])
+@pytest.mark.parametrize("B,H,W", SHAPES)
 def test_gradients_match_oracle(ctx, ws, torch_cuda, B, H, W):
     torch = torch_cuda
     net = ws.UNet(ctx, seed=3)
@@ -92,9 +97,28 @@ def test_gradients_match_oracle(ctx, ws, torch_cuda, B, H, W):
     assert not grad[w0:b0].reshape(co0, 9, ci0)[:, :, R.IN_REAL:].any()
 
 
+def test_tma_and_gather_paths_agree(ctx, ws, torch_cuda, monkeypatch):
+    """The same step through the TMA halo kernels and through the gather
+    kernels (PAINTOP_UNET_TMA=0): equal up to accumulation order."""
+    net = ws.UNet(ctx, seed=5)
+    g, a, m = _realistic(ws, torch_cuda, 2, 64, 256, seed=13)
+    f = net.features(g, a, m)
+    lm = ws.interior_mask(m)
+    pred_t = net.forward(f).cpu().numpy()
+    l_t, g_t = net.loss_grad(f, a, lm)
+    monkeypatch.setenv("PAINTOP_UNET_TMA", "0")
+    pred_g = net.forward(f).cpu().numpy()
+    l_g, g_g = net.loss_grad(f, a, lm)
+    assert _rel(pred_t, pred_g) < 1e-2
+    assert abs(l_t - l_g) <= 1e-2 * abs(l_g)
+    layout, head_w, total = R.param_layout()
+    for l, (w, b, co, ci) in enumerate(layout):
+        assert _rel(g_t[w:b], g_g[w:b]) < 3e-2, l
+
+
 def test_loss_grad_is_deterministic(ctx, ws, torch_cuda):
     net = ws.UNet(ctx, seed=4)
-    g, a, m = _realistic(ws, torch_cuda, 2, 64, 64, seed=8)
+    g, a, m = _realistic(ws, torch_cuda, 2, 64, 256, seed=8)
     f = net.features(g, a, m)
     lm = ws.interior_mask(m)
     l1, g1 = net.loss_grad(f, a, lm)
