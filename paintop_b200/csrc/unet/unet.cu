@@ -124,7 +124,7 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
   for (int l = 0; l < 14; ++l) {
     const int lev = (l <= 1 || l >= 12) ? 0 : (l <= 3 || l >= 10) ? 1 : (l <= 5 || l >= 8) ? 2 : 3;
     int ch = wgrad_chunks(B, H >> lev, W >> lev);
-    if ((W >> lev) % 128 == 0) ch = std::max(ch, wgrad_tma_chunks(B, H >> lev, W >> lev));
+    ch = std::max(ch, wgrad_tma_chunks(B, H >> lev, W >> lev));
     const size_t need = (size_t)ch * 9 * kLayers[l].cout * kLayers[l].cin;
     if (need > maxch) maxch = need;
   }
@@ -196,7 +196,7 @@ pt_status dgrad(pt_unet *n, int l, const Act &dy, const Act &dx, int dx_off, con
 pt_status wgrad(pt_unet *n, int l, const Act &dy, const Act &x, int x_off) {
   WgradArgs a{};
   a.dy = dy.p; a.lddy = dy.c; a.dy_off = 0; a.cout = kLayers[l].cout;
-  a.x = x.p; a.ldx = x.c; a.x_off = x_off;
+  a.x = x.p; a.ldx = x.c; a.x_off = x_off; a.cin = kLayers[l].cin;
   a.B = n->B; a.H = n->H >> dy.level; a.W = n->W >> dy.level;
   a.part = n->wpart; a.dw = n->grad + n->w_off[l]; a.err = n->err;
   bool done = false;

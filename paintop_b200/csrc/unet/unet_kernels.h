@@ -39,6 +39,7 @@ struct WgradArgs {
   int lddy, dy_off, cout;   // cout <= 128, multiple of 8
   const __nv_bfloat16 *x;   // forward input, pitch ldx, offset x_off
   int ldx, x_off;
+  int cin;                  // input channels (the TMA path reads it; the gather path takes it as an argument)
   int B, H, W;
   float *part;              // [chunks][9][cout][cin] partials
   float *dw;                // [cout][9][cin] result
