@@ -1,35 +1,41 @@
 // conv_tma.cu -- persistent, warp-specialised 3x3 convolutions on tcgen05 with
-// TMA halo loads.
+// TMA halo loads, on activations in the channel-blocked layout
+// [B][C/8][H][W][8] (unet_kernels.h).
 //
-// Tiling. A tile is one segment of SW = min(W, 128) pixels of one image row
-// (W a multiple of SW, SW a multiple of 16). For channel group g (8 channels)
-// and halo row r (image row y - 1 + r), TMA loads the box {8 channels, HP
-// pixels, 1 row} starting at x0 - 1, HP = SW + 8 (a multiple of 8, so every
-// box starts on a 128-byte boundary); out-of-image pixels read as zero, which
-// is the convolution's zero padding. Box (g, r) lands at row (3g + r) * HP of
-// the stage, one 16-byte row per pixel (8 channels). In the canonical
-// no-swizzle layout consecutive 16-byte rows are consecutive core-matrix rows
-// along M (K-major operand) or K (MN-major operand), so the operand of tap
-// (dy, dx) for output pixel m is row (3g + 1 + dy) * HP + 1 + dx + m: a shift
-// of the descriptor's start address by 16 bytes per pixel. One halo tile feeds
-// all nine taps.
+// Tiling. A tile is one segment of SW pixels of one image row: SW = 128, or
+// W rounded up to 16 for narrower images; a row's last segment may reach past
+// W (those pixels load as zero and are never stored). TMA sees a plane row as
+// W / CW chunks of CW pixels (CW = 16, or the largest power of two dividing W
+// when W is not a multiple of 16): a 4-D tensor {CW * 8 elements, W / CW
+// chunks, H rows, C/8 * B planes}. For channel group g one box of {CW * 8, HP
+// / CW chunks, 3 rows} starting one chunk left of the segment and one row
+// above it lands in shared memory as 3 rows of HP 16-byte entries (one entry =
+// one pixel's 8 channels), each row one contiguous line per chunk; pixels
+// outside the image read as zero, the convolution's zero padding. Entry CW of
+// a row is pixel x0. Row (g, r) sits at (3g + r) * HP entries. In the
+// canonical no-swizzle layout consecutive 16-byte entries are consecutive
+// core-matrix rows along M (K-major operand) or K (MN-major operand), so the
+// operand of tap (dy, dx) for output pixel m is entry
+// (3g + 1 + dy) * HP + CW + dx + m: a shift of the descriptor's start address
+// by 16 bytes per pixel. One halo tile feeds all nine taps.
 //
 // k_conv_tma<N> (forward / backward-data): GEMM rows = the segment's pixels
 // (M = 128; rows past SW are never stored), columns = N output channels (the
-// CTA's part [n0, n0 + N) of them: blockIdx.y), K = (tap, channel): K groups
-// (g, g+1) of one tap are 3 * HP rows apart. The CTA's weights stay resident
-// in shared memory. Roles: one warp's lane 0 issues TMA loads into a ring of
-// stages (full/empty mbarriers); one warp allocates TMEM and its lane 0 issues
-// the MMAs into one accumulator per epilogue warpgroup; two warpgroups take
+// CTA's part [n0, n0 + N) of them: blockIdx.y), K = (tap, channel) taken in
+// chunks of up to 64 channels per pipeline stage: K groups (g, g+1) of one
+// tap are 3 * HP entries apart. The CTA's weights stay resident in shared
+// memory. Roles: one warp's lane 0 issues TMA loads into a ring of stages
+// (full/empty mbarriers); one warp allocates TMEM and its lane 0 issues the
+// MMAs into one accumulator per epilogue warpgroup; two warpgroups take
 // alternate tiles through the epilogue (bias, ReLU, ReLU mask -> bf16).
 //
 // k_wgrad_tma<CP> (backward-weights): D[co][tap][ci] += sum over the segment's
 // pixels of dY[p][co] X[p + off(tap)][ci]. GEMM rows = output channels
 // (padded to 128: rows past cout read whatever follows in shared memory and
 // are never stored), K = pixels, and columns = (channel group, dy, channel):
-// the halo boxes of one part of CP channels are 3 * CP / 8 groups of 8
-// columns at a constant stride of HP rows, so one MMA covers the three dy taps
-// of that part (N = 3 CP) and dx selects the start row. A CTA owns a fixed
+// the halo rows of one part of CP channels are 3 * CP / 8 groups of 8 columns
+// at a constant stride of HP entries, so one MMA covers the three dy taps of
+// that part (N = 3 CP) and dx selects the start entry. A CTA owns a fixed
 // range of segments, one part of the channels and one or all three dx values,
 // accumulates in TMEM and writes one fp32 partial per (tap, co, ci); the
 // partials are summed in chunk order by k_wgrad_reduce.
@@ -42,6 +48,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -75,7 +82,7 @@ __host__ __device__ inline uint32_t pow2_cols(int n) {
 
 // Segment geometry shared by both kernels.
 struct SegGeom {
-  int SW, HP;           // segment width, halo row pitch (pixels)
+  int SW, CW, HP;       // segment width, TMA chunk width, halo row pitch (pixels)
   int segs_x, nseg;     // segments per row, segments in total
   int nst;              // pipeline stages
 };
@@ -92,6 +99,8 @@ constexpr int kEpiGroups = 2;                            // epilogue warpgroups 
 constexpr int kConvThreads = 32 * (4 * kEpiGroups + 2);  // + producer warp + MMA warp
 constexpr int kProdWarp = 4 * kEpiGroups, kMmaWarp = 4 * kEpiGroups + 1;
 
+constexpr int kChunkGroups = 8;  // channel groups (64 channels) per pipeline stage
+
 template <int N>
 __global__ void __launch_bounds__(kConvThreads, 2)
     k_conv_tma(const __grid_constant__ CUtensorMap xmap, ConvArgs a, ConvTmaGeom g) {
@@ -103,9 +112,10 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g8 = a.cin / 8;           // channel groups of the input
   const int KK = 9 * g8;              // 8-element K groups of the weights
-  const int SW = g.s.SW, HP = g.s.HP, nst = g.s.nst, ntiles = g.s.nseg;
-  const int rowb = HP * 16;           // bytes of one halo row box
-  const int stage_bytes = 3 * g8 * rowb;
+  const int nkc = (g8 + kChunkGroups - 1) / kChunkGroups;  // K chunks per tile
+  const int SW = g.s.SW, HP = g.s.HP, CW = g.s.CW, nst = g.s.nst, ntiles = g.s.nseg;
+  const int rowb = HP * 16;           // bytes of one halo row
+  const int stage_bytes = 3 * min(g8, kChunkGroups) * rowb;
   const int n0 = blockIdx.y * N;      // the CTA's output channels
   unsigned char *sW = sm;
   unsigned char *sA = sm + g.w_bytes;
@@ -143,22 +153,27 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int HW = a.H * g.s.segs_x;  // tiles per image
 
   if (warp == kProdWarp) {
-    // ---------------- producer ----------------
+    // ---------------- producer: one item = (tile, K chunk) ----------------
     if (lane == 0) {
       int it = 0;
-      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int s = it % nst;
-        if (!wait_phase(&empty[s], ((it / nst) & 1) ^ 1) || *(volatile int *)&s_abort) {
-          atomicExch(&s_abort, 1);
-          break;
-        }
+      bool stop = false;
+      for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x) {
         const int b = tile / HW, r = tile - b * HW, y = r / g.s.segs_x, x0 = (r - y * g.s.segs_x) * SW;
-        mbar_arrive_expect_tx(&full[s], (uint32_t)(3 * g8 * rowb));
-        unsigned char *st = sA + s * stage_bytes;
-        for (int j = 0; j < g8; ++j)
-          for (int rr = 0; rr < 3; ++rr)
-            tma_load_4d(st + (3 * j + rr) * rowb, &xmap, a.x_off + j * 8, x0 - 1, y - 1 + rr, b, &full[s]);
-        s_issued = it + 1;
+        for (int c = 0; c < nkc; ++c, ++it) {
+          const int s = it % nst;
+          if (!wait_phase(&empty[s], ((it / nst) & 1) ^ 1) || *(volatile int *)&s_abort) {
+            atomicExch(&s_abort, 1);
+            stop = true;
+            break;
+          }
+          const int gcn = min(kChunkGroups, g8 - c * kChunkGroups);
+          mbar_arrive_expect_tx(&full[s], (uint32_t)(3 * gcn * rowb));
+          unsigned char *st = sA + s * stage_bytes;
+          for (int j = 0; j < gcn; ++j)
+            tma_load_4d(st + 3 * j * rowb, &xmap, 0, x0 / CW - 1, y - 1, b * a.x.cg + a.x.g0 + c * kChunkGroups + j,
+                        &full[s]);
+          s_issued = it + 1;
+        }
       }
     }
   } else if (warp == kMmaWarp) {
@@ -167,34 +182,44 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       const uint32_t idesc = instr_desc_bf16(128, N, false, false);
       // descriptors advance by adding (bytes >> 4) to their address field
       const uint64_t bdesc0 = smem_desc(smem_u32(sW), (N / 8) * 128, 128);
-      const uint32_t bstep = (uint32_t)((N / 8) * 128 * 2) >> 4;  // two K groups of the weights
-      const uint32_t astep = (uint32_t)(2 * 3 * rowb) >> 4;       // two channel groups of the halo
-      int it = 0;
-      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int s = it % nst, acc = it % kEpiGroups;
-        if (!wait_phase(&tempty[acc], ((it / kEpiGroups) & 1) ^ 1) || !wait_phase(&full[s], (it / nst) & 1) ||
-            *(volatile int *)&s_abort) {
+      const uint32_t bgrp = (uint32_t)((N / 8) * 128) >> 4;   // one K group of the weights
+      const uint32_t astep = (uint32_t)(2 * 3 * rowb) >> 4;   // two channel groups of the halo
+      int it = 0, ti = 0;
+      bool stop = false;
+      for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x, ++ti) {
+        const int acc = ti % kEpiGroups;
+        if (!wait_phase(&tempty[acc], ((ti / kEpiGroups) & 1) ^ 1)) {
           atomicExch(&s_abort, 1);
           break;
         }
-        tc_fence_after_sync();
-        const uint64_t adesc0 = smem_desc(smem_u32(sA + s * stage_bytes), 3 * rowb, 128);
         const uint32_t d = tm + acc * acc_cols;
-        uint64_t bd = bdesc0;
         uint32_t accumulate = 0;
-#pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-          uint64_t ad = adesc0 + (uint32_t)((tap / 3) * HP + (tap % 3));  // rows of 16 bytes
-          for (int j = 0; j < g8; j += 2) {
-            mma_bf16(d, ad, bd, idesc, accumulate);
-            accumulate = 1;
-            ad += astep;
-            bd += bstep;
+        for (int c = 0; c < nkc; ++c, ++it) {
+          const int s = it % nst;
+          if (!wait_phase(&full[s], (it / nst) & 1) || *(volatile int *)&s_abort) {
+            atomicExch(&s_abort, 1);
+            stop = true;
+            break;
           }
+          tc_fence_after_sync();
+          const int gcn = min(kChunkGroups, g8 - c * kChunkGroups);
+          const uint64_t adesc0 = smem_desc(smem_u32(sA + s * stage_bytes), 3 * rowb, 128);
+#pragma unroll 1
+          for (int tap = 0; tap < 9; ++tap) {
+            uint64_t ad = adesc0 + (uint32_t)((tap / 3) * HP + CW - 1 + (tap % 3));  // entries of 16 bytes
+            uint64_t bd = bdesc0 + (uint32_t)(tap * g8 + c * kChunkGroups) * bgrp;
+            for (int j = 0; j < gcn; j += 2) {
+              mma_bf16(d, ad, bd, idesc, accumulate);
+              accumulate = 1;
+              ad += astep;
+              bd += 2 * bgrp;
+            }
+          }
+          mma_commit(&empty[s]);
+          s_consumed = it + 1;
         }
-        mma_commit(&empty[s]);
+        if (stop) break;
         mma_commit(&tfull[acc]);
-        s_consumed = it + 1;
       }
     }
   } else {
@@ -213,13 +238,13 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       if (!__shfl_sync(0xffffffffu, go, 0)) break;
       tc_fence_after_sync();
       const int b = tile / HW, r = tile - b * HW, y = r / g.s.segs_x, x = (r - y * g.s.segs_x) * SW + m;
-      const long long p = ((long long)b * a.H + y) * a.W + x;
+      const bool valid = m < SW && x < a.W;
       const uint32_t taddr = tm + wg * acc_cols + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
       for (int c16 = 0; c16 < N / 16; ++c16) {
         uint32_t rr[16];
         tmem_ld16(taddr + c16 * 16, rr);
-        if (m < SW) {
+        if (valid) {
           float v[16];
 #pragma unroll
           for (int kk = 0; kk < 16; ++kk) {
@@ -227,23 +252,22 @@ __global__ void __launch_bounds__(kConvThreads, 2)
             if (a.relu) f = fmaxf(f, 0.0f);
             v[kk] = f;
           }
-          if (a.mask) {
-            const uint4 *mk = reinterpret_cast<const uint4 *>(a.mask + p * a.ldm + a.m_off + n0 + c16 * 16);
-            const uint4 m0 = mk[0], m1 = mk[1];
-            const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&m0);
-            const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&m1);
 #pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
-              if (!(__bfloat162float(mb0[kk]) > 0.0f)) v[kk] = 0.0f;
-              if (!(__bfloat162float(mb1[kk]) > 0.0f)) v[8 + kk] = 0.0f;
+          for (int h = 0; h < 2; ++h) {
+            const int grp = n0 / 8 + 2 * c16 + h;  // group of the output slice
+            if (a.mask.p) {
+              const uint4 mq = *reinterpret_cast<const uint4 *>(a.mask.p + act_index(a.mask, b, grp, y, x, a.H, a.W));
+              const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mq);
+#pragma unroll
+              for (int kk = 0; kk < 8; ++kk)
+                if (!(__bfloat162float(mb[kk]) > 0.0f)) v[8 * h + kk] = 0.0f;
             }
-          }
-          __align__(16) __nv_bfloat16 o[16];
+            __align__(16) __nv_bfloat16 o[8];
 #pragma unroll
-          for (int kk = 0; kk < 16; ++kk) o[kk] = __float2bfloat16_rn(v[kk]);
-          uint4 *dst = reinterpret_cast<uint4 *>(a.y + p * a.ldy + a.y_off + n0 + c16 * 16);
-          dst[0] = reinterpret_cast<const uint4 *>(o)[0];
-          dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+            for (int kk = 0; kk < 8; ++kk) o[kk] = __float2bfloat16_rn(v[8 * h + kk]);
+            *reinterpret_cast<uint4 *>(a.y.p + act_index(a.y, b, grp, y, x, a.H, a.W)) =
+                *reinterpret_cast<const uint4 *>(o);
+          }
         }
       }
       tc_fence_before_sync();
@@ -290,7 +314,7 @@ __global__ void __launch_bounds__(192, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int G8 = CP / 8;          // channel groups of the part
   constexpr int NC = 3 * CP;          // GEMM columns per dx: (group, dy, channel)
-  const int SW = g.s.SW, HP = g.s.HP, nst = g.s.nst;
+  const int SW = g.s.SW, HP = g.s.HP, CW = g.s.CW, nst = g.s.nst;
   const int rowb = HP * 16;
   const int ga = a.cout / 8;
   const int stage_bytes = g.a_bytes + 3 * G8 * rowb;
@@ -332,11 +356,10 @@ __global__ void __launch_bounds__(192, 2)
         unsigned char *st = sm + s * stage_bytes;
         mbar_arrive_expect_tx(&full[s], (uint32_t)(ga * SW * 16 + 3 * G8 * rowb));
         for (int j = 0; j < ga; ++j)
-          tma_load_4d(st + j * SW * 16, &dymap, a.dy_off + j * 8, x0, y, b, &full[s]);
+          tma_load_4d(st + j * SW * 16, &dymap, 0, x0 / CW, y, b * a.dy.cg + a.dy.g0 + j, &full[s]);
         for (int j = 0; j < G8; ++j)
-          for (int rr = 0; rr < 3; ++rr)
-            tma_load_4d(st + g.a_bytes + (3 * j + rr) * rowb, &xmap, a.x_off + c0 + j * 8, x0 - 1, y - 1 + rr, b,
-                        &full[s]);
+          tma_load_4d(st + g.a_bytes + 3 * j * rowb, &xmap, 0, x0 / CW - 1, y - 1, b * a.x.cg + a.x.g0 + c0 / 8 + j,
+                      &full[s]);
         s_issued = it + 1;
       }
     }
@@ -356,7 +379,7 @@ __global__ void __launch_bounds__(192, 2)
         // 256 bytes = 16 in the descriptors' address field.
         const uint64_t adesc0 = smem_desc(a0, 128, SW * 16);
         for (int t = 0; t < g.ndx; ++t) {
-          const uint64_t bdesc0 = smem_desc(b0 + (uint32_t)((dx0 + t) * 16), 128, rowb);
+          const uint64_t bdesc0 = smem_desc(b0 + (uint32_t)((CW - 1 + dx0 + t) * 16), 128, rowb);
           const uint32_t d = tm + t * NC;
           mma_bf16(d, adesc0, bdesc0, idesc, it > 0 ? 1u : 0u);
           for (int k = 1; k < SW / 16; ++k) mma_bf16(d, adesc0 + 16 * k, bdesc0 + 16 * k, idesc, 1u);
@@ -429,17 +452,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// NHWC bf16 activation (pitch ld channels) as a 4-D tensor map {ld, W, H, B}
-// with box {8, box_w, 1, 1}.
-static bool act_map(CUtensorMap *m, const void *base, int B, int H, int W, int ld, int box_w) {
+// A blocked activation buffer as the 4-D tensor {CW * 8 elements, W / CW
+// chunks, H rows, CG * B planes} with box {CW * 8, box_chunks, box_rows, 1}.
+static bool act_map(CUtensorMap *m, const ActView &v, int B, int H, int W, int CW, int box_chunks, int box_rows) {
   auto fn = encode_fn();
   if (!fn) return false;
-  const cuuint64_t dims[4] = {(cuuint64_t)ld, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
-  const cuuint64_t strides[3] = {(cuuint64_t)ld * 2, (cuuint64_t)W * ld * 2, (cuuint64_t)H * W * ld * 2};
-  const cuuint32_t box[4] = {8, (cuuint32_t)box_w, 1, 1};
+  const cuuint64_t dims[4] = {(cuuint64_t)CW * 8, (cuuint64_t)(W / CW), (cuuint64_t)H, (cuuint64_t)v.cg * B};
+  const cuuint64_t strides[3] = {(cuuint64_t)CW * 16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16};
+  const cuuint32_t box[4] = {(cuuint32_t)CW * 8, (cuuint32_t)box_chunks, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, v.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -457,17 +480,17 @@ static int num_sms() {
 constexpr int kSmemCap = 227 * 1024 - 4096;  // dynamic shared memory a CTA may take
 constexpr int kHalfSm = 110 * 1024;          // two CTAs per SM
 
-// Segment width: the whole row up to 128 pixels, a multiple of 16 dividing W.
-static int seg_width(int W) {
-  if (W % 16 != 0) return 0;
-  return W >= 128 ? (W % 128 == 0 ? 128 : 0) : W;
-}
-
+// Segments: 128 pixels, or the whole row rounded up to 16 for narrower
+// images. Chunks: 16 pixels, or the largest power of two dividing W. The halo
+// row spans one chunk left of the segment to at least one pixel past it,
+// rounded up to 8 entries so that every row starts on a 128-byte boundary.
 static SegGeom seg_geom(int B, int H, int W) {
   SegGeom s{};
-  s.SW = seg_width(W);
-  s.HP = s.SW + 8;
-  s.segs_x = s.SW ? W / s.SW : 0;
+  s.SW = W >= 128 ? 128 : (W + 15) / 16 * 16;
+  s.CW = 16;
+  while (W % s.CW) s.CW >>= 1;
+  s.HP = (s.SW + 2 * s.CW + 7) / 8 * 8;
+  s.segs_x = (W + s.SW - 1) / s.SW;
   s.nseg = B * H * s.segs_x;
   return s;
 }
@@ -480,26 +503,21 @@ static int conv_part(int n, int cin) {
   return 0;
 }
 
-bool conv_tma_ok(const ConvArgs &a, int n) {
-  return seg_width(a.W) != 0 && a.cin % 16 == 0 && a.cin <= 256 && conv_part(n, a.cin) != 0 &&
-         encode_fn() != nullptr;
-}
-
 template <int NP>
 static cudaError_t launch_conv_tma_t(const ConvArgs &a, int parts, cudaStream_t st) {
   ConvTmaGeom g{};
   g.s = seg_geom(a.B, a.H, a.W);
   CUtensorMap xm;
-  if (!act_map(&xm, a.x, a.B, a.H, a.W, a.ldx, g.s.HP)) return cudaErrorNotSupported;
+  if (!act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, 3)) return cudaErrorInvalidValue;
   g.w_bytes = (NP * 9 * a.cin * 2 + 1023) / 1024 * 1024;
-  const int stage = 3 * (a.cin / 8) * g.s.HP * 16;
+  const int stage = 3 * std::min(a.cin / 8, kChunkGroups) * g.s.HP * 16;
   // two CTAs per SM when that leaves at least 3 stages each, else one CTA
   // with the deepest ring that fits
   int per_sm = 2, budget = kHalfSm - kTail;
   if ((budget - g.w_bytes) / stage < 3) per_sm = 1, budget = kSmemCap - kTail;
   g.s.nst = (budget - g.w_bytes) / stage;
   if (g.s.nst > kMaxStages) g.s.nst = kMaxStages;
-  if (g.s.nst < 2) return cudaErrorNotSupported;
+  if (g.s.nst < 2) return cudaErrorInvalidValue;
   const int smem = g.w_bytes + g.s.nst * stage + kTail;
   cudaError_t e = cudaFuncSetAttribute(k_conv_tma<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
@@ -510,26 +528,25 @@ static cudaError_t launch_conv_tma_t(const ConvArgs &a, int parts, cudaStream_t 
   return cudaGetLastError();
 }
 
-cudaError_t launch_conv_tma(const ConvArgs &a, int n, cudaStream_t st) {
+cudaError_t launch_conv3x3(const ConvArgs &a, int n, cudaStream_t st) {
+  if (a.cin % 16 != 0 || a.cin > 256 || a.W < 1 || a.H < 1 || a.B < 1) return cudaErrorInvalidValue;
   const int p = conv_part(n, a.cin);
-  if (!p) return cudaErrorNotSupported;
   switch (p) {
     case 16: return launch_conv_tma_t<16>(a, n / p, st);
     case 32: return launch_conv_tma_t<32>(a, n / p, st);
     case 48: return launch_conv_tma_t<48>(a, n / p, st);
     case 64: return launch_conv_tma_t<64>(a, n / p, st);
     case 96: return launch_conv_tma_t<96>(a, n / p, st);
-    default: return cudaErrorNotSupported;
+    default: return cudaErrorInvalidValue;
   }
 }
 
-// Partial-sum chunks of the TMA weight-gradient path: a fixed count, so the
-// order of the final sum does not depend on the device.
+// Partial-sum chunks of the weight gradient: a fixed count, so the order of
+// the final sum does not depend on the device.
 constexpr int kWgChunks = 296;
 
-int wgrad_tma_chunks(int B, int H, int W) {
+int wgrad_chunks(int B, int H, int W) {
   const SegGeom s = seg_geom(B, H, W);
-  if (!s.SW) return 0;
   const int per = (s.nseg + kWgChunks - 1) / kWgChunks;
   return (s.nseg + per - 1) / per;
 }
@@ -542,19 +559,14 @@ static int wgrad_part(int cin) {
   return 0;
 }
 
-bool wgrad_tma_ok(const WgradArgs &a, int cin) {
-  if (seg_width(a.W) == 0 || a.cout % 8 != 0 || a.cout > 128) return false;
-  const int p = wgrad_part(cin);
-  return (p == 16 || p == 32 || p == 48 || p == 64) && encode_fn() != nullptr;
-}
-
 template <int CP>
 static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *chunks) {
   WgradTmaGeom g{};
   g.s = seg_geom(a.B, a.H, a.W);
   CUtensorMap dym, xm;
-  if (!act_map(&dym, a.dy, a.B, a.H, a.W, a.lddy, g.s.SW) || !act_map(&xm, a.x, a.B, a.H, a.W, a.ldx, g.s.HP))
-    return cudaErrorNotSupported;
+  if (!act_map(&dym, a.dy, a.B, a.H, a.W, g.s.CW, g.s.SW / g.s.CW, 1) ||
+      !act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, 3))
+    return cudaErrorInvalidValue;
   g.seg_per_chunk = (g.s.nseg + kWgChunks - 1) / kWgChunks;
   const int nchunks = (g.s.nseg + g.seg_per_chunk - 1) / g.seg_per_chunk;
   g.ndx = (9 * CP <= 256) ? 3 : 1;
@@ -569,7 +581,7 @@ static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *
   g.s.nst = (kHalfSm - tail) / stage;
   if (g.s.nst < 3) g.s.nst = (kSmemCap - tail) / stage;
   if (g.s.nst > kMaxStages) g.s.nst = kMaxStages;
-  if (g.s.nst < 2) return cudaErrorNotSupported;
+  if (g.s.nst < 2) return cudaErrorInvalidValue;
   int smem = g.s.nst * stage + tail;
   // at most two CTAs per SM when each holds 256 TMEM columns
   if (pow2_cols(g.ndx * 3 * CP) >= 256 && smem < 80 * 1024) smem = 80 * 1024;
@@ -580,14 +592,19 @@ static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *
   return cudaGetLastError();
 }
 
-cudaError_t launch_wgrad_tma(const WgradArgs &a, int cin, cudaStream_t st, int *chunks) {
-  switch (wgrad_part(cin)) {
-    case 16: return launch_wgrad_tma_t<16>(a, st, chunks);
-    case 32: return launch_wgrad_tma_t<32>(a, st, chunks);
-    case 48: return launch_wgrad_tma_t<48>(a, st, chunks);
-    case 64: return launch_wgrad_tma_t<64>(a, st, chunks);
-    default: return cudaErrorNotSupported;
+cudaError_t launch_wgrad(const WgradArgs &a, cudaStream_t st) {
+  if (a.cout % 8 != 0 || a.cout > 128 || a.cin % 16 != 0 || a.W < 1) return cudaErrorInvalidValue;
+  int chunks = 0;
+  cudaError_t e;
+  switch (wgrad_part(a.cin)) {
+    case 16: e = launch_wgrad_tma_t<16>(a, st, &chunks); break;
+    case 32: e = launch_wgrad_tma_t<32>(a, st, &chunks); break;
+    case 48: e = launch_wgrad_tma_t<48>(a, st, &chunks); break;
+    case 64: e = launch_wgrad_tma_t<64>(a, st, &chunks); break;
+    default: return cudaErrorInvalidValue;
   }
+  if (e != cudaSuccess) return e;
+  return launch_wgrad_reduce(a.part, chunks, a.cout, a.cin, a.dw, st);
 }
 
 }  // namespace unet

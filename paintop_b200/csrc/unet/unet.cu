@@ -17,7 +17,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -123,8 +122,7 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
   size_t maxch = 0;
   for (int l = 0; l < 14; ++l) {
     const int lev = (l <= 1 || l >= 12) ? 0 : (l <= 3 || l >= 10) ? 1 : (l <= 5 || l >= 8) ? 2 : 3;
-    int ch = wgrad_chunks(B, H >> lev, W >> lev);
-    ch = std::max(ch, wgrad_tma_chunks(B, H >> lev, W >> lev));
+    const int ch = wgrad_chunks(B, H >> lev, W >> lev);
     const size_t need = (size_t)ch * 9 * kLayers[l].cout * kLayers[l].cin;
     if (need > maxch) maxch = need;
   }
@@ -153,66 +151,42 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
   return cudaMemset(n->err, 0, sizeof(int)) == cudaSuccess ? PT_OK : PT_LAUNCH_FAILED;
 }
 
-// The TMA halo kernels serve layers whose width is a multiple of 128;
-// PAINTOP_UNET_TMA=0 routes every layer through the gather kernels instead.
-bool tma_enabled() {
-  const char *e = std::getenv("PAINTOP_UNET_TMA");
-  return !(e && e[0] == '0');
-}
-
-cudaError_t launch_conv_any(const ConvArgs &a, int n, cudaStream_t st) {
-  if (tma_enabled() && conv_tma_ok(a, n)) {
-    const cudaError_t e = launch_conv_tma(a, n, st);
-    if (e != cudaErrorNotSupported) return e;
-  }
-  return launch_conv3x3(a, n, st);
-}
+// A channel slice [off, ...) of a buffer (off a multiple of 8).
+ActView view(const Act &t, int off = 0) { return ActView{t.p, t.c / 8, off / 8}; }
 
 pt_status conv(pt_unet *n, int l, const Act &x, int x_off, const Act &y, int y_off, bool relu) {
   ConvArgs a{};
-  a.x = x.p; a.ldx = x.c; a.x_off = x_off; a.cin = kLayers[l].cin;
+  a.x = view(x, x_off); a.cin = kLayers[l].cin;
   a.w = n->wbf + n->wb_off[l];
   a.bias = n->params + n->b_off[l];
-  a.y = y.p; a.ldy = y.c; a.y_off = y_off; a.relu = relu ? 1 : 0;
+  a.y = view(y, y_off); a.relu = relu ? 1 : 0;
   a.B = n->B; a.H = n->H >> x.level; a.W = n->W >> x.level; a.err = n->err;
-  CK(launch_conv_any(a, kLayers[l].cout, n->ctx->stream), "conv forward");
+  CK(launch_conv3x3(a, kLayers[l].cout, n->ctx->stream), "conv forward");
   return PT_OK;
 }
 
 // dX = conv(dY, W') (times the ReLU mask of X when `mask` is given)
 pt_status dgrad(pt_unet *n, int l, const Act &dy, const Act &dx, int dx_off, const Act *mask, int m_off) {
   ConvArgs a{};
-  a.x = dy.p; a.ldx = dy.c; a.x_off = 0; a.cin = kLayers[l].cout;
+  a.x = view(dy); a.cin = kLayers[l].cout;
   a.w = n->wbf + n->wt_off[l];
   a.bias = nullptr;
-  a.y = dx.p; a.ldy = dx.c; a.y_off = dx_off; a.relu = 0;
-  if (mask) { a.mask = mask->p; a.ldm = mask->c; a.m_off = m_off; }
+  a.y = view(dx, dx_off); a.relu = 0;
+  if (mask) a.mask = view(*mask, m_off);
   a.B = n->B; a.H = n->H >> dy.level; a.W = n->W >> dy.level; a.err = n->err;
-  CK(launch_conv_any(a, kLayers[l].cin, n->ctx->stream), "conv backward-data");
+  CK(launch_conv3x3(a, kLayers[l].cin, n->ctx->stream), "conv backward-data");
   return PT_OK;
 }
 
 // dW (into grad) from dY (pre-activation) and the forward input x; db = colsum(dY)
 pt_status wgrad(pt_unet *n, int l, const Act &dy, const Act &x, int x_off) {
   WgradArgs a{};
-  a.dy = dy.p; a.lddy = dy.c; a.dy_off = 0; a.cout = kLayers[l].cout;
-  a.x = x.p; a.ldx = x.c; a.x_off = x_off; a.cin = kLayers[l].cin;
+  a.dy = view(dy); a.cout = kLayers[l].cout;
+  a.x = view(x, x_off); a.cin = kLayers[l].cin;
   a.B = n->B; a.H = n->H >> dy.level; a.W = n->W >> dy.level;
   a.part = n->wpart; a.dw = n->grad + n->w_off[l]; a.err = n->err;
-  bool done = false;
-  if (tma_enabled() && wgrad_tma_ok(a, kLayers[l].cin)) {
-    int chunks = 0;
-    const cudaError_t e = launch_wgrad_tma(a, kLayers[l].cin, n->ctx->stream, &chunks);
-    if (e == cudaSuccess) {
-      CK(launch_wgrad_reduce(a.part, chunks, a.cout, kLayers[l].cin, a.dw, n->ctx->stream), "weight reduce");
-      done = true;
-    } else if (e != cudaErrorNotSupported) {
-      return cfail(n, e, "conv backward-weights");
-    }
-  }
-  if (!done) CK(launch_wgrad(a, kLayers[l].cin, n->ctx->stream), "conv backward-weights");
-  CK(launch_colsum(dy.p, dy.c, 0, kLayers[l].cout, npix(n, dy.level), n->cpart, n->grad + n->b_off[l],
-                   n->ctx->stream),
+  CK(launch_wgrad(a, n->ctx->stream), "conv backward-weights");
+  CK(launch_colsum(view(dy), kLayers[l].cout / 8, a.B, a.H, a.W, n->cpart, n->grad + n->b_off[l], n->ctx->stream),
      "bias gradient");
   return PT_OK;
 }
@@ -226,28 +200,29 @@ pt_status wgrad(pt_unet *n, int l, const Act &dy, const Act &x, int x_off) {
 pt_status forward(pt_unet *n, const float *features) {
   cudaStream_t st = n->ctx->stream;
   const long long P0 = npix(n, 0);
-  CK(launch_features_to_input(features, n->X0.p, P0, st), "input");
+  (void)P0;
+  CK(launch_features_to_input(features, view(n->X0), n->B, n->H, n->W, st), "input");
   RET(conv(n, 0, n->X0, 0, n->E0a, 0, true));
   RET(conv(n, 1, n->E0a, 0, n->CAT0, 32, true));  // e0 -> skip slice
-  CK(launch_avgpool2(n->CAT0.p, 48, 32, n->P1.p, 16, 0, n->B, n->H, n->W, 16, st), "pool");
+  CK(launch_avgpool2(view(n->CAT0, 32), view(n->P1), n->B, n->H, n->W, 2, st), "pool");
   RET(conv(n, 2, n->P1, 0, n->E1a, 0, true));
   RET(conv(n, 3, n->E1a, 0, n->CAT1, 64, true));  // e1
-  CK(launch_avgpool2(n->CAT1.p, 96, 64, n->P2.p, 32, 0, n->B, n->H >> 1, n->W >> 1, 32, st), "pool");
+  CK(launch_avgpool2(view(n->CAT1, 64), view(n->P2), n->B, n->H >> 1, n->W >> 1, 4, st), "pool");
   RET(conv(n, 4, n->P2, 0, n->E2a, 0, true));
   RET(conv(n, 5, n->E2a, 0, n->CAT2, 128, true));  // e2
-  CK(launch_avgpool2(n->CAT2.p, 192, 128, n->P3.p, 64, 0, n->B, n->H >> 2, n->W >> 2, 64, st), "pool");
+  CK(launch_avgpool2(view(n->CAT2, 128), view(n->P3), n->B, n->H >> 2, n->W >> 2, 8, st), "pool");
   RET(conv(n, 6, n->P3, 0, n->E3a, 0, true));
   RET(conv(n, 7, n->E3a, 0, n->E3, 0, true));
-  CK(launch_upsample2(n->E3.p, 128, 0, n->CAT2.p, 192, 0, n->B, n->H >> 3, n->W >> 3, 128, st), "up");
+  CK(launch_upsample2(view(n->E3), view(n->CAT2), n->B, n->H >> 3, n->W >> 3, 16, st), "up");
   RET(conv(n, 8, n->CAT2, 0, n->D2a, 0, true));
   RET(conv(n, 9, n->D2a, 0, n->D2, 0, true));
-  CK(launch_upsample2(n->D2.p, 64, 0, n->CAT1.p, 96, 0, n->B, n->H >> 2, n->W >> 2, 64, st), "up");
+  CK(launch_upsample2(view(n->D2), view(n->CAT1), n->B, n->H >> 2, n->W >> 2, 8, st), "up");
   RET(conv(n, 10, n->CAT1, 0, n->D1a, 0, true));
   RET(conv(n, 11, n->D1a, 0, n->D1, 0, true));
-  CK(launch_upsample2(n->D1.p, 32, 0, n->CAT0.p, 48, 0, n->B, n->H >> 1, n->W >> 1, 32, st), "up");
+  CK(launch_upsample2(view(n->D1), view(n->CAT0), n->B, n->H >> 1, n->W >> 1, 4, st), "up");
   RET(conv(n, 12, n->CAT0, 0, n->D0a, 0, true));
   RET(conv(n, 13, n->D0a, 0, n->D0, 0, true));
-  CK(launch_head_fwd(n->D0.p, 16, kHeadIn, n->params + n->head_w, n->params + n->head_b, n->pred, P0, st),
+  CK(launch_head_fwd(view(n->D0), n->params + n->head_w, n->params + n->head_b, n->pred, n->B, n->H, n->W, st),
      "head");
   return PT_OK;
 }
@@ -258,7 +233,7 @@ pt_status backward(pt_unet *n, const float *target, const float *mask, double *l
   const int nlb = loss_blocks(P0);
   CK(launch_loss(n->pred, target, mask, P0, n->dpred, n->lpart, n->count, st), "loss");
   // head
-  CK(launch_head_bwd(n->D0.p, 16, kHeadIn, n->params + n->head_w, n->dpred, P0, n->dD0.p, 16, n->cpart, st),
+  CK(launch_head_bwd(view(n->D0), n->params + n->head_w, n->dpred, view(n->dD0), n->B, n->H, n->W, n->cpart, st),
      "head backward");
   // the head partials [blocks][17], in block order, into grad[head_w .. head_b]
   CK(launch_reduce_rows(n->cpart, head_bwd_blocks(P0), kHeadIn + 1, n->grad + n->head_w, st), "head reduce");
@@ -268,43 +243,41 @@ pt_status backward(pt_unet *n, const float *target, const float *mask, double *l
   RET(dgrad(n, 13, n->dD0, n->dD0a, 0, &n->D0a, 0));
   RET(wgrad(n, 12, n->dD0a, n->CAT0, 0));
   RET(dgrad(n, 12, n->dD0a, n->dCAT0, 0, nullptr, 0));
-  CK(launch_upsample2_bwd(n->dCAT0.p, 48, 0, n->D1.p, 32, 0, n->dD1.p, 32, 0, B, H >> 1, W >> 1, 32, st), "up bwd");
+  CK(launch_upsample2_bwd(view(n->dCAT0), view(n->D1), view(n->dD1), B, H >> 1, W >> 1, 4, st), "up bwd");
   // decoder level 1
   RET(wgrad(n, 11, n->dD1, n->D1a, 0));
   RET(dgrad(n, 11, n->dD1, n->dD1a, 0, &n->D1a, 0));
   RET(wgrad(n, 10, n->dD1a, n->CAT1, 0));
   RET(dgrad(n, 10, n->dD1a, n->dCAT1, 0, nullptr, 0));
-  CK(launch_upsample2_bwd(n->dCAT1.p, 96, 0, n->D2.p, 64, 0, n->dD2.p, 64, 0, B, H >> 2, W >> 2, 64, st), "up bwd");
+  CK(launch_upsample2_bwd(view(n->dCAT1), view(n->D2), view(n->dD2), B, H >> 2, W >> 2, 8, st), "up bwd");
   // decoder level 2
   RET(wgrad(n, 9, n->dD2, n->D2a, 0));
   RET(dgrad(n, 9, n->dD2, n->dD2a, 0, &n->D2a, 0));
   RET(wgrad(n, 8, n->dD2a, n->CAT2, 0));
   RET(dgrad(n, 8, n->dD2a, n->dCAT2, 0, nullptr, 0));
-  CK(launch_upsample2_bwd(n->dCAT2.p, 192, 0, n->E3.p, 128, 0, n->dE3.p, 128, 0, B, H >> 3, W >> 3, 128, st),
-     "up bwd");
+  CK(launch_upsample2_bwd(view(n->dCAT2), view(n->E3), view(n->dE3), B, H >> 3, W >> 3, 16, st), "up bwd");
   // bottleneck
   RET(wgrad(n, 7, n->dE3, n->E3a, 0));
   RET(dgrad(n, 7, n->dE3, n->dE3a, 0, &n->E3a, 0));
   RET(wgrad(n, 6, n->dE3a, n->P3, 0));
   RET(dgrad(n, 6, n->dE3a, n->dP3, 0, nullptr, 0));
-  CK(launch_unpool_add_mask(n->dCAT2.p, 192, 128, n->dP3.p, 64, 0, n->CAT2.p, 192, 128, n->de2.p, 64, 0, B,
-                            H >> 2, W >> 2, 64, st),
+  CK(launch_unpool_add_mask(view(n->dCAT2, 128), view(n->dP3), view(n->CAT2, 128), view(n->de2), B, H >> 2,
+                            W >> 2, 8, st),
      "unpool");
   // encoder level 2
   RET(wgrad(n, 5, n->de2, n->E2a, 0));
   RET(dgrad(n, 5, n->de2, n->dE2a, 0, &n->E2a, 0));
   RET(wgrad(n, 4, n->dE2a, n->P2, 0));
   RET(dgrad(n, 4, n->dE2a, n->dP2, 0, nullptr, 0));
-  CK(launch_unpool_add_mask(n->dCAT1.p, 96, 64, n->dP2.p, 32, 0, n->CAT1.p, 96, 64, n->de1.p, 32, 0, B, H >> 1,
-                            W >> 1, 32, st),
+  CK(launch_unpool_add_mask(view(n->dCAT1, 64), view(n->dP2), view(n->CAT1, 64), view(n->de1), B, H >> 1,
+                            W >> 1, 4, st),
      "unpool");
   // encoder level 1
   RET(wgrad(n, 3, n->de1, n->E1a, 0));
   RET(dgrad(n, 3, n->de1, n->dE1a, 0, &n->E1a, 0));
   RET(wgrad(n, 2, n->dE1a, n->P1, 0));
   RET(dgrad(n, 2, n->dE1a, n->dP1, 0, nullptr, 0));
-  CK(launch_unpool_add_mask(n->dCAT0.p, 48, 32, n->dP1.p, 16, 0, n->CAT0.p, 48, 32, n->de0.p, 16, 0, B, H, W, 16,
-                            st),
+  CK(launch_unpool_add_mask(view(n->dCAT0, 32), view(n->dP1), view(n->CAT0, 32), view(n->de0), B, H, W, 2, st),
      "unpool");
   // encoder level 0
   RET(wgrad(n, 1, n->de0, n->E0a, 0));

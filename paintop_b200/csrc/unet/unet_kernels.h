@@ -1,4 +1,11 @@
-// unet_kernels.h -- launch interface of the U-Net kernels (unet_kernels.cu).
+// unet_kernels.h -- launch interface of the U-Net kernels (unet_kernels.cu,
+// conv_tma.cu).
+//
+// Activations are bf16 in a channel-blocked layout [B][C/8][H][W][8]: one
+// plane per group of 8 channels, so a row of one plane is contiguous (16
+// bytes per pixel) and the tensor-memory-accelerator (TMA) loads a run of
+// pixels of one plane as a single wide line. A channel slice of a buffer (the
+// decoder's concatenations write into slices) is a range of planes.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -6,78 +13,70 @@
 
 namespace unet {
 
+// A channel slice of a blocked activation buffer.
+struct ActView {
+  __nv_bfloat16 *p;  // buffer base
+  int cg;            // 8-channel groups of the whole buffer
+  int g0;            // first group of the slice
+};
+
+// Element index of (image b, slice group g, row y, column x, channel 0 of the group).
+__host__ __device__ __forceinline__ long long act_index(const ActView &v, int b, int g, int y, int x, int H,
+                                                        int W) {
+  return ((((long long)b * v.cg + v.g0 + g) * H + y) * W + x) * 8;
+}
+
 // 3x3 convolution (forward, or backward-data with flipped weights).
 struct ConvArgs {
-  const __nv_bfloat16 *x;  // input, NHWC, row pitch ldx channels, first channel x_off
-  int ldx, x_off, cin;     // cin: channels read (multiple of 16)
+  ActView x;               // input slice
+  int cin;                 // its channels (multiple of 16)
   const __nv_bfloat16 *w;  // [N][9][cin] bf16
   const float *bias;       // [N] or nullptr
-  __nv_bfloat16 *y;        // output, NHWC, pitch ldy, first channel y_off
-  int ldy, y_off;
+  ActView y;               // output slice (N channels)
   int relu;                // apply max(0, .) after the bias
-  const __nv_bfloat16 *mask;  // optional: zero outputs where mask <= 0 (ReLU backward)
-  int ldm, m_off;
+  ActView mask;            // mask.p != nullptr: zero outputs where mask <= 0 (ReLU backward)
   int B, H, W;
   int *err;                // set to 1 if a bounded wait gave up
 };
 
-// How a convolution's reduction axis (9 taps x cin channels) is cut into
-// pipeline chunks (unet_kernels.cu states the rule).
-struct ConvChunking {
-  int kc;       // channels per part
-  int cpt;      // channel parts
-  int tpc;      // taps per chunk
-  int ntg;      // tap groups
-  int nchunks;  // ntg * cpt
-  int kmax;     // K elements of the largest chunk
-  int stages;   // pipeline stages in shared memory
-};
-
 // 3x3 convolution backward-weights.
 struct WgradArgs {
-  const __nv_bfloat16 *dy;  // output gradient (pre-activation), pitch lddy, offset dy_off
-  int lddy, dy_off, cout;   // cout <= 128, multiple of 8
-  const __nv_bfloat16 *x;   // forward input, pitch ldx, offset x_off
-  int ldx, x_off;
-  int cin;                  // input channels (the TMA path reads it; the gather path takes it as an argument)
+  ActView dy;               // output gradient (pre-activation)
+  int cout;                 // cout <= 128, multiple of 8
+  ActView x;                // forward input
+  int cin;                  // multiple of 16
   int B, H, W;
   float *part;              // [chunks][9][cout][cin] partials
   float *dw;                // [cout][9][cin] result
   int *err;
 };
 
+// conv_tma.cu
 cudaError_t launch_conv3x3(const ConvArgs &a, int n, cudaStream_t st);
-// TMA halo path (conv_tma.cu) for widths that are multiples of 128; the
-// launchers return cudaErrorNotSupported when a tensor map cannot be built.
-bool conv_tma_ok(const ConvArgs &a, int n);
-cudaError_t launch_conv_tma(const ConvArgs &a, int n, cudaStream_t st);
-bool wgrad_tma_ok(const WgradArgs &a, int cin);
-int wgrad_tma_chunks(int B, int H, int W);
-cudaError_t launch_wgrad_tma(const WgradArgs &a, int cin, cudaStream_t st, int *chunks);
-cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st);
-int wgrad_chunks(int B, int H, int W);
-cudaError_t launch_wgrad(const WgradArgs &a, int cin, cudaStream_t st);
-int colsum_parts(long long P);
+int wgrad_chunks(int B, int H, int W);  // partial-sum chunks launch_wgrad writes
+cudaError_t launch_wgrad(const WgradArgs &a, cudaStream_t st);
+
+// unet_kernels.cu
 // out[j] = sum over k = 0 .. nparts-1 (in order) of part[k][j], j < c
 cudaError_t launch_reduce_rows(const float *part, int nparts, int c, float *out, cudaStream_t st);
-cudaError_t launch_colsum(const __nv_bfloat16 *dy, int ld, int off, int c, long long P, float *part,
-                          float *out, cudaStream_t st);
-cudaError_t launch_avgpool2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bfloat16 *out, int ldo, int ooff,
-                            int B, int H, int W, int c, cudaStream_t st);
-cudaError_t launch_unpool_add_mask(const __nv_bfloat16 *dskip, int lds, int soff, const __nv_bfloat16 *dpool,
-                                   int ldp, int poff, const __nv_bfloat16 *act, int lda, int aoff,
-                                   __nv_bfloat16 *out, int ldo, int ooff, int B, int H, int W, int c,
-                                   cudaStream_t st);
-cudaError_t launch_upsample2(const __nv_bfloat16 *in, int ldi, int ioff, __nv_bfloat16 *out, int ldo, int ooff,
-                             int B, int Hi, int Wi, int c, cudaStream_t st);
-cudaError_t launch_upsample2_bwd(const __nv_bfloat16 *dout, int ldd, int doff, const __nv_bfloat16 *act, int lda,
-                                 int aoff, __nv_bfloat16 *din, int ldo, int ooff, int B, int Hi, int Wi, int c,
-                                 cudaStream_t st);
-cudaError_t launch_head_fwd(const __nv_bfloat16 *x, int ldx, int c, const float *w, const float *b, float *pred,
-                            long long P, cudaStream_t st);
+cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st);
+int colsum_parts(long long P);
+cudaError_t launch_colsum(const ActView &dy, int groups, int B, int H, int W, float *part, float *out,
+                          cudaStream_t st);
+cudaError_t launch_avgpool2(const ActView &in, const ActView &out, int B, int H, int W, int groups,
+                            cudaStream_t st);
+cudaError_t launch_unpool_add_mask(const ActView &dskip, const ActView &dpool, const ActView &act,
+                                   const ActView &out, int B, int H, int W, int groups, cudaStream_t st);
+cudaError_t launch_upsample2(const ActView &in, const ActView &out, int B, int Hi, int Wi, int groups,
+                             cudaStream_t st);
+cudaError_t launch_upsample2_bwd(const ActView &dout, const ActView &act, const ActView &din, int B, int Hi,
+                                 int Wi, int groups, cudaStream_t st);
+// 1x1 head on 16 channels (2 groups)
+cudaError_t launch_head_fwd(const ActView &x, const float *w, const float *b, float *pred, int B, int H, int W,
+                            cudaStream_t st);
 int head_bwd_blocks(long long P);
-cudaError_t launch_head_bwd(const __nv_bfloat16 *x, int ldx, int c, const float *w, const float *dpred,
-                            long long P, __nv_bfloat16 *dx, int lddx, float *part, cudaStream_t st);
+cudaError_t launch_head_bwd(const ActView &x, const float *w, const float *dpred, const ActView &dx, int B, int H,
+                            int W, float *part, cudaStream_t st);
 int loss_blocks(long long P);
 // count: 1 + loss_blocks(P) floats of scratch; count[0] receives the interior count
 cudaError_t launch_loss(const float *pred, const float *target, const float *mask, long long P, float *dpred,
@@ -86,7 +85,8 @@ cudaError_t launch_adam(float *w, float *m, float *v, const float *g, __nv_bfloa
                         int step, cudaStream_t st);
 cudaError_t launch_prep_weights(const float *w, int cout, int cin, __nv_bfloat16 *wb, __nv_bfloat16 *wt,
                                 cudaStream_t st);
-cudaError_t launch_features_to_input(const float *f, __nv_bfloat16 *x, long long P, cudaStream_t st);
+// fp32 features (B x H x W x 4) -> the 16-channel input (2 groups, channels 4..15 zero)
+cudaError_t launch_features_to_input(const float *f, const ActView &x, int B, int H, int W, cudaStream_t st);
 cudaError_t launch_features(const float *guid, const float *anchor, const float *mask, int B, int H, int W,
                             float *f, cudaStream_t st);
 // Warm start at another resolution: pool interleaved inputs by s into a
