@@ -2,40 +2,42 @@
 // TMA halo loads, on activations in the channel-blocked layout
 // [B][C/8][H][W][8] (unet_kernels.h).
 //
-// Tiling. A tile is one segment of SW pixels of one image row: SW = 128, or
-// W rounded up to 16 for narrower images; a row's last segment may reach past
-// W (those pixels load as zero and are never stored). TMA sees a plane row as
-// W / CW chunks of CW pixels (CW = 16, or the largest power of two dividing W
-// when W is not a multiple of 16): a 4-D tensor {CW * 8 elements, W / CW
-// chunks, H rows, C/8 * B planes}. For channel group g one box of {CW * 8, HP
-// / CW chunks, 3 rows} starting one chunk left of the segment and one row
-// above it lands in shared memory as 3 rows of HP 16-byte entries (one entry =
-// one pixel's 8 channels), each row one contiguous line per chunk; pixels
-// outside the image read as zero, the convolution's zero padding. Entry CW of
-// a row is pixel x0. Row (g, r) sits at (3g + r) * HP entries. In the
-// canonical no-swizzle layout consecutive 16-byte entries are consecutive
-// core-matrix rows along M (K-major operand) or K (MN-major operand), so the
-// operand of tap (dy, dx) for output pixel m is entry
-// (3g + 1 + dy) * HP + CW + dx + m: a shift of the descriptor's start address
-// by 16 bytes per pixel. One halo tile feeds all nine taps.
+// Tiling. A tile is R output rows (R = 1, 2 or 4) of one segment of SW pixels:
+// SW = 128, or W rounded up to 16 for narrower images; a row's last segment
+// may reach past W and the last row group past H (those pixels load as zero
+// and are never stored). TMA sees a buffer as the 5-D tensor {CW * 8 elements,
+// W / CW chunks, H rows, C/8 planes, B}: a plane row in chunks of CW pixels
+// (CW = 16, or the largest power of two dividing W). One box {CW * 8, HP / CW
+// chunks, R + 2 rows, planes, 1} starting one chunk left of the segment and
+// one row above it brings the tile's whole halo: in shared memory, for each
+// channel group g and halo row h, a row of HP 16-byte entries (one entry =
+// one pixel's 8 channels) at entry (g * (R + 2) + h) * HP, entry CW being
+// pixel x0. Pixels outside the image read as zero, the convolution's zero
+// padding. In the canonical no-swizzle layout consecutive 16-byte entries are
+// consecutive core-matrix rows along M (K-major operand) or K (MN-major
+// operand), so the operand of tap (dy, dx) for output row r and pixel m is
+// entry (g * (R + 2) + r + 1 + dy) * HP + CW + dx + m: a shift of the
+// descriptor's start address by 16 bytes per pixel. One halo tile feeds all
+// nine taps of all R rows.
 //
-// k_conv_tma<N> (forward / backward-data): GEMM rows = the segment's pixels
-// (M = 128; rows past SW are never stored), columns = N output channels (the
-// CTA's part [n0, n0 + N) of them: blockIdx.y), K = (tap, channel) taken in
-// chunks of up to 64 channels per pipeline stage: K groups (g, g+1) of one
-// tap are 3 * HP entries apart. The CTA's weights stay resident in shared
+// k_conv_tma<N> (forward / backward-data): per output row, GEMM rows = the
+// segment's pixels (M = 128; rows past SW are never stored), columns = N
+// output channels (the CTA's part [n0, n0 + N) of them: blockIdx.y), K = (tap,
+// channel) taken in chunks of up to 64 channels per pipeline stage: K groups
+// (g, g+1) of one tap are (R + 2) * HP entries apart. The CTA's weights stay resident in shared
 // memory. Roles: one warp's lane 0 issues TMA loads into a ring of stages
 // (full/empty mbarriers); one warp allocates TMEM and its lane 0 issues the
 // MMAs into one accumulator per epilogue warpgroup; two warpgroups take
 // alternate tiles through the epilogue (bias, ReLU, ReLU mask -> bf16).
 //
-// k_wgrad_tma<CP> (backward-weights): D[co][tap][ci] += sum over the segment's
-// pixels of dY[p][co] X[p + off(tap)][ci]. GEMM rows = output channels
-// (padded to 128: rows past cout read whatever follows in shared memory and
-// are never stored), K = pixels, and columns = (channel group, dy, channel):
-// the halo rows of one part of CP channels are 3 * CP / 8 groups of 8 columns
-// at a constant stride of HP entries, so one MMA covers the three dy taps of
-// that part (N = 3 CP) and dx selects the start entry. A CTA owns a fixed
+// k_wgrad_tma<CP> (backward-weights, R = 1): D[co][tap][ci] += sum over the
+// segment's pixels of dY[p][co] X[p + off(tap)][ci]. GEMM rows = output
+// channels (padded to 128: rows past cout read whatever follows in shared
+// memory and are never stored), K = pixels, and columns = (channel group, dy,
+// channel): with one output row the halo rows of one part of CP channels are
+// 3 * CP / 8 groups of 8 columns at a constant stride of HP entries, so one
+// MMA covers the three dy taps of that part (N = 3 CP) and dx selects the
+// start entry. A CTA owns a fixed
 // range of segments, one part of the channels and one or all three dx values,
 // accumulates in TMEM and writes one fp32 partial per (tap, co, ci); the
 // partials are summed in chunk order by k_wgrad_reduce.
@@ -83,7 +85,9 @@ __host__ __device__ inline uint32_t pow2_cols(int n) {
 // Segment geometry shared by both kernels.
 struct SegGeom {
   int SW, CW, HP;       // segment width, TMA chunk width, halo row pitch (pixels)
-  int segs_x, nseg;     // segments per row, segments in total
+  int R;                // output rows per tile
+  int segs_x, ngr;      // segments per row, row groups per image
+  int nseg;             // tiles in total: B * ngr * segs_x
   int nst;              // pipeline stages
 };
 
@@ -113,14 +117,16 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int g8 = a.cin / 8;           // channel groups of the input
   const int KK = 9 * g8;              // 8-element K groups of the weights
   const int nkc = (g8 + kChunkGroups - 1) / kChunkGroups;  // K chunks per tile
-  const int SW = g.s.SW, HP = g.s.HP, CW = g.s.CW, nst = g.s.nst, ntiles = g.s.nseg;
-  const int rowb = HP * 16;           // bytes of one halo row
-  const int stage_bytes = 3 * min(g8, kChunkGroups) * rowb;
+  const int SW = g.s.SW, HP = g.s.HP, CW = g.s.CW, R = g.s.R, nst = g.s.nst, ntiles = g.s.nseg;
+  const int GB = min(g8, kChunkGroups);  // planes per chunk box
+  const int gstride = (R + 2) * HP;      // entries between channel groups of a stage
+  const int stage_bytes = GB * gstride * 16;
   const int n0 = blockIdx.y * N;      // the CTA's output channels
   unsigned char *sW = sm;
   unsigned char *sA = sm + g.w_bytes;
   const uint32_t acc_cols = pow2_cols(N);
-  const uint32_t ncols = pow2_cols(kEpiGroups * acc_cols);
+  const uint32_t buf_cols = R * acc_cols;  // one accumulator per output row
+  const uint32_t ncols = pow2_cols(kEpiGroups * buf_cols);
 
   if (warp == kMmaWarp) tmem_alloc(&tbase, ncols);
   if (tid == 0) {
@@ -150,7 +156,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   __syncthreads();
   tc_fence_after_sync();
   const uint32_t tm = tbase;
-  const int HW = a.H * g.s.segs_x;  // tiles per image
+  const int HW = g.s.ngr * g.s.segs_x;  // tiles per image
 
   if (warp == kProdWarp) {
     // ---------------- producer: one item = (tile, K chunk) ----------------
@@ -158,7 +164,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       int it = 0;
       bool stop = false;
       for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x) {
-        const int b = tile / HW, r = tile - b * HW, y = r / g.s.segs_x, x0 = (r - y * g.s.segs_x) * SW;
+        const int b = tile / HW, r = tile - b * HW, rg = r / g.s.segs_x, x0 = (r - rg * g.s.segs_x) * SW;
         for (int c = 0; c < nkc; ++c, ++it) {
           const int s = it % nst;
           if (!wait_phase(&empty[s], ((it / nst) & 1) ^ 1) || *(volatile int *)&s_abort) {
@@ -166,12 +172,10 @@ __global__ void __launch_bounds__(kConvThreads, 2)
             stop = true;
             break;
           }
-          const int gcn = min(kChunkGroups, g8 - c * kChunkGroups);
-          mbar_arrive_expect_tx(&full[s], (uint32_t)(3 * gcn * rowb));
-          unsigned char *st = sA + s * stage_bytes;
-          for (int j = 0; j < gcn; ++j)
-            tma_load_4d(st + 3 * j * rowb, &xmap, 0, x0 / CW - 1, y - 1, b * a.x.cg + a.x.g0 + c * kChunkGroups + j,
-                        &full[s]);
+          // the box is GB planes; planes past the buffer read as zero
+          mbar_arrive_expect_tx(&full[s], (uint32_t)stage_bytes);
+          tma_load_5d(sA + s * stage_bytes, &xmap, 0, x0 / CW - 1, rg * R - 1, a.x.g0 + c * kChunkGroups, b,
+                      &full[s]);
           s_issued = it + 1;
         }
       }
@@ -183,7 +187,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       // descriptors advance by adding (bytes >> 4) to their address field
       const uint64_t bdesc0 = smem_desc(smem_u32(sW), (N / 8) * 128, 128);
       const uint32_t bgrp = (uint32_t)((N / 8) * 128) >> 4;   // one K group of the weights
-      const uint32_t astep = (uint32_t)(2 * 3 * rowb) >> 4;   // two channel groups of the halo
+      const uint32_t astep = (uint32_t)(2 * gstride);          // two channel groups of the halo (entries)
       int it = 0, ti = 0;
       bool stop = false;
       for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x, ++ti) {
@@ -192,8 +196,6 @@ __global__ void __launch_bounds__(kConvThreads, 2)
           atomicExch(&s_abort, 1);
           break;
         }
-        const uint32_t d = tm + acc * acc_cols;
-        uint32_t accumulate = 0;
         for (int c = 0; c < nkc; ++c, ++it) {
           const int s = it % nst;
           if (!wait_phase(&full[s], (it / nst) & 1) || *(volatile int *)&s_abort) {
@@ -203,16 +205,21 @@ __global__ void __launch_bounds__(kConvThreads, 2)
           }
           tc_fence_after_sync();
           const int gcn = min(kChunkGroups, g8 - c * kChunkGroups);
-          const uint64_t adesc0 = smem_desc(smem_u32(sA + s * stage_bytes), 3 * rowb, 128);
+          const uint64_t adesc0 = smem_desc(smem_u32(sA + s * stage_bytes), gstride * 16, 128);
 #pragma unroll 1
-          for (int tap = 0; tap < 9; ++tap) {
-            uint64_t ad = adesc0 + (uint32_t)((tap / 3) * HP + CW - 1 + (tap % 3));  // entries of 16 bytes
-            uint64_t bd = bdesc0 + (uint32_t)(tap * g8 + c * kChunkGroups) * bgrp;
-            for (int j = 0; j < gcn; j += 2) {
-              mma_bf16(d, ad, bd, idesc, accumulate);
-              accumulate = 1;
-              ad += astep;
-              bd += 2 * bgrp;
+          for (int rr = 0; rr < R; ++rr) {
+            const uint32_t d = tm + acc * buf_cols + rr * acc_cols;
+            uint32_t accumulate = c > 0 ? 1u : 0u;
+            for (int tap = 0; tap < 9; ++tap) {
+              // entries of 16 bytes
+              uint64_t ad = adesc0 + (uint32_t)((rr + tap / 3) * HP + CW - 1 + (tap % 3));
+              uint64_t bd = bdesc0 + (uint32_t)(tap * g8 + c * kChunkGroups) * bgrp;
+              for (int j = 0; j < gcn; j += 2) {
+                mma_bf16(d, ad, bd, idesc, accumulate);
+                accumulate = 1;
+                ad += astep;
+                bd += 2 * bgrp;
+              }
             }
           }
           mma_commit(&empty[s]);
@@ -237,9 +244,13 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       }
       if (!__shfl_sync(0xffffffffu, go, 0)) break;
       tc_fence_after_sync();
-      const int b = tile / HW, r = tile - b * HW, y = r / g.s.segs_x, x = (r - y * g.s.segs_x) * SW + m;
+      const int b = tile / HW, r = tile - b * HW, rg = r / g.s.segs_x, x = (r - rg * g.s.segs_x) * SW + m;
       const bool valid = m < SW && x < a.W;
-      const uint32_t taddr = tm + wg * acc_cols + ((uint32_t)(32 * q) << 16);
+#pragma unroll 1
+      for (int orow = 0; orow < R; ++orow) {
+      const int y = rg * R + orow;
+      if (y >= a.H) break;  // uniform across the warp
+      const uint32_t taddr = tm + wg * buf_cols + orow * acc_cols + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
       for (int c16 = 0; c16 < N / 16; ++c16) {
         uint32_t rr[16];
@@ -269,6 +280,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
                 *reinterpret_cast<const uint4 *>(o);
           }
         }
+      }
       }
       tc_fence_before_sync();
       __syncwarp();
@@ -324,7 +336,7 @@ __global__ void __launch_bounds__(192, 2)
   const uint32_t ncols = pow2_cols(g.ndx * NC);
   const int seg0 = blockIdx.x * g.seg_per_chunk;
   const int nitems = max(0, min(g.seg_per_chunk, g.s.nseg - seg0));
-  const int HW = a.H * g.s.segs_x;
+  const int HW = a.H * g.s.segs_x;  // R = 1: one tile per row and segment
 
   if (warp == 5) tmem_alloc(&tbase, ncols);
   if (tid == 0) {
@@ -355,11 +367,8 @@ __global__ void __launch_bounds__(192, 2)
         const int b = seg / HW, r = seg - b * HW, y = r / g.s.segs_x, x0 = (r - y * g.s.segs_x) * SW;
         unsigned char *st = sm + s * stage_bytes;
         mbar_arrive_expect_tx(&full[s], (uint32_t)(ga * SW * 16 + 3 * G8 * rowb));
-        for (int j = 0; j < ga; ++j)
-          tma_load_4d(st + j * SW * 16, &dymap, 0, x0 / CW, y, b * a.dy.cg + a.dy.g0 + j, &full[s]);
-        for (int j = 0; j < G8; ++j)
-          tma_load_4d(st + g.a_bytes + 3 * j * rowb, &xmap, 0, x0 / CW - 1, y - 1, b * a.x.cg + a.x.g0 + c0 / 8 + j,
-                      &full[s]);
+        tma_load_5d(st, &dymap, 0, x0 / CW, y, a.dy.g0, b, &full[s]);
+        tma_load_5d(st + g.a_bytes, &xmap, 0, x0 / CW - 1, y - 1, a.x.g0 + c0 / 8, b, &full[s]);
         s_issued = it + 1;
       }
     }
@@ -452,16 +461,21 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// A blocked activation buffer as the 4-D tensor {CW * 8 elements, W / CW
-// chunks, H rows, CG * B planes} with box {CW * 8, box_chunks, box_rows, 1}.
-static bool act_map(CUtensorMap *m, const ActView &v, int B, int H, int W, int CW, int box_chunks, int box_rows) {
+// A blocked activation buffer as the 5-D tensor {CW * 8 elements, W / CW
+// chunks, H rows, CG planes, B} with box {CW * 8, box_chunks, box_rows,
+// box_planes, 1}.
+static bool act_map(CUtensorMap *m, const ActView &v, int B, int H, int W, int CW, int box_chunks, int box_rows,
+                    int box_planes) {
   auto fn = encode_fn();
   if (!fn) return false;
-  const cuuint64_t dims[4] = {(cuuint64_t)CW * 8, (cuuint64_t)(W / CW), (cuuint64_t)H, (cuuint64_t)v.cg * B};
-  const cuuint64_t strides[3] = {(cuuint64_t)CW * 16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16};
-  const cuuint32_t box[4] = {(cuuint32_t)CW * 8, (cuuint32_t)box_chunks, (cuuint32_t)box_rows, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, v.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+  const cuuint64_t dims[5] = {(cuuint64_t)CW * 8, (cuuint64_t)(W / CW), (cuuint64_t)H, (cuuint64_t)v.cg,
+                              (cuuint64_t)B};
+  const cuuint64_t strides[4] = {(cuuint64_t)CW * 16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16,
+                                 (cuuint64_t)v.cg * H * W * 16};
+  const cuuint32_t box[5] = {(cuuint32_t)CW * 8, (cuuint32_t)box_chunks, (cuuint32_t)box_rows,
+                             (cuuint32_t)box_planes, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, v.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -484,14 +498,16 @@ constexpr int kHalfSm = 110 * 1024;          // two CTAs per SM
 // images. Chunks: 16 pixels, or the largest power of two dividing W. The halo
 // row spans one chunk left of the segment to at least one pixel past it,
 // rounded up to 8 entries so that every row starts on a 128-byte boundary.
-static SegGeom seg_geom(int B, int H, int W) {
+static SegGeom seg_geom(int B, int H, int W, int R) {
   SegGeom s{};
   s.SW = W >= 128 ? 128 : (W + 15) / 16 * 16;
   s.CW = 16;
   while (W % s.CW) s.CW >>= 1;
   s.HP = (s.SW + 2 * s.CW + 7) / 8 * 8;
+  s.R = R;
   s.segs_x = (W + s.SW - 1) / s.SW;
-  s.nseg = B * H * s.segs_x;
+  s.ngr = (H + R - 1) / R;
+  s.nseg = B * s.ngr * s.segs_x;
   return s;
 }
 
@@ -506,11 +522,17 @@ static int conv_part(int n, int cin) {
 template <int NP>
 static cudaError_t launch_conv_tma_t(const ConvArgs &a, int parts, cudaStream_t st) {
   ConvTmaGeom g{};
-  g.s = seg_geom(a.B, a.H, a.W);
-  CUtensorMap xm;
-  if (!act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, 3)) return cudaErrorInvalidValue;
   g.w_bytes = (NP * 9 * a.cin * 2 + 1023) / 1024 * 1024;
-  const int stage = 3 * std::min(a.cin / 8, kChunkGroups) * g.s.HP * 16;
+  const int GB = std::min(a.cin / 8, kChunkGroups);
+  // rows per tile: as many as the TMEM (two buffers of R accumulators within
+  // 256 columns) and three stages of shared memory allow
+  int R = 256 / (2 * (int)pow2_cols(NP));
+  if (R > 4) R = 4;
+  while (R > 1 && g.w_bytes + 3 * GB * (R + 2) * seg_geom(a.B, a.H, a.W, R).HP * 16 + kTail > kSmemCap) R >>= 1;
+  g.s = seg_geom(a.B, a.H, a.W, R);
+  CUtensorMap xm;
+  if (!act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, R + 2, GB)) return cudaErrorInvalidValue;
+  const int stage = GB * (R + 2) * g.s.HP * 16;
   // two CTAs per SM when that leaves at least 3 stages each, else one CTA
   // with the deepest ring that fits
   int per_sm = 2, budget = kHalfSm - kTail;
@@ -546,7 +568,7 @@ cudaError_t launch_conv3x3(const ConvArgs &a, int n, cudaStream_t st) {
 constexpr int kWgChunks = 296;
 
 int wgrad_chunks(int B, int H, int W) {
-  const SegGeom s = seg_geom(B, H, W);
+  const SegGeom s = seg_geom(B, H, W, 1);
   const int per = (s.nseg + kWgChunks - 1) / kWgChunks;
   return (s.nseg + per - 1) / per;
 }
@@ -562,10 +584,10 @@ static int wgrad_part(int cin) {
 template <int CP>
 static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *chunks) {
   WgradTmaGeom g{};
-  g.s = seg_geom(a.B, a.H, a.W);
+  g.s = seg_geom(a.B, a.H, a.W, 1);
   CUtensorMap dym, xm;
-  if (!act_map(&dym, a.dy, a.B, a.H, a.W, g.s.CW, g.s.SW / g.s.CW, 1) ||
-      !act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, 3))
+  if (!act_map(&dym, a.dy, a.B, a.H, a.W, g.s.CW, g.s.SW / g.s.CW, 1, a.cout / 8) ||
+      !act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, 3, CP / 8))
     return cudaErrorInvalidValue;
   g.seg_per_chunk = (g.s.nseg + kWgChunks - 1) / kWgChunks;
   const int nchunks = (g.s.nseg + g.seg_per_chunk - 1) / g.seg_per_chunk;

@@ -135,6 +135,15 @@ __device__ __forceinline__ void tma_load_4d(void *smem_dst, const void *tmap, in
       : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(void *smem_dst, const void *tmap, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t *mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(smem_dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // ---- cp.async ---------------------------------------------------------------
 __device__ __forceinline__ void cp16(void *smem_dst, const void *gmem_src, bool in) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src),
