@@ -315,7 +315,12 @@ struct WgradTmaGeom {
   int a_bytes;          // dY bytes of one stage (cout / 8 groups of SW rows)
 };
 
-template <int CP>
+// T = false: D[co][(group, dy, channel)] as described above. T = true (used
+// when cout <= 32): the transposed product D[(group, dy, channel)][co], GEMM
+// rows = the halo's 3 * CP / 8 (group, dy) groups (padded to 128 the same
+// way), columns = the output channels: the same MMA count with N = cout
+// instead of 3 * CP, a third of the tensor work when cout = 16 = CP.
+template <int CP, bool T>
 __global__ void __launch_bounds__(192, 2)
     k_wgrad_tma(const __grid_constant__ CUtensorMap dymap, const __grid_constant__ CUtensorMap xmap, WgradArgs a,
                 WgradTmaGeom g) {
@@ -333,7 +338,8 @@ __global__ void __launch_bounds__(192, 2)
   const int part = (g.ndx == 3) ? blockIdx.y : blockIdx.y / 3;
   const int dx0 = (g.ndx == 3) ? 0 : blockIdx.y % 3;  // index 0..2 of dx = -1..1
   const int c0 = part * CP;
-  const uint32_t ncols = pow2_cols(g.ndx * NC);
+  const int dcols = T ? a.cout : NC;  // accumulator columns per dx
+  const uint32_t ncols = pow2_cols(g.ndx * dcols);
   const int seg0 = blockIdx.x * g.seg_per_chunk;
   const int nitems = max(0, min(g.seg_per_chunk, g.s.nseg - seg0));
   const int HW = a.H * g.s.segs_x;  // R = 1: one tile per row and segment
@@ -374,7 +380,7 @@ __global__ void __launch_bounds__(192, 2)
     }
   } else if (warp == 5) {
     if (lane == 0) {
-      const uint32_t idesc = instr_desc_bf16(128, NC, true, true);
+      const uint32_t idesc = instr_desc_bf16(128, T ? a.cout : NC, true, true);
       for (int it = 0; it < nitems; ++it) {
         const int s = it % nst;
         if (!wait_phase(&full[s], (it / nst) & 1) || *(volatile int *)&s_abort) {
@@ -386,10 +392,11 @@ __global__ void __launch_bounds__(192, 2)
         // A: co groups at SW rows, pixel groups at 128 bytes; B: (group, dy)
         // column groups at HP rows, pixel groups at 128 bytes. 16 pixels =
         // 256 bytes = 16 in the descriptors' address field.
-        const uint64_t adesc0 = smem_desc(a0, 128, SW * 16);
+        const uint64_t ydesc = smem_desc(a0, 128, SW * 16);
         for (int t = 0; t < g.ndx; ++t) {
-          const uint64_t bdesc0 = smem_desc(b0 + (uint32_t)((CW - 1 + dx0 + t) * 16), 128, rowb);
-          const uint32_t d = tm + t * NC;
+          const uint64_t xdesc = smem_desc(b0 + (uint32_t)((CW - 1 + dx0 + t) * 16), 128, rowb);
+          const uint64_t adesc0 = T ? xdesc : ydesc, bdesc0 = T ? ydesc : xdesc;
+          const uint32_t d = tm + t * dcols;
           mma_bf16(d, adesc0, bdesc0, idesc, it > 0 ? 1u : 0u);
           for (int k = 1; k < SW / 16; ++k) mma_bf16(d, adesc0 + 16 * k, bdesc0 + 16 * k, idesc, 1u);
         }
@@ -408,7 +415,27 @@ __global__ void __launch_bounds__(192, 2)
   }
   __syncthreads();
   ok = !s_abort;
-  if (ok && warp < 4) {
+  if (ok && warp < 4 && T) {
+    tc_fence_after_sync();
+    // lane m = GEMM row: halo group k = m / 8 = 3 * group + (dy + 1), channel m % 8
+    const int m = 32 * warp + lane, k = m >> 3, grp = k / 3, dyi = k - 3 * grp;
+    const int ci = c0 + 8 * grp + (m & 7);
+    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    for (int t = 0; t < g.ndx; ++t) {
+      const int tap = dyi * 3 + dx0 + t;
+#pragma unroll 1
+      for (int c16 = 0; c16 < a.cout / 16; ++c16) {
+        uint32_t rr[16];
+        tmem_ld16(tm + lane_base + t * dcols + c16 * 16, rr);
+        if (m < 3 * CP) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            a.part[(((long long)blockIdx.x * 9 + tap) * a.cout + c16 * 16 + j) * a.cin + ci] =
+                nitems > 0 ? __uint_as_float(rr[j]) : 0.0f;
+        }
+      }
+    }
+  } else if (ok && warp < 4) {
     tc_fence_after_sync();
     const int co = 32 * warp + lane;
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
@@ -581,7 +608,7 @@ static int wgrad_part(int cin) {
   return 0;
 }
 
-template <int CP>
+template <int CP, bool T>
 static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *chunks) {
   WgradTmaGeom g{};
   g.s = seg_geom(a.B, a.H, a.W, 1);
@@ -591,14 +618,14 @@ static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *
     return cudaErrorInvalidValue;
   g.seg_per_chunk = (g.s.nseg + kWgChunks - 1) / kWgChunks;
   const int nchunks = (g.s.nseg + g.seg_per_chunk - 1) / g.seg_per_chunk;
-  g.ndx = (9 * CP <= 256) ? 3 : 1;
+  g.ndx = (T || 9 * CP <= 256) ? 3 : 1;
   const int nparts = a.cin / CP;
   const int gy = nparts * (g.ndx == 3 ? 1 : 3);
   g.a_bytes = a.cout / 8 * g.s.SW * 16;
-  // A rows past cout address the bytes that follow the dY groups: keep the
-  // full 128-row span (16 groups) inside the allocation
+  // GEMM rows past the real ones address the bytes that follow their groups:
+  // keep the full 128-row span (16 groups) inside the allocation
   const int stage = g.a_bytes + 3 * (CP / 8) * g.s.HP * 16;
-  int tail = 16 * g.s.SW * 16 - g.a_bytes;
+  int tail = T ? (16 - 3 * CP / 8) * g.s.HP * 16 + 512 : 16 * g.s.SW * 16 - g.a_bytes;
   if (tail < kTail) tail = kTail;
   g.s.nst = (kHalfSm - tail) / stage;
   if (g.s.nst < 3) g.s.nst = (kSmemCap - tail) / stage;
@@ -606,10 +633,10 @@ static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *
   if (g.s.nst < 2) return cudaErrorInvalidValue;
   int smem = g.s.nst * stage + tail;
   // at most two CTAs per SM when each holds 256 TMEM columns
-  if (pow2_cols(g.ndx * 3 * CP) >= 256 && smem < 80 * 1024) smem = 80 * 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_wgrad_tma<CP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (pow2_cols(g.ndx * (T ? a.cout : 3 * CP)) >= 256 && smem < 80 * 1024) smem = 80 * 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_wgrad_tma<CP, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_wgrad_tma<CP><<<dim3(nchunks, gy), 192, smem, st>>>(dym, xm, a, g);
+  k_wgrad_tma<CP, T><<<dim3(nchunks, gy), 192, smem, st>>>(dym, xm, a, g);
   *chunks = nchunks;
   return cudaGetLastError();
 }
@@ -618,12 +645,18 @@ cudaError_t launch_wgrad(const WgradArgs &a, cudaStream_t st) {
   if (a.cout % 8 != 0 || a.cout > 128 || a.cin % 16 != 0 || a.W < 1) return cudaErrorInvalidValue;
   int chunks = 0;
   cudaError_t e;
-  switch (wgrad_part(a.cin)) {
-    case 16: e = launch_wgrad_tma_t<16>(a, st, &chunks); break;
-    case 32: e = launch_wgrad_tma_t<32>(a, st, &chunks); break;
-    case 48: e = launch_wgrad_tma_t<48>(a, st, &chunks); break;
-    case 64: e = launch_wgrad_tma_t<64>(a, st, &chunks); break;
-    default: return cudaErrorInvalidValue;
+  if (a.cout <= 32) {
+    // transposed product: parts of at most 32 channels (3 * 32 GEMM rows)
+    const int cp = a.cin % 32 == 0 ? 32 : 16;
+    e = cp == 32 ? launch_wgrad_tma_t<32, true>(a, st, &chunks) : launch_wgrad_tma_t<16, true>(a, st, &chunks);
+  } else {
+    switch (wgrad_part(a.cin)) {
+      case 16: e = launch_wgrad_tma_t<16, false>(a, st, &chunks); break;
+      case 32: e = launch_wgrad_tma_t<32, false>(a, st, &chunks); break;
+      case 48: e = launch_wgrad_tma_t<48, false>(a, st, &chunks); break;
+      case 64: e = launch_wgrad_tma_t<64, false>(a, st, &chunks); break;
+      default: return cudaErrorInvalidValue;
+    }
   }
   if (e != cudaSuccess) return e;
   return launch_wgrad_reduce(a.part, chunks, a.cout, a.cin, a.dw, st);
