@@ -590,8 +590,9 @@ cudaError_t launch_conv3x3(const ConvArgs &a, int n, cudaStream_t st) {
   }
 }
 
-// Partial-sum chunks of the weight gradient: a fixed count, so the order of
-// the final sum does not depend on the device.
+// Partial-sum chunks of the weight gradient: at most a fixed count (divided by
+// the CTAs a chunk already spans), so the order of the final sum does not
+// depend on the device; wgrad_chunks bounds it for buffer sizing.
 constexpr int kWgChunks = 296;
 
 int wgrad_chunks(int B, int H, int W) {
@@ -616,11 +617,14 @@ static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *
   if (!act_map(&dym, a.dy, a.B, a.H, a.W, g.s.CW, g.s.SW / g.s.CW, 1, a.cout / 8) ||
       !act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, 3, CP / 8))
     return cudaErrorInvalidValue;
-  g.seg_per_chunk = (g.s.nseg + kWgChunks - 1) / kWgChunks;
-  const int nchunks = (g.s.nseg + g.seg_per_chunk - 1) / g.seg_per_chunk;
   g.ndx = (T || 9 * CP <= 256) ? 3 : 1;
   const int nparts = a.cin / CP;
   const int gy = nparts * (g.ndx == 3 ? 1 : 3);
+  // about kWgChunks CTAs in all: fewer segment chunks when the channels and
+  // dx already split the work (fewer partials to write and sum)
+  const int target = std::max(1, kWgChunks / gy);
+  g.seg_per_chunk = (g.s.nseg + target - 1) / target;
+  const int nchunks = (g.s.nseg + g.seg_per_chunk - 1) / g.seg_per_chunk;
   g.a_bytes = a.cout / 8 * g.s.SW * 16;
   // GEMM rows past the real ones address the bytes that follow their groups:
   // keep the full 128-row span (16 groups) inside the allocation

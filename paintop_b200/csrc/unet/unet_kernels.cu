@@ -438,18 +438,24 @@ __global__ void k_compose_guess(const float *g, const float *corr, int W, int H,
 // ----------------------------------------------------------------------------
 // (the weight gradient's final sum, launched by launch_wgrad_reduce)
 // Sum the per-chunk partials in chunk order: dW[co][tap][ci] (fp32).
+// One warp per weight: lane l sums chunks l, l + 32, ... and a fixed shuffle
+// tree combines the lanes.
 __global__ void k_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw) {
-  const int total = cout * 9 * cin;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+  const int total = cout * 9 * cin, lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * blockDim.x / 32;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += nwarps) {
     const int co = i / (9 * cin), r = i - co * 9 * cin, tap = r / cin, ci = r - tap * cin;
     float s = 0.0f;
-    for (int k = 0; k < nchunks; ++k) s += part[(((long long)k * 9 + tap) * cout + co) * cin + ci];
-    dw[i] = s;
+    for (int k = lane; k < nchunks; k += 32) s += part[(((long long)k * 9 + tap) * cout + co) * cin + ci];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) dw[i] = s;
   }
 }
 
 cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st) {
-  k_wgrad_reduce<<<256, 256, 0, st>>>(part, nchunks, cout, cin, dw);
+  long long blocks = ((long long)cout * 9 * cin * 32 + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_wgrad_reduce<<<(unsigned)blocks, 256, 0, st>>>(part, nchunks, cout, cin, dw);
   return cudaGetLastError();
 }
 
