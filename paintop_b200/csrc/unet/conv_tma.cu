@@ -538,11 +538,13 @@ static SegGeom seg_geom(int B, int H, int W, int R) {
   return s;
 }
 
-// Output channels per CTA: all of them when the resident weights stay small,
-// else the largest part (a multiple of 16 dividing N) whose weights fit.
+// Output channels per CTA: the largest part (a multiple of 16 dividing N, at
+// most 96) whose resident weights fit in 110 KB. Wider parts mean fewer,
+// larger MMAs and fewer reloads of the input halo; the rest of the shared
+// memory still holds at least two pipeline stages.
 static int conv_part(int n, int cin) {
   for (int p = n; p >= 16; p -= 16)
-    if (n % p == 0 && p <= 96 && p * 9 * cin * 2 <= 64 * 1024) return p;
+    if (n % p == 0 && p <= 96 && p * 9 * cin * 2 <= 110 * 1024) return p;
   return 0;
 }
 
