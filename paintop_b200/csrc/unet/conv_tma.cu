@@ -539,12 +539,17 @@ static SegGeom seg_geom(int B, int H, int W, int R) {
 }
 
 // Output channels per CTA: the largest part (a multiple of 16 dividing N, at
-// most 96) whose resident weights fit in 110 KB. Wider parts mean fewer,
-// larger MMAs and fewer reloads of the input halo; the rest of the shared
-// memory still holds at least two pipeline stages.
-static int conv_part(int n, int cin) {
-  for (int p = n; p >= 16; p -= 16)
-    if (n % p == 0 && p <= 96 && p * 9 * cin * 2 <= 110 * 1024) return p;
+// most 96) whose resident weights fit in 110 KB and still leave shared memory
+// for two one-row pipeline stages at this width. Wider parts mean fewer,
+// larger MMAs and fewer reloads of the input halo.
+static int conv_part(int n, int cin, int W) {
+  const int HP = seg_geom(1, 1, W, 1).HP;
+  const int stage1 = std::min(cin / 8, kChunkGroups) * 3 * HP * 16;
+  for (int p = n; p >= 16; p -= 16) {
+    const int w_bytes = (p * 9 * cin * 2 + 1023) / 1024 * 1024;
+    if (n % p == 0 && p <= 96 && p * 9 * cin * 2 <= 110 * 1024 && w_bytes + 2 * stage1 + kTail <= kSmemCap)
+      return p;
+  }
   return 0;
 }
 
@@ -581,7 +586,7 @@ static cudaError_t launch_conv_tma_t(const ConvArgs &a, int parts, cudaStream_t 
 
 cudaError_t launch_conv3x3(const ConvArgs &a, int n, cudaStream_t st) {
   if (a.cin % 16 != 0 || a.cin > 256 || a.W < 1 || a.H < 1 || a.B < 1) return cudaErrorInvalidValue;
-  const int p = conv_part(n, a.cin);
+  const int p = conv_part(n, a.cin, a.W);
   switch (p) {
     case 16: return launch_conv_tma_t<16>(a, n / p, st);
     case 32: return launch_conv_tma_t<32>(a, n / p, st);

@@ -110,6 +110,7 @@ def evaluate_multi4096(ctx, net, seed=1, scale=8, size=4096, tol=1e-6):
     m = torch.as_tensor(inst.mask, device="cuda").contiguous()
     ref, rref, _ = solve_image_device(ctx, g, a, m, tol=1e-10)
     up, rp, tp = solve_image_device(ctx, g, a, m, tol=tol)
+    ws.guess_image(net, g, a, m, scale)  # warm-up: sizes the network's buffers for the pooled images
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     guess = ws.guess_image(net, g, a, m, scale)

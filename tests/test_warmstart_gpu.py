@@ -107,6 +107,19 @@ def test_guess_pooled_matches_host_emulation(ctx, ws, torch_cuda):
     assert np.abs(got - want).max() < 1e-5
 
 
+def test_guess_at_a_large_coarse_size(ctx, ws, torch_cuda):
+    """A 1024x1024 RGB problem pooled by 2: the network runs on 512x512
+    images, where the deeper layers meet other widths than in training."""
+    torch = torch_cuda
+    net = ws.UNet(ctx, seed=33)
+    gg, aa, mm = ws.make_instances(3, 1024, seed=25)
+    g = gg.permute(1, 2, 0).contiguous()
+    a = aa.permute(1, 2, 0).contiguous()
+    m = mm[0].contiguous()
+    got = ws.guess_image(net, g, a, m, scale=2)
+    assert got.shape == g.shape and bool(torch.isfinite(got).all())
+
+
 def test_trainer_resume_is_bit_identical(ctx, ws, torch_cuda, tmp_path):
     data = ws.build_dataset(ctx, n=256, size=64, seed=5, chunk=256)
     straight = ws.Trainer(ws.UNet(ctx, seed=7), data, batch=64, seed=3)
