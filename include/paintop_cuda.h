@@ -299,6 +299,21 @@ pt_status pt_unet_loss_grad(pt_unet *net, const float *features, const float *ta
 pt_status pt_unet_train_step(pt_unet *net, const float *features, const float *target,
                              const float *loss_mask, uint32_t batch, uint32_t h, uint32_t w,
                              float lr, double *loss);
+/* Data-parallel training, one replica per GPU. A replica's share of a step is
+ * its gradient record: the gradient of the masked mean squared error over its
+ * own part of the batch (pt_unet_param_count floats) followed by that part's
+ * interior-pixel count, written to `record` (device memory, param_count + 1
+ * floats). Does not update the parameters; *loss as in pt_unet_loss_grad. */
+pt_status pt_unet_grad_record(pt_unet *net, const float *features, const float *target,
+                              const float *loss_mask, uint32_t batch, uint32_t h, uint32_t w,
+                              double *loss, float *record);
+/* One Adam step on `replicas` gradient records laid end to end in device
+ * memory (replica-major): each gradient weighted by its share of the interior
+ * pixels and summed in replica order in fp64, which is the gradient of the
+ * whole batch's masked mean squared error. Replicas that apply the same
+ * records from the same state stay bit-identical; one record reproduces
+ * pt_unet_train_step exactly. */
+pt_status pt_unet_apply_records(pt_unet *net, const float *records, uint32_t replicas, float lr);
 /* The warm start of one pt_poisson_solve problem (device pointers; images
  * width x height x channels interleaved, mask width x height): every channel
  * is pooled by `scale` (area average, 1 = full resolution), the network

@@ -30,7 +30,8 @@ EXPORTED = (
     "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_poisson_solve_noalloc",
     "pt_unet_create", "pt_unet_destroy", "pt_unet_param_count", "pt_unet_get_params",
     "pt_unet_set_params", "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad",
-    "pt_unet_train_step", "pt_unet_save", "pt_unet_load", "pt_unet_guess",
+    "pt_unet_train_step", "pt_unet_save", "pt_unet_load", "pt_unet_guess", "pt_unet_grad_record",
+    "pt_unet_apply_records",
 )
 PT_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
@@ -151,11 +152,14 @@ def lib():
     L.pt_unet_loss_grad.argtypes = [vp, vp, vp, vp, u32, u32, u32, C.POINTER(C.c_double), vp]
     L.pt_unet_train_step.argtypes = [vp, vp, vp, vp, u32, u32, u32, f32, C.POINTER(C.c_double)]
     L.pt_unet_guess.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, vp]
+    L.pt_unet_grad_record.argtypes = [vp, vp, vp, vp, u32, u32, u32, C.POINTER(C.c_double), vp]
+    L.pt_unet_apply_records.argtypes = [vp, vp, u32, f32]
     L.pt_unet_save.argtypes = [vp, C.c_char_p]
     L.pt_unet_load.argtypes = [vp, C.c_char_p]
     for name in ("pt_unet_create", "pt_unet_destroy", "pt_unet_get_params", "pt_unet_set_params",
                  "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad", "pt_unet_train_step",
-                 "pt_unet_save", "pt_unet_load", "pt_unet_guess"):
+                 "pt_unet_save", "pt_unet_load", "pt_unet_guess", "pt_unet_grad_record",
+                 "pt_unet_apply_records"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -462,6 +462,35 @@ pt_status pt_unet_train_step(pt_unet *n, const float *features, const float *tar
   return PT_OK;
 }
 
+pt_status pt_unet_grad_record(pt_unet *n, const float *features, const float *target, const float *loss_mask,
+                              uint32_t batch, uint32_t h, uint32_t w, double *loss, float *record) {
+  if (!n || !features || !target || !loss_mask || !record) return PT_INVALID_ARG;
+  RET(check_shape(batch, h, w));
+  std::lock_guard<std::mutex> lock(n->ctx->mu);
+  cudaSetDevice(n->ctx->device);
+  RET(ensure_acts(n, (int)batch, (int)h, (int)w));
+  RET(forward(n, features));
+  RET(backward(n, target, loss_mask, loss));
+  cudaStream_t st = n->ctx->stream;
+  CK(cudaMemcpyAsync(record, n->grad, n->nparam * 4, cudaMemcpyDeviceToDevice, st), "record copy");
+  CK(cudaMemcpyAsync(record + n->nparam, n->count, 4, cudaMemcpyDeviceToDevice, st), "count copy");
+  CK(cudaStreamSynchronize(st), "sync");
+  return PT_OK;
+}
+
+pt_status pt_unet_apply_records(pt_unet *n, const float *records, uint32_t replicas, float lr) {
+  if (!n || !records || replicas == 0 || !(lr > 0.0f)) return PT_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(n->ctx->mu);
+  cudaSetDevice(n->ctx->device);
+  n->step += 1;
+  CK(launch_adam_records(n->params, n->m, n->v, records, (int)replicas, (long long)n->nparam, lr, n->step,
+                         n->ctx->stream),
+     "adam");
+  RET(refresh_weights(n));
+  CK(cudaStreamSynchronize(n->ctx->stream), "sync");
+  return PT_OK;
+}
+
 pt_status pt_unet_guess(pt_unet *n, const float *guidance, const float *anchor, const float *mask,
                         uint32_t width, uint32_t height, uint32_t channels, uint32_t scale, float *guess) {
   if (!n || !guidance || !anchor || !mask || !guess || !width || !height || !channels || !scale)

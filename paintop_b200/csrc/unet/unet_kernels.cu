@@ -299,18 +299,43 @@ __global__ void k_head_bwd(ActView x, const float *w, const float *dpred, ActVie
 
 // Adam (Kingma & Ba): m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
 // w -= lr * mhat / (sqrt(vhat) + eps); refreshes the bf16 copy.
+__device__ __forceinline__ void adam_update(long long i, float gi, float *w, float *m, float *v, __nv_bfloat16 *wb,
+                                            float lr, float b1, float b2, float eps, float bc1, float bc2) {
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16_rn(wi);
+}
+
 __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, long long n, float lr,
                        float b1, float b2, float eps, float bc1, float bc2) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    adam_update(i, g[i], w, m, v, wb, lr, b1, b2, eps, bc1, bc2);
+}
+
+// Adam on the combination of `R` replicas' gradient records laid end to end,
+// each n gradients of that replica's mean loss followed by its interior count
+// c_r: g = (sum over r = 0 .. R-1, in order, of c_r g_r) / max(1, sum c_r),
+// accumulated in fp64 (each product c_r g_r is exact there). Every replica
+// that runs this on the same records takes the same step bit for bit; with
+// one record g is that record's gradient exactly.
+__global__ void k_adam_records(float *w, float *m, float *v, const float *rec, int R, __nv_bfloat16 *wb,
+                               long long n, float lr, float b1, float b2, float eps, float bc1, float bc2) {
+  double total = 0.0;
+  for (int r = 0; r < R; ++r) total += (double)rec[(long long)r * (n + 1) + n];
+  total = fmax(total, 1.0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
-    w[i] = wi;
-    if (wb) wb[i] = __float2bfloat16_rn(wi);
+    double acc = 0.0;
+    for (int r = 0; r < R; ++r) {
+      const float *q = rec + (long long)r * (n + 1);
+      acc += (double)q[n] * (double)q[i];
+    }
+    adam_update(i, (float)(acc / total), w, m, v, wb, lr, b1, b2, eps, bc1, bc2);
   }
 }
 
@@ -531,6 +556,14 @@ cudaError_t launch_adam(float *w, float *m, float *v, const float *g, __nv_bfloa
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
   k_adam<<<blocks_for(n, 256), 256, 0, st>>>(w, m, v, g, wb, n, lr, b1, b2, eps, bc1, bc2);
+  return cudaGetLastError();
+}
+cudaError_t launch_adam_records(float *w, float *m, float *v, const float *records, int replicas, long long n,
+                                float lr, int step, cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+  k_adam_records<<<blocks_for(n, 256), 256, 0, st>>>(w, m, v, records, replicas, nullptr, n, lr, b1, b2, eps, bc1,
+                                                     bc2);
   return cudaGetLastError();
 }
 cudaError_t launch_prep_weights(const float *w, int cout, int cin, __nv_bfloat16 *wb, __nv_bfloat16 *wt,

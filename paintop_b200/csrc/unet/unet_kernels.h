@@ -83,6 +83,10 @@ cudaError_t launch_loss(const float *pred, const float *target, const float *mas
                         double *part, float *count, cudaStream_t st);
 cudaError_t launch_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, long long n, float lr,
                         int step, cudaStream_t st);
+// Adam on the fixed-order combination of `replicas` gradient records (n
+// gradients + the interior count each, replica-major).
+cudaError_t launch_adam_records(float *w, float *m, float *v, const float *records, int replicas, long long n,
+                                float lr, int step, cudaStream_t st);
 cudaError_t launch_prep_weights(const float *w, int cout, int cin, __nv_bfloat16 *wb, __nv_bfloat16 *wt,
                                 cudaStream_t st);
 // fp32 features (B x H x W x 4) -> the 16-channel input (2 groups, channels 4..15 zero)

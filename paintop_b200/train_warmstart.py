@@ -13,6 +13,13 @@ pixels) through ``pt_unet_train_step``, writes the parameters, a resumable
 checkpoint and a JSON report (dataset, throughput in TFLOP/s of the
 convolutions, loss curve, held-out evaluation).
 
+Under torchrun (``python -m torch.distributed.run --nproc-per-node N -m
+paintop_b200.train_warmstart train ...``) ``train`` is data-parallel: the
+dataset's solves are split over the ranks and broadcast, every rank trains a
+replica on its part of each batch of 64, and the gradient records are
+all-gathered over NCCL and summed in rank order (DataParallelTrainer), so the
+replicas stay identical; rank 0 writes the outputs.
+
 ``eval256`` and ``multi4096`` compare the learned warm start with the plain
 solve on the same inputs: both stop at the same absolute bar, tolerance x
 ||r(anchor)|| in FP64, and the plain solve is the fallback (a guess whose
@@ -136,20 +143,42 @@ def evaluate_multi4096(ctx, net, seed=1, scale=8, size=4096, tol=1e-6):
         guess_error=err(guess), anchor_error=err(a))
 
 
+def _init_ranks():
+    """Under torchrun (WORLD_SIZE > 1): one NCCL rank per GPU; returns (rank, world, device)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world == 1:
+        return 0, 1, 0
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return dist.get_rank(), world, local
+
+
 def cmd_train(args):
     torch = ws._torch()
+    rank, world, dev = _init_ranks()
     os.makedirs(args.out, exist_ok=True)
-    ctx = _lib.Context(0)
+    ctx = _lib.Context(dev)
     report = dict(config=dict(instances=args.instances, size=256, tol=1e-7, epochs=args.epochs, batch=64,
-                              lr=1e-3, seed=args.seed))
+                              lr=1e-3, seed=args.seed, ranks=world))
     t0 = time.perf_counter()
-    data = ws.build_dataset(ctx, n=args.instances, size=256, seed=args.seed, tol=1e-7)
+    if world > 1:
+        data = ws.build_dataset_sharded(ctx, n=args.instances, size=256, seed=args.seed, tol=1e-7)
+    else:
+        data = ws.build_dataset(ctx, n=args.instances, size=256, seed=args.seed, tol=1e-7)
     report["dataset"] = dict(gen_s=data.gen_s, solve_s=data.solve_s, wall_s=time.perf_counter() - t0,
-                             solves_per_s=args.instances / data.solve_s,
+                             solves_per_s=args.instances / world / max(data.solve_s, 1e-9),
                              sweeps_mean=float(data.sweeps.mean()), sweeps_max=int(data.sweeps.max()))
-    _log("dataset", report["dataset"])
+    if rank == 0:
+        _log("dataset", report["dataset"])
     net = ws.UNet(ctx, seed=args.seed)
-    tr = ws.Trainer(net, data, batch=64, lr=1e-3, seed=args.seed)
+    if world > 1:
+        tr = ws.DataParallelTrainer(net, data, batch=64, lr=1e-3, seed=args.seed)
+    else:
+        tr = ws.Trainer(net, data, batch=64, lr=1e-3, seed=args.seed)
     ckpt = os.path.join(args.out, "checkpoint.bin")
     if args.resume and os.path.exists(ckpt):
         tr.load(ckpt)
@@ -158,12 +187,18 @@ def cmd_train(args):
     t0 = time.perf_counter()
     while tr.steps < total:
         losses.append(tr.step())
-        if tr.steps % 100 == 0:
+        if rank == 0 and tr.steps % 100 == 0:
             _log(f"epoch {tr.epoch} step {tr.steps} loss {np.mean(losses[-100:]):.4e}")
         if args.checkpoint_every and tr.steps % args.checkpoint_every == 0:
             tr.save(ckpt)
     wall = time.perf_counter() - t0
     tr.save(ckpt)
+    if rank != 0:
+        import torch.distributed as dist
+        dist.barrier()  # rank 0 evaluates and writes the report
+        dist.destroy_process_group()
+        ctx.close()
+        return
     ws.save_params(net, os.path.join(args.out, "warmstart_unet.params"))
     flops = ws.train_flops_per_pixel() * 64 * 256 * 256
     report["train"] = dict(
@@ -180,6 +215,10 @@ def cmd_train(args):
         json.dump(report, f, indent=1)
     del data
     torch.cuda.empty_cache()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
     ctx.close()
 
 

@@ -128,6 +128,30 @@ class UNet:
                                                   B, H, W, C.c_float(lr), C.byref(loss)), "train_step")
         return loss.value
 
+    def grad_record(self, feats, target, loss_mask, out=None):
+        """This replica's gradient record (device float32 tensor of param_count + 1:
+        the gradient of the mean loss over its batch, then its interior count)
+        and its loss; the parameters do not change."""
+        torch = _torch()
+        B, H, W, _ = feats.shape
+        if out is None:
+            out = torch.empty(self.param_count + 1, dtype=torch.float32, device=feats.device)
+        loss = C.c_double()
+        torch.cuda.synchronize()
+        self._check(_lib.lib().pt_unet_grad_record(self.h, _dptr(feats), _dptr(target), _dptr(loss_mask),
+                                                   B, H, W, C.byref(loss), _dptr(out)), "grad_record")
+        return loss.value, out
+
+    def apply_records(self, records, lr: float = 1e-3) -> None:
+        """One Adam step on gradient records stacked replica-major (R x (param_count + 1),
+        device float32), combined in replica order."""
+        torch = _torch()
+        if records.dim() != 2 or records.shape[1] != self.param_count + 1 or not records.is_contiguous():
+            raise ValueError("records must be a contiguous (replicas, param_count + 1) tensor")
+        torch.cuda.synchronize()
+        self._check(_lib.lib().pt_unet_apply_records(self.h, _dptr(records), records.shape[0], C.c_float(lr)),
+                    "apply_records")
+
 
 # ---------------------------------------------------------------------------
 # seeded synthetic training instances on the device
@@ -255,15 +279,18 @@ class Dataset:
 
 
 def build_dataset(ctx, n: int = 20000, size: int = 256, seed: int = 0, chunk: int = 512,
-                  tol: float = 1e-7) -> Dataset:
-    """Generate and solve n training instances on the device (solves by the plain method)."""
+                  tol: float = 1e-7, _seed_base=None) -> Dataset:
+    """Generate and solve n training instances on the device (solves by the plain
+    method). Chunk c0 (instances c0 .. c0 + chunk - 1) comes from the seed
+    seed * 1000003 + c0."""
     torch = _torch()
     gs, an, ms, us, sw = [], [], [], [], []
     t_gen = t_solve = 0.0
+    base = seed * 1000003 if _seed_base is None else _seed_base
     for c0 in range(0, n, chunk):
         k = min(chunk, n - c0)
         t0 = time.perf_counter()
-        g, a, m = make_instances(k, size, seed * 1000003 + c0)
+        g, a, m = make_instances(k, size, base + c0)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         u, reps = solve_batch_device(ctx, g, a, m, tol=tol)
@@ -341,6 +368,119 @@ class Trainer:
         self.lr = state["lr"]
         self.rng.bit_generator.state = state["rng"]
         self.order = z["order"]
+
+
+class DataParallelTrainer(Trainer):
+    """Data-parallel :class:`Trainer`: one replica per rank of a process group
+    (NCCL between GPUs), every rank holding the whole dataset and the same
+    network state.
+
+    Every rank draws the same global batch from the same shuffled order and
+    takes its contiguous part (rank r of R: positions r*b//R .. (r+1)*b//R).
+    A step computes the rank's gradient record (``pt_unet_grad_record``),
+    all-gathers the records in rank order and applies them with
+    ``pt_unet_apply_records``, which sums them in that fixed order; so all
+    ranks take the same step bit for bit, a rerun repeats it bit for bit, and
+    the step is the whole batch's gradient up to fp64 summation order. With
+    one rank it is :class:`Trainer` exactly.
+
+    `net` needs ``features``, ``param_count``, ``grad_record`` and
+    ``apply_records`` (a :class:`UNet`); :meth:`save` writes from rank 0 only."""
+
+    def __init__(self, net, data: Dataset, *, group=None, batch: int = 64, lr: float = 1e-3, seed: int = 0):
+        import torch.distributed as dist
+        super().__init__(net, data, batch=batch, lr=lr, seed=seed)
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        if self.world > batch:
+            raise ValueError("more ranks than samples in a batch")
+        torch = _torch()
+        dev = data.guidance.device
+        self._rec = torch.empty(net.param_count + 1, dtype=torch.float32, device=dev)
+        # flat gather targets (gloo wants them flat), viewed rank-major
+        self._records = torch.empty(self.world * (net.param_count + 1), dtype=torch.float32, device=dev)
+        self._loss = torch.zeros(2, dtype=torch.float64, device=dev)
+        self._losses = torch.empty(self.world * 2, dtype=torch.float64, device=dev)
+
+    def local_slice(self):
+        """Positions of this rank's samples within a global batch."""
+        return self.rank * self.batch // self.world, (self.rank + 1) * self.batch // self.world
+
+    def step(self) -> float:
+        """One data-parallel step; returns the whole batch's loss (the interior-weighted
+        mean of the ranks' losses)."""
+        import torch.distributed as dist
+        torch = _torch()
+        d = self.data
+        lo, hi = self.local_slice()
+        idx = torch.as_tensor(self._next_indices()[lo:hi], device=d.guidance.device)
+        g = d.guidance[idx].contiguous()
+        a = d.anchor[idx].contiguous()
+        m = d.mask[idx].contiguous()
+        target = (d.solution[idx] - g).contiguous()
+        f = self.net.features(g, a, m)
+        lm = interior_mask(m)
+        cuda = g.is_cuda
+        if cuda:
+            torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, rec = self.net.grad_record(f, target, lm, out=self._rec)
+        dist.all_gather_into_tensor(self._records, rec, group=self.group)
+        self.net.apply_records(self._records.view(self.world, -1), self.lr)
+        if cuda:
+            torch.cuda.synchronize()
+        self.step_s += time.perf_counter() - t0
+        self.steps += 1
+        # whole-batch loss from the ranks' losses and interior counts, in rank order
+        self._loss[0] = loss
+        self._loss[1] = float(rec[-1])
+        dist.all_gather_into_tensor(self._losses, self._loss, group=self.group)
+        lc = self._losses.view(self.world, 2).cpu().numpy()
+        num = 0.0
+        for r in range(self.world):
+            num += lc[r, 0] * lc[r, 1]
+        return num / max(1.0, float(lc[:, 1].sum()))
+
+    def save(self, path: str) -> None:
+        if self.rank == 0:
+            super().save(path)
+
+
+def build_dataset_sharded(ctx, n: int = 20000, size: int = 256, seed: int = 0, chunk: int = 512,
+                          tol: float = 1e-7, group=None) -> Dataset:
+    """:func:`build_dataset` with its chunks solved round-robin over the ranks of
+    `group` and broadcast from their owners in chunk order: every rank ends with
+    the single-process dataset (the chunks are seeded by position, and each
+    solve depends only on its own instance)."""
+    import torch.distributed as dist
+    torch = _torch()
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    starts = list(range(0, n, chunk))
+    mine = {c0: build_dataset(ctx, n=min(chunk, n - c0), size=size, seed=0, chunk=chunk, tol=tol,
+                              _seed_base=seed * 1000003 + c0)
+            for j, c0 in enumerate(starts) if j % world == rank}
+    gs, an, ms, us = [], [], [], []
+    sweeps = np.zeros(n, dtype=np.int64)
+    gen_s = solve_s = 0.0
+    for j, c0 in enumerate(starts):
+        k = min(chunk, n - c0)
+        if c0 in mine:
+            part = mine[c0]
+            tens = [part.guidance, part.anchor, part.mask, part.solution]
+            sw = torch.as_tensor(part.sweeps, device=dev)
+            gen_s += part.gen_s
+            solve_s += part.solve_s
+        else:
+            tens = [torch.empty((k, size, size), dtype=torch.float32, device=dev) for _ in range(4)]
+            sw = torch.empty(k, dtype=torch.int64, device=dev)
+        src = dist.get_global_rank(group, j % world) if group is not None else j % world
+        for t in tens + [sw]:
+            dist.broadcast(t, src=src, group=group)
+        gs.append(tens[0]); an.append(tens[1]); ms.append(tens[2]); us.append(tens[3])
+        sweeps[c0:c0 + k] = sw.cpu().numpy()
+    return Dataset(torch.cat(gs), torch.cat(an), torch.cat(ms), torch.cat(us), sweeps, gen_s, solve_s)
 
 
 def train(net: UNet, data: Dataset, *, epochs: int = 4, batch: int = 64, lr: float = 1e-3,

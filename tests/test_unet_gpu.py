@@ -151,3 +151,71 @@ def test_shape_checks(ctx, ws, torch_cuda):
     with pytest.raises(_lib.CudaError) as e:
         net.forward(f)  # 20 is not a multiple of 8
     assert e.value.status == _lib.PT_INVALID_ARG
+
+
+def test_one_gradient_record_is_a_training_step(ctx, ws, torch_cuda):
+    """grad_record then apply_records with one record repeats train_step bit for bit."""
+    g, a, m = _realistic(ws, torch_cuda, 4, 64, 64, seed=14)
+    lm = ws.interior_mask(m)
+    nets = [ws.UNet(ctx, seed=15) for _ in range(2)]
+    f = nets[0].features(g, a, m)
+    for _ in range(3):
+        la = nets[0].train_step(f, a, lm, 1e-3)
+        lb, rec = nets[1].grad_record(f, a, lm)
+        nets[1].apply_records(rec.view(1, -1), 1e-3)
+        assert la == lb
+    assert np.array_equal(nets[0].get_params().view(np.uint32), nets[1].get_params().view(np.uint32))
+
+
+def test_gradient_records_combine_in_replica_order(ctx, ws, torch_cuda):
+    """Two replicas' records (halves of a batch with different interior counts)
+    combine to c0 g0 + c1 g1 over c0 + c1 summed in fp64 in replica order, which
+    is the whole batch's gradient up to the bf16 rounding of each half's backward."""
+    torch = torch_cuda
+    g, a, m = _realistic(ws, torch, 4, 64, 64, seed=16)
+    m[2:, 20:40, 10:50] = 0.0  # uneven interior counts
+    lm = ws.interior_mask(m)
+    net = ws.UNet(ctx, seed=17)
+    f = net.features(g, a, m)
+    P = net.param_count
+    recs = torch.empty((2, P + 1), dtype=torch.float32, device="cuda")
+    net.grad_record(f[:2].contiguous(), a[:2].contiguous(), lm[:2].contiguous(), out=recs[0])
+    net.grad_record(f[2:].contiguous(), a[2:].contiguous(), lm[2:].contiguous(), out=recs[1])
+    _, full = net.grad_record(f, a, lm)
+    r = recs.cpu().numpy().astype(np.float64)
+    c = r[:, -1]
+    assert c[0] != c[1] and c[0] + c[1] == float(full[-1])
+    acc = np.zeros(P)
+    for k in range(2):
+        acc = acc + c[k] * r[k, :-1]
+    comb = (acc / (c[0] + c[1])).astype(np.float32)
+    layout, head_w, _ = R.param_layout()
+    fg = full[:-1].cpu().numpy()
+    for l, (w, b, co, ci) in enumerate(layout):
+        assert _rel(comb[w:b], fg[w:b]) < 3e-2, l
+    # the device combination is that fp64 sum bit for bit: the same step as one
+    # record that already holds it
+    one = torch.from_numpy(np.append(comb, np.float32(c[0] + c[1]))).cuda().view(1, -1)
+    other = ws.UNet(ctx, seed=17)
+    net.apply_records(recs, 1e-3)
+    other.apply_records(one, 1e-3)
+    assert np.array_equal(net.get_params().view(np.uint32), other.get_params().view(np.uint32))
+
+
+def test_data_parallel_trainer_over_nccl(ctx, ws, torch_cuda):
+    """DataParallelTrainer over a one-rank NCCL group is Trainer bit for bit."""
+    import torch.distributed as dist
+    torch = torch_cuda
+    data = ws.build_dataset(ctx, n=16, size=64, seed=3, chunk=16)
+    dist.init_process_group("nccl", store=dist.HashStore(), rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        a, b = ws.UNet(ctx, seed=18), ws.UNet(ctx, seed=18)
+        ta = ws.Trainer(a, data, batch=8, lr=1e-3, seed=4)
+        tb = ws.DataParallelTrainer(b, data, batch=8, lr=1e-3, seed=4)
+        la = [ta.step() for _ in range(3)]
+        lb = [tb.step() for _ in range(3)]
+    finally:
+        dist.destroy_process_group()
+    assert lb == pytest.approx(la, rel=1e-12)  # the count-weighted mean of one loss
+    assert np.array_equal(a.get_params().view(np.uint32), b.get_params().view(np.uint32))
