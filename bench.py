@@ -14,6 +14,10 @@ Arms:
                      region.
   learned_warm_start (N=1) solves/s of U-Net guess + SOR vs plain SOR on the
                      same 4096x4096 RGB, 8-polygon inputs (``learned_leg``).
+  --workload masks   the 4096x4096 workload's 8 polygon masks (``mask_arm``).
+  mask_raster        (N=1) the workloads' polygon masks rasterised on the device
+                     (mask.polygon@1 semantics, ``mask_leg``) beside the
+                     oracle's single-core rasteriser.
   --impl reference   the reference op's CPU algorithm (the oracle restatement of
                      crates/paintop-cpu/src/poisson.rs) on the host cores, one
                      channel solve per step as a bounded sample.
@@ -201,6 +205,163 @@ def cpu_baseline_sample(inst):
             "sample": f"one full {W}x{H}x{C} solve ({dt:.1f} s) of the restated reference op"}
 
 
+def mask_leg(ctx, dev, peak_gbs, reps: int = 20):
+    """Device rasterisation (pt_mask_polygon, device pointers) of the workloads'
+    masks: the 12-vertex star of the 2048x2048 screened solve and the 8 polygons
+    of the 4096x4096 learned-warm-start workload (one launch per polygon into
+    its own plane). CUDA events over `reps` repetitions after 3 warm-ups; the
+    output planes (16.8 MB / 537 MB) are written anew each repetition."""
+    import torch
+    from paintop_b200 import masks, synth
+    st = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    out = {}
+    for name, inst in (("star_2048", synth.screened_2048(1)), ("polygons8_4096", synth.multi_4096(1))):
+        W, H = inst.width, inst.height
+        planes = torch.empty((len(inst.polygons), H, W), dtype=torch.float32, device=dev)
+
+        def run():
+            for k, pts in enumerate(inst.polygons):
+                masks.polygon(ctx, W, H, pts, out=planes[k])
+        for _ in range(3):
+            run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            run()
+        e1.record(st)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        px = len(inst.polygons) * W * H
+        gbs = 4.0 * px / t / 1e9
+        # the union of the planes is the workload's mask up to the generator's
+        # own (non-fused) crossing arithmetic: report the share of pixels that agree
+        union = planes.amax(0).cpu().numpy()
+        out[name] = {"extent": [W, H], "polygons": len(inst.polygons),
+                     "vertices": [len(p) for p in inst.polygons], "us_per_mask": t * 1e6,
+                     "mpx_per_s": px / t / 1e6, "write_gbs": gbs, "write_frac_of_hbm": gbs / peak_gbs,
+                     "agree_with_workload_mask": float((union == inst.mask).mean())}
+        del planes
+    return out
+
+
+def mask_arm(args):
+    """Mask workload: the 8 polygon masks of the 4096x4096 learned-warm-start
+    workload rasterised with mask.polygon@1 semantics, one pt_mask_polygon call
+    per polygon into its own 4096x4096 plane (537 MB per step, larger than L2).
+    A step = the 8 masks. `value`: pixels/s with the planes in HBM (device
+    pointers); `e2e`: the same calls writing pinned host buffers. Every rank
+    rasterises its own 8 (weak scaling)."""
+    import ctypes as Ct
+    import torch
+    from paintop_b200 import _lib, synth
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    L = _lib.lib()
+    ctx = _lib.Context(dev.index)
+    inst = synth.multi_4096(1)
+    W, H, P = inst.width, inst.height, len(inst.polygons)
+    pts = [np.ascontiguousarray(np.asarray(p, dtype=np.float64)) for p in inst.polygons]
+    planes = torch.empty((P, H, W), dtype=torch.float32, device=dev)
+    host = torch.empty((P, H, W), dtype=torch.float32).pin_memory()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def step(device_out):
+        kms = 0.0
+        for k in range(P):
+            dst = planes[k] if device_out else host[k]
+            st = L.pt_mask_polygon(ctx.h, W, H, pts[k].ctypes.data_as(Ct.c_void_p), pts[k].shape[0],
+                                   _lib.PT_FILL_NONZERO, dst.data_ptr(),
+                                   _lib.PT_FLAG_DEVICE_POINTERS if device_out else 0)
+            if st != _lib.PT_OK:
+                raise _lib.CudaError(st, ctx.last_error())
+            kms += ctx.last_timing()[0]
+        return kms
+
+    def timed(device_out):
+        for _ in range(args.warmup):
+            step(device_out)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kms = []
+        a.record(stream)
+        for _ in range(args.steps):
+            kms.append(step(device_out))
+        b.record(stream)
+        b.synchronize()
+        el = a.elapsed_time(b) / 1e3
+        if ws > 1:
+            import torch.distributed as dist
+            t = torch.tensor([el], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        return el, kms
+
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    elapsed, kms = timed(True)
+    clocks = sampler.stop()
+    e2e_elapsed, _ = timed(False)
+    px = P * W * H
+    peak, peak_kind = _peaks()
+    kernel_s = float(np.mean(kms)) / 1e3 / P        # one launch = one 4096x4096 plane
+    achieved = 4.0 * W * H / kernel_s / 1e9
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            from oracle import oracle as O
+            t0 = time.perf_counter()
+            O.mask_polygon(W, H, inst.polygons[0])
+            dt = time.perf_counter() - t0
+            cpu = {"value": W * H / dt, "unit": "px/s", "cores": 1, "kind": "port",
+                   "sample": f"polygon 0 of 8 on its 4096x4096 plane ({dt:.1f} s), the oracle's rasterize()"}
+        line = {
+            "metric": "mask.polygon px/s (8 polygons of 8-13 vertices, 4096x4096 planes)",
+            "value": ws * px * args.steps / elapsed, "unit": "px/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded polygons)",
+            "config": {"workload": "polygons8_4096", "width": W, "height": H, "polygons": P,
+                       "vertices": [len(p) for p in inst.polygons], "subsamples": 16,
+                       "l2": "output planes larger than L2 (537 MB per step)"},
+            "e2e": {"value": ws * px * args.steps / e2e_elapsed, "unit": "px/s", "h2d_bytes_per_step":
+                    int(sum(p.nbytes for p in pts)), "d2h_bytes_per_step": 4 * px},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_mask_polygon",
+                         "peak_kind": peak_kind, "kernel_us_mean": kernel_s * 1e6,
+                         "algorithmic_bytes_per_launch": 4 * W * H},
+            "cpu_baseline": cpu, "gpu_launches": P * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def mask_cpu_baseline():
+    """The oracle's mask.polygon (the reference's rasterize(), one host core) on
+    the 2048x2048 star."""
+    from oracle import oracle as O
+    from paintop_b200 import synth
+    inst = synth.screened_2048(1)
+    t0 = time.perf_counter()
+    O.mask_polygon(inst.width, inst.height, inst.polygons[0])
+    dt = time.perf_counter() - t0
+    return {"mpx_per_s": inst.width * inst.height / dt / 1e6, "cores": 1, "kind": "port",
+            "sample": f"one 2048x2048 star mask ({dt:.2f} s)"}
+
+
 def gpu_arm(args):
     import torch
     ws, rank, local = _dist()
@@ -329,6 +490,11 @@ def gpu_arm(args):
     learned = None
     if ws == 1 and not args.no_learned and not args.device_only:
         learned = learned_leg(ctx, dev)  # reported apart; outside the timed region above
+    mask_raster = None
+    if ws == 1 and not args.device_only:
+        mask_raster = mask_leg(ctx, dev, peak)
+        if not args.no_cpu_baseline:
+            mask_raster["cpu_baseline"] = mask_cpu_baseline()
 
     line = None
     if rank == 0:
@@ -358,6 +524,7 @@ def gpu_arm(args):
             "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
                        "converged": converged, "worst_final_residual": worst_res},
             "learned_warm_start": learned,
+            "mask_raster": mask_raster,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -588,7 +755,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--device-only", action="store_true",
                     help="time only the device-resident arm (for profiler runs)")
-    ap.add_argument("--workload", default="screened_2048", choices=["screened_2048", "batch_uneven"])
+    ap.add_argument("--workload", default="screened_2048", choices=["screened_2048", "batch_uneven", "masks"])
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-warm-start leg (4096x4096 RGB, learned vs plain)")
@@ -599,6 +766,8 @@ def main():
         return reference_arm(args)
     if args.workload == "batch_uneven":
         return batch_arm(args)
+    if args.workload == "masks":
+        return mask_arm(args)
     return gpu_arm(args)
 
 

@@ -17,7 +17,11 @@
  *                           image per op call)
  *   pt_op_compute           replaces PoissonBlend::compute / ScreenedPoisson::compute
  *                           (poisson_blend.rs:534-600, screened_poisson.rs:361-430)
- *                           including resolve_controls / check_shapes validation
+ *                           including resolve_controls / check_shapes validation,
+ *                           and EllipseMask::compute / PolygonMask::compute
+ *                           (ellipse.rs:506-540, mask_polygon.rs:427-452)
+ *   pt_mask_ellipse         replaces ellipse.rs rasterize (:545-565)
+ *   pt_mask_polygon         replaces mask_polygon.rs rasterize (:259-286)
  *                           (poisson_blend.rs:102-139,417-445; screened_poisson.rs:66-112)
  *   pt_status_str           message for a status code (the reference's typed
  *                           errors: crates/paintop-ir/src/error.rs:23-114)
@@ -125,6 +129,34 @@ pt_status pt_poisson_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n,
                                  float *const *outs, pt_report *const *reports,
                                  double *const *histories);
 
+/* ---- mask generators (mask.ellipse@1, mask.polygon@1) ---------------------
+ * The masks the solve consumes, made on the device so that a mask produced by
+ * a plan node needs no host round trip. `mask` is width*height f32 coverage,
+ * row-major; a device pointer when flags has PT_FLAG_DEVICE_POINTERS, else
+ * host memory. Geometry is in pixel coordinates, pixel (i, j) spanning
+ * [i, i+1) x [j, j+1). Non-finite geometry, a radius <= 0 or a negative
+ * half-width is PT_INVALID_ARG (the op layer, pt_op_compute, reports the
+ * reference's messages for them). */
+
+/* mask.ellipse@1 (crates/paintop-cpu/src/ellipse.rs:168-218,545-565): the
+ * analytic coverage at each pixel centre, a smoothstep feather of half-width
+ * half_width_px about the first-order signed distance (0: hard, half-open
+ * edge). Within the reference's tolerance (its hypot's last bit may differ). */
+pt_status pt_mask_ellipse(pt_ctx *ctx, uint32_t width, uint32_t height, double center_x,
+                          double center_y, double radius_x, double radius_y, double angle_rad,
+                          double half_width_px, float *mask, uint32_t flags);
+
+#define PT_FILL_NONZERO 0
+#define PT_FILL_EVEN_ODD 1
+
+/* mask.polygon@1 (crates/paintop-cpu/src/mask_polygon.rs:161-196,259-286): the
+ * fraction of each pixel's 4 x 4 subsamples inside the polygon (vertices
+ * points_xy[2k], points_xy[2k+1], closed implicitly) by the half-open +x ray
+ * cast under fill_rule (PT_FILL_*). Fewer than 3 vertices give an all-zero
+ * mask. Bit-identical to the reference. */
+pt_status pt_mask_polygon(pt_ctx *ctx, uint32_t width, uint32_t height, const double *points_xy,
+                          uint32_t n_points, int32_t fill_rule, float *mask, uint32_t flags);
+
 /* ---- op-level entry (the OpImplementation::compute seam) ------------------ */
 
 /* Resource kinds of an input port (crates/paintop-ir ResourceKind). */
@@ -195,9 +227,10 @@ pt_status pt_ctx_set_budget(pt_ctx *ctx, double seconds);
  * work or events with the library's. */
 void *pt_ctx_stream(const pt_ctx *ctx);
 
-/* Timing of the context's last solve, from CUDA events on its stream: the
- * persistent solve kernel alone, the whole call (first upload to last
- * download), and the number of kernels the call launched. */
+/* Timing of the context's last solve or mask call, from CUDA events on its
+ * stream: its main kernel alone (the persistent solve kernel, or the mask
+ * rasteriser), the whole call (first upload to last download), and the number
+ * of kernels the call launched. */
 pt_status pt_ctx_last_timing(const pt_ctx *ctx, double *solve_kernel_ms, double *call_ms,
                              int64_t *kernel_launches);
 

@@ -8,6 +8,8 @@ Wraps ``oracle/_build/libpaintop_oracle.so`` (built by ``oracle/Makefile``):
   (crates/paintop-cpu/src/poisson_blend.rs:168-246) on interleaved f32 images.
 * :func:`cg_blend_channels` -- the FP64 CG tight oracle on the same system.
 * :func:`rb_blend_channels` -- FP64 red-black SOR: the GPU method in FP64.
+* :func:`mask_ellipse`, :func:`mask_polygon` -- the ``mask.ellipse@1`` and
+  ``mask.polygon@1`` generators (``oracle/mask_ref.c``).
 
 The C restatement is checked bit-for-bit against the pure-Python restatement in
 ``oracle/pyref.py`` and against the reference's analytic known-answer tests.
@@ -80,8 +82,8 @@ def build() -> None:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
-            build()
+        if not os.path.exists(_LIB_PATH) or os.path.exists(os.path.join(_HERE, "Makefile")):
+            build()  # a no-op when the library is newer than every source
         L = C.CDLL(_LIB_PATH)
         L.pr_classify_cells.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p]
         L.pr_classify_cells.restype = None
@@ -106,6 +108,10 @@ def lib():
                                            C.c_size_t, C.c_size_t, _Controls, C.c_double,
                                            C.c_void_p, C.POINTER(_Report), C.c_void_p]
         L.pr_rb_blend_channels.restype = C.c_int
+        L.or_mask_ellipse.argtypes = [C.c_uint32, C.c_uint32] + [C.c_double] * 6 + [C.c_void_p]
+        L.or_mask_ellipse.restype = None
+        L.or_mask_polygon.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+        L.or_mask_polygon.restype = None
         _lib = L
     return _lib
 
@@ -222,3 +228,21 @@ def cg_blend_channels(source, target, mask, channels, width, height, lam=0.0, re
     if it < 0:
         raise MemoryError("oracle allocation failed")
     return out, ach[:channels]
+
+
+def mask_ellipse(width, height, center, radii, angle_rad=0.0, half_width_px=0.0) -> np.ndarray:
+    """``mask.ellipse@1`` coverage (height, width) f32 (ellipse.rs:168-218,545-565)."""
+    out = np.empty((height, width), dtype=np.float32)
+    lib().or_mask_ellipse(width, height, float(center[0]), float(center[1]), float(radii[0]),
+                          float(radii[1]), float(angle_rad), float(half_width_px), _p(out))
+    return out
+
+
+def mask_polygon(width, height, points, fill_rule="nonzero") -> np.ndarray:
+    """``mask.polygon@1`` coverage (height, width) f32, 4x4 supersampled, half-open
+    (mask_polygon.rs:161-196,259-286)."""
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 2))
+    out = np.empty((height, width), dtype=np.float32)
+    rule = {"nonzero": 0, "even-odd": 1}[fill_rule]
+    lib().or_mask_polygon(width, height, _p(pts), pts.shape[0], rule, _p(out))
+    return out

@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "libpaintop_cuda.so")
 PT_OK, PT_NO_DEVICE, PT_INVALID_ARG, PT_LAUNCH_FAILED, PT_TIMEOUT, PT_OOM, PT_INTERNAL = range(7)
 PT_FLAG_WARM_START = 0x1
 PT_FLAG_DEVICE_POINTERS = 0x2
+PT_FILL_NONZERO, PT_FILL_EVEN_ODD = 0, 1
 PT_FLAG_OMEGA_AUTO = 0x4
 PT_KIND_IMAGE, PT_KIND_MASK = 0, 1
 STOP_REASONS = ("converged", "max-iterations", "stalled")
@@ -31,7 +32,7 @@ EXPORTED = (
     "pt_unet_create", "pt_unet_destroy", "pt_unet_param_count", "pt_unet_get_params",
     "pt_unet_set_params", "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad",
     "pt_unet_train_step", "pt_unet_save", "pt_unet_load", "pt_unet_guess", "pt_unet_grad_record",
-    "pt_unet_apply_records",
+    "pt_unet_apply_records", "pt_mask_ellipse", "pt_mask_polygon",
 )
 PT_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
@@ -152,6 +153,11 @@ def lib():
     L.pt_unet_loss_grad.argtypes = [vp, vp, vp, vp, u32, u32, u32, C.POINTER(C.c_double), vp]
     L.pt_unet_train_step.argtypes = [vp, vp, vp, vp, u32, u32, u32, f32, C.POINTER(C.c_double)]
     L.pt_unet_guess.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, vp]
+    d = C.c_double
+    L.pt_mask_ellipse.argtypes = [vp, u32, u32, d, d, d, d, d, d, vp, u32]
+    L.pt_mask_ellipse.restype = C.c_int
+    L.pt_mask_polygon.argtypes = [vp, u32, u32, vp, u32, C.c_int32, vp, u32]
+    L.pt_mask_polygon.restype = C.c_int
     L.pt_unet_grad_record.argtypes = [vp, vp, vp, vp, u32, u32, u32, C.POINTER(C.c_double), vp]
     L.pt_unet_apply_records.argtypes = [vp, vp, u32, f32]
     L.pt_unet_save.argtypes = [vp, C.c_char_p]
@@ -338,11 +344,14 @@ class Context:
             nm = name.encode()
             keep.append(nm)
             ports[k] = PtPort(nm, kind, w, h, c, s.ctypes.data, s.size)
-        # output is the target/anchor descriptor
+        # output is the target/anchor descriptor (a mask generator's: extent_from's extent)
         for name in ("target", "anchor"):
             if name in inputs:
                 _, w, h, c, _ = inputs[name]
                 out_shape = (w, h, c)
+        if op_id.startswith("mask.") and "extent_from" in inputs:
+            _, w, h, _, _ = inputs["extent_from"]
+            out_shape = (w, h, 1)
         count = out_shape[0] * out_shape[1] * out_shape[2] if out_shape else 0
         cand = np.empty(max(count, 1), dtype=np.float32)
         sd = PtSolverData()

@@ -1,5 +1,6 @@
 // op_host.cpp -- C++ host side of the `cuda` backend, mirroring the reference's
-// operator interface for the two Poisson ops.
+// operator interface for the two Poisson ops and the two mask generators
+// whose output they consume (mask.ellipse@1, mask.polygon@1).
 //
 // The reference's op body is `OpImplementation::compute(&InputValues, &Value)`
 // (crates/paintop-core/src/executor/op_impl.rs:51-70), implemented by
@@ -42,6 +43,7 @@ struct JsonValue {
   std::string str;
   std::string lexeme;  // source text, for error context
   std::map<std::string, JsonValue> members;
+  std::vector<JsonValue> items;  // array elements, in order
 
   // serde_json::Value::as_u64
   bool as_u64(uint64_t *out) const {
@@ -192,6 +194,7 @@ class JsonParser {
       for (;;) {
         JsonValue child;
         if (!value(&child, depth + 1)) return false;
+        v->items.push_back(std::move(child));
         ws();
         if (*p_ == ',') { ++p_; continue; }
         if (*p_ == ']') { ++p_; break; }
@@ -306,6 +309,222 @@ void set_error(pt_error *e, const OpError &o) {
   std::snprintf(e->actual, sizeof(e->actual), "%s", o.actual.c_str());
 }
 
+// ---------------------------------------------------------------------------
+// mask.ellipse@1 and mask.polygon@1 (the generators the solve's masks come from)
+// ---------------------------------------------------------------------------
+
+// Rust's Display for f64: the shortest digits that round-trip, written out
+// positionally (never an exponent), "-0" for negative zero.
+std::string rust_f64(double v) {
+  if (v == 0.0) return std::signbit(v) ? "-0" : "0";
+  if (!std::isfinite(v)) return std::isnan(v) ? "NaN" : (v > 0 ? "inf" : "-inf");
+  char buf[48];
+  for (int p = 0; p < 17; ++p) {
+    std::snprintf(buf, sizeof buf, "%.*e", p, v);
+    if (std::strtod(buf, nullptr) == v) break;
+  }
+  std::string s(buf);
+  const bool neg = s[0] == '-';
+  if (neg) s.erase(0, 1);
+  const size_t e = s.find('e');
+  const int point = std::atoi(s.c_str() + e + 1) + 1;  // digits before the decimal point
+  std::string digits;
+  for (size_t k = 0; k < e; ++k)
+    if (s[k] != '.') digits.push_back(s[k]);
+  std::string out;
+  if (point <= 0) out = "0." + std::string((size_t)-point, '0') + digits;
+  else if (point >= (int)digits.size()) out = digits + std::string((size_t)point - digits.size(), '0');
+  else out = digits.substr(0, (size_t)point) + "." + digits.substr((size_t)point);
+  return (neg ? "-" : "") + out;
+}
+
+struct EllipseParams {
+  double cx = 0, cy = 0, rx = 0, ry = 0, angle = 0, half = 0;
+};
+
+OpError ellipse_param_error(const std::string &name, const std::string &detail, const std::string &actual) {
+  // ellipse.rs param_error
+  return OpError{"schema", "E_ELLIPSE_PARAM", "mask.ellipse parameter `" + name + "`: " + detail, actual};
+}
+
+// finite_number (ellipse.rs): a number, and finite
+bool ellipse_number(const JsonValue &v, const std::string &name, double *out, OpError *err) {
+  if (!v.as_f64(out)) { *err = ellipse_param_error(name, "must be a number", v.lexeme); return false; }
+  if (!std::isfinite(*out)) { *err = ellipse_param_error(name, "must be finite", v.lexeme); return false; }
+  return true;
+}
+
+bool ellipse_pair(const JsonValue &params, const char *name, double *x, double *y, OpError *err) {
+  const JsonValue *v = params.get(name);
+  if (!v) { *err = ellipse_param_error(name, "missing required parameter", "null"); return false; }
+  if (v->type != JsonValue::Array) { *err = ellipse_param_error(name, "must be a [x, y] array", v->lexeme); return false; }
+  if (v->items.size() != 2) {
+    *err = ellipse_param_error(name, "must have exactly two elements", v->lexeme);
+    return false;
+  }
+  return ellipse_number(v->items[0], name, x, err) && ellipse_number(v->items[1], name, y, err);
+}
+
+// EllipseGeometry::resolve, pair_param, finite_number and parse_edge
+// (ellipse.rs:119-159, :221-252, :261-297)
+bool resolve_ellipse(const JsonValue &params, EllipseParams *g, OpError *err) {
+  if (!ellipse_pair(params, "center_px", &g->cx, &g->cy, err)) return false;
+  if (!ellipse_pair(params, "radii_px", &g->rx, &g->ry, err)) return false;
+  const std::pair<const char *, double> radii[2] = {{"radii_px.x", g->rx}, {"radii_px.y", g->ry}};
+  for (const auto &r : radii)
+    if (!(std::isfinite(r.second) && r.second > 0.0)) {
+      *err = OpError{"schema", "E_ELLIPSE_PARAM",
+                     std::string("mask.ellipse `") + r.first + "` must be a strictly positive radius, got " +
+                         rust_f64(r.second),
+                     rust_f64(r.second)};
+      return false;
+    }
+  g->angle = 0.0;
+  if (const JsonValue *v = params.get("angle_rad"))
+    if (!ellipse_number(*v, "angle_rad", &g->angle, err)) return false;
+  if (const JsonValue *v = params.get("antialias")) {
+    if (v->type != JsonValue::String) {
+      *err = ellipse_param_error("antialias", "`antialias` must be a string", v->lexeme);
+      return false;
+    }
+    if (v->str != "analytic") {
+      *err = OpError{"schema", "E_ELLIPSE_PARAM",
+                     "mask.ellipse only supports `antialias: analytic`, got `" + v->str + "`", ""};
+      return false;
+    }
+  }
+  g->half = 0.0;
+  if (const JsonValue *edge = params.get("edge")) {
+    if (edge->type != JsonValue::Object) {
+      *err = ellipse_param_error("edge", "`edge` must be an object", edge->lexeme);
+      return false;
+    }
+    const JsonValue *profile = edge->get("profile");
+    if (!profile || profile->type != JsonValue::String) {
+      *err = ellipse_param_error("edge.profile", "`edge.profile` must be a string", edge->lexeme);
+      return false;
+    }
+    if (profile->str != "smoothstep") {
+      *err = OpError{"schema", "E_ELLIPSE_PARAM",
+                     "mask.ellipse only supports `edge.profile: smoothstep`, got `" + profile->str + "`", ""};
+      return false;
+    }
+    const JsonValue *half = edge->get("half_width_px");
+    if (!half) {
+      *err = ellipse_param_error("edge.half_width_px", "`edge.half_width_px` is required", edge->lexeme);
+      return false;
+    }
+    if (!ellipse_number(*half, "edge.half_width_px", &g->half, err)) return false;
+    if (g->half < 0.0) {
+      *err = ellipse_param_error("edge.half_width_px", "must be non-negative", half->lexeme);
+      return false;
+    }
+  }
+  return true;
+}
+
+OpError polygon_param_error(const std::string &detail, const std::string &actual) {
+  // mask_polygon.rs param_error
+  return OpError{"schema", "E_POLYGON_PARAM", "mask.polygon parameter: " + detail, actual};
+}
+
+// FillRule::resolve and Polygon::resolve (mask_polygon.rs:90-104, :124-152)
+bool resolve_polygon(const JsonValue &params, std::vector<double> *pts, int32_t *rule, OpError *err) {
+  const JsonValue *v = params.get("points");
+  if (!v) {
+    *err = OpError{"schema", "E_POLYGON_PARAM", "mask.polygon requires a `points` array of [x, y] vertices", ""};
+    return false;
+  }
+  if (v->type != JsonValue::Array) {
+    *err = polygon_param_error("`points` must be an array of [x, y] pairs", v->lexeme);
+    return false;
+  }
+  for (const JsonValue &vertex : v->items) {
+    if (vertex.type != JsonValue::Array) {
+      *err = polygon_param_error("each vertex must be a [x, y] array", vertex.lexeme);
+      return false;
+    }
+    if (vertex.items.size() != 2) {
+      *err = polygon_param_error("each vertex must have exactly two elements", vertex.lexeme);
+      return false;
+    }
+    for (const JsonValue &c : vertex.items) {
+      double d;
+      if (!c.as_f64(&d)) { *err = polygon_param_error("coordinates must be numbers", c.lexeme); return false; }
+      if (!std::isfinite(d)) { *err = polygon_param_error("coordinates must be finite", c.lexeme); return false; }
+      pts->push_back(d);
+    }
+  }
+  *rule = PT_FILL_NONZERO;
+  if (const JsonValue *f = params.get("fill_rule")) {
+    if (f->type == JsonValue::String && f->str == "nonzero") *rule = PT_FILL_NONZERO;
+    else if (f->type == JsonValue::String && f->str == "even-odd") *rule = PT_FILL_EVEN_ODD;
+    else {
+      *err = OpError{"schema", "E_POLYGON_PARAM", "mask.polygon `fill_rule` must be `nonzero` or `even-odd`",
+                     f->lexeme};
+      return false;
+    }
+  }
+  return true;
+}
+
+// EllipseMask::compute (ellipse.rs:506-540) and PolygonMask::compute
+// (mask_polygon.rs:427-452): the extent first, then the params, then the
+// rasteriser; the output is the mask (width*height f32) in `candidate`.
+pt_status mask_op_compute(pt_ctx *ctx, bool ellipse, const pt_port *inputs, uint32_t n_inputs,
+                          const char *params_json, float *candidate, size_t candidate_count,
+                          int32_t *all_finite, pt_error *err) {
+  const char *op = ellipse ? "mask.ellipse" : "mask.polygon";
+  const char *e_input = ellipse ? "E_ELLIPSE_INPUT" : "E_POLYGON_INPUT";
+  const char *e_param = ellipse ? "E_ELLIPSE_PARAM" : "E_POLYGON_PARAM";
+  const pt_port *src = find_port(inputs, n_inputs, "extent_from");
+  if (!src) {
+    set_error(err, OpError{"reference", e_input, std::string(op) + " requires an `extent_from` input value", ""});
+    return PT_INVALID_ARG;
+  }
+  JsonValue params;
+  if (params_json && *params_json) {
+    JsonParser jp(params_json);
+    if (!jp.parse(&params)) {
+      set_error(err, OpError{"parse", e_param, std::string(op) + ": params are not valid JSON", ""});
+      return PT_INVALID_ARG;
+    }
+  }
+  OpError oe;
+  EllipseParams g;
+  std::vector<double> pts;
+  int32_t rule = PT_FILL_NONZERO;
+  if (ellipse ? !resolve_ellipse(params, &g, &oe) : !resolve_polygon(params, &pts, &rule, &oe)) {
+    set_error(err, oe);
+    return PT_INVALID_ARG;
+  }
+  const size_t count = (size_t)src->width * src->height;
+  if ((count && !candidate) || candidate_count != count) {
+    set_error(err, OpError{"execution", e_input,
+                           std::string(op) + (ellipse ? " produced a sample buffer" : " produced a mask buffer") +
+                               " of unexpected length " + std::to_string(candidate_count),
+                           ""});
+    return PT_INVALID_ARG;
+  }
+  if (!ctx) {
+    set_error(err, OpError{"policy", "E_CUDA_UNAVAILABLE", std::string(op) + ": the cuda backend has no device context",
+                           ""});
+    return PT_NO_DEVICE;
+  }
+  const pt_status st =
+      ellipse ? pt_mask_ellipse(ctx, src->width, src->height, g.cx, g.cy, g.rx, g.ry, g.angle, g.half, candidate, 0)
+              : pt_mask_polygon(ctx, src->width, src->height, pts.data(), (uint32_t)(pts.size() / 2), rule,
+                                candidate, 0);
+  if (st != PT_OK) {
+    set_error(err, OpError{st == PT_NO_DEVICE ? "policy" : "execution",
+                           st == PT_NO_DEVICE ? "E_CUDA_UNAVAILABLE" : "E_CUDA_EXECUTION",
+                           std::string(op) + ": " + pt_status_str(st) + ": " + pt_ctx_last_error(ctx), ""});
+    return st;
+  }
+  if (all_finite) *all_finite = 1;  // coverage in [0, 1] by construction
+  return PT_OK;
+}
+
 }  // namespace pt_op
 
 using namespace pt_op;
@@ -316,7 +535,11 @@ extern "C" pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port
                                    double *residual_history, uint32_t history_cap,
                                    int32_t *all_finite, pt_error *err) {
   if (err) std::memset(err, 0, sizeof(*err));
-  if (!op_id || (n_inputs && !inputs) || !solver) return PT_INVALID_ARG;
+  if (!op_id || (n_inputs && !inputs)) return PT_INVALID_ARG;
+  if (std::strcmp(op_id, "mask.ellipse@1") == 0 || std::strcmp(op_id, "mask.polygon@1") == 0)
+    return mask_op_compute(ctx, op_id[5] == 'e', inputs, n_inputs, params_json, candidate, candidate_count,
+                           all_finite, err);
+  if (!solver) return PT_INVALID_ARG;
   const OpSpec *spec = nullptr;
   if (std::strcmp(op_id, "repair.poisson_blend@1") == 0) spec = &kBlend;
   else if (std::strcmp(op_id, "repair.screened_poisson@1") == 0) spec = &kScreened;

@@ -1,5 +1,6 @@
 """The ``cuda.poisson@1`` implementation of ``repair.poisson_blend@1`` and
-``repair.screened_poisson@1``, as seen from Python.
+``repair.screened_poisson@1``, and of the mask generators ``mask.ellipse@1``
+and ``mask.polygon@1`` that feed them, as seen from Python.
 
 Mirrors the reference's operator interface: ``compute(inputs, params)`` takes a
 map of port name -> resource value and the op's JSON params and returns the
@@ -156,3 +157,38 @@ class ScreenedPoisson(_PoissonOp):
 
     OP_ID = "repair.screened_poisson@1"
     PORTS = ("guidance", "anchor", "mask")
+
+
+class _MaskOp:
+    """A mask generator: ``compute({"extent_from": value}, params)`` returns
+    ``{"mask": mask value}`` sized to the input's extent."""
+
+    OP_ID = ""
+
+    def compute(self, inputs: dict, params) -> dict:
+        ctx = context()
+        ports = {}
+        for name, v in inputs.items():
+            kind = _lib.PT_KIND_MASK if v.kind == "mask" else _lib.PT_KIND_IMAGE
+            ports[name] = (kind, v.width, v.height, v.channels, v.samples)
+        pj = json.dumps(params) if not isinstance(params, str) else params
+        st, out, _, _, _, err = ctx.op_compute(self.OP_ID, ports, pj)
+        if st != _lib.PT_OK:
+            if err.code:
+                raise PaintopError(err.error_class.decode(), err.code.decode(),
+                                   err.message.decode(), err.actual.decode())
+            raise _lib.CudaError(st, ctx.last_error())
+        src = inputs["extent_from"]
+        return {"mask": mask_value(src.width, src.height, out)}
+
+
+class EllipseMask(_MaskOp):
+    """``mask.ellipse@1`` on the ``cuda`` backend (crates/paintop-cpu/src/ellipse.rs:506-540)."""
+
+    OP_ID = "mask.ellipse@1"
+
+
+class PolygonMask(_MaskOp):
+    """``mask.polygon@1`` on the ``cuda`` backend (crates/paintop-cpu/src/mask_polygon.rs:427-452)."""
+
+    OP_ID = "mask.polygon@1"

@@ -130,6 +130,7 @@ class Instance:
     tolerance: float = 1e-6
     max_iterations: int = 2000
     omega: float = 1.8
+    polygons: list = None  # the polygons (vertex lists) the mask was drawn from
 
     def problem(self, **over) -> dict:
         d = dict(source=self.source, target=self.target, mask=self.mask, width=self.width,
@@ -159,7 +160,7 @@ def screened_2048(seed: int = 1, size: int = 2048) -> Instance:
     r_out = math.sqrt(area / (3.0 * ratio))
     pts = star_polygon(w / 2, h / 2, r_out, ratio * r_out, 12, rng.uniform(0, math.pi / 6))
     mask = polygon_mask(w, h, pts)
-    return Instance(w, h, 4, src, tgt, mask, 0.01, 1e-6, 2000, 1.8)
+    return Instance(w, h, 4, src, tgt, mask, 0.01, 1e-6, 2000, 1.8, [pts])
 
 
 def uneven_instance(rng: np.random.Generator, tol: float = 1e-6) -> Instance:
@@ -205,6 +206,7 @@ def multi_4096(seed: int = 1, size: int = 4096) -> Instance:
     src = sinusoid_image(rng, w, h, 3)
     tgt = sinusoid_image(rng, w, h, 3)
     mask = np.zeros((h, w), dtype=np.float32)
+    polys = []
     cw, ch = w // 4, h // 2           # 8 cells, one polygon each: never overlapping
     for k in range(8):
         gx, gy = k % 4, k // 4
@@ -219,5 +221,6 @@ def multi_4096(seed: int = 1, size: int = 4096) -> Instance:
         fy = (0.5 * ch - 2) / max(max(ys) - cy, cy - min(ys))
         f = min(1.0, fx, fy)
         pts = [(cx + (px - cx) * f, cy + (py - cy) * f) for px, py in pts]
+        polys.append(pts)
         mask = np.maximum(mask, polygon_mask(w, h, pts))
-    return Instance(w, h, 3, src, tgt, mask, 0.0, 1e-6, 100000, 1.8)
+    return Instance(w, h, 3, src, tgt, mask, 0.0, 1e-6, 100000, 1.8, polys)
