@@ -69,6 +69,12 @@ class Report:
     all_finite: bool
     solver: Optional[SolverData] = None
 
+    def to_json(self) -> str:
+        """The canonical JSON an evidence bundle stores for this report
+        (:mod:`paintop_b200.report_json`)."""
+        from .report_json import report_json
+        return report_json(self)
+
 
 @dataclass
 class ResourceValue:

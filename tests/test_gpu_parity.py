@@ -407,3 +407,22 @@ def test_device_pointers_graph_replay_matches_host_path(ctx):
                 assert hh[k * 800: k * 800 + n].tolist() == rper[k]["residual_history"]
         outs.append(got)
     assert np.array_equal(outs[0], outs[3])
+
+
+def test_report_export_carries_the_convergence_record(ops, tmp_path):
+    """The op's report written as a bundle artifact (canonical JSON) holds the
+    solve's convergence metrics: the residual history, one entry per sweep."""
+    import json
+    from paintop_b200.report_json import write_report
+    w = h = 32
+    rng = np.random.default_rng(3)
+    src = rng.uniform(0, 1, w * h).astype(np.float32)
+    tgt = rng.uniform(0, 1, w * h).astype(np.float32)
+    _, rep = run(ops, "screened", w, h, src, tgt, square_mask(w, h, 4, 28), {"lambda": 0.05, "tolerance": 1e-6})
+    rel = write_report(str(tmp_path), "report", rep)
+    v = json.loads((tmp_path / rel).read_text(encoding="utf-8"))
+    s = v["solver"]
+    assert s["kind"] == "screened-poisson" and s["stop_reason"] == "converged" and s["converged"]
+    assert s["iterations"] == s["steps"] == len(s["residual_history"]) > 0
+    assert s["residual_history"][-1] == s["final_residual"] <= 1e-6
+    assert v["extent"] == {"width": w, "height": h} and v["channels"] == 1 and v["all_finite"]
