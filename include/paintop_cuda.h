@@ -65,6 +65,10 @@ typedef enum pt_status {
 #define PT_FLAG_WARM_START 0x1u      /* initial_guess holds the interior start values */
 #define PT_FLAG_DEVICE_POINTERS 0x2u /* every buffer (inputs, outputs, history) is device memory */
 #define PT_FLAG_OMEGA_AUTO 0x4u      /* ignore `omega`; pick the red-black optimum per channel */
+#define PT_FLAG_MULTIGRID 0x8u       /* solve by multigrid-preconditioned CG (FP32) inside FP64
+                                        refinement instead of red-black SOR: the same system,
+                                        bar and report fields; iterations count CG iterations,
+                                        omega is ignored. Every problem of a batch must agree. */
 
 /* Stop reasons: the kebab-case SolverStopReason of
  * crates/paintop-ir/src/resource.rs:1185-1194 in declaration order. */

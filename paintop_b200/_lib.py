@@ -20,6 +20,7 @@ PT_FLAG_WARM_START = 0x1
 PT_FLAG_DEVICE_POINTERS = 0x2
 PT_FILL_NONZERO, PT_FILL_EVEN_ODD = 0, 1
 PT_FLAG_OMEGA_AUTO = 0x4
+PT_FLAG_MULTIGRID = 0x8
 PT_KIND_IMAGE, PT_KIND_MASK = 0, 1
 STOP_REASONS = ("converged", "max-iterations", "stalled")
 

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                    "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
 SOURCES = ["rbsor_kernels.cu", "solver_host.cu", "op_host.cpp", "autotune.cpp", "noalloc.cu",
-           "mask_kernels.cu", "unet/unet_kernels.cu", "unet/conv_tma.cu", "unet/unet.cu"]
+           "mask_kernels.cu", "mg_solver.cu", "unet/unet_kernels.cu", "unet/conv_tma.cu", "unet/unet.cu"]
 
 
 def nvcc() -> str:

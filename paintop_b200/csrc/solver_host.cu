@@ -68,7 +68,7 @@ pt_status validate(pt_ctx *ctx, const pt_problem &p) {
     return fail(ctx, PT_INVALID_ARG, "lambda must be a finite value >= 0");
   if (!finite(p.tolerance) || p.tolerance <= 0.0)
     return fail(ctx, PT_INVALID_ARG, "tolerance must be a finite value > 0");
-  if (!(p.flags & PT_FLAG_OMEGA_AUTO) && (!finite(p.omega) || p.omega <= 0.0 || p.omega >= 2.0))
+  if (!(p.flags & (PT_FLAG_OMEGA_AUTO | PT_FLAG_MULTIGRID)) && (!finite(p.omega) || p.omega <= 0.0 || p.omega >= 2.0))
     return fail(ctx, PT_INVALID_ARG, "omega must be in (0, 2)");
   if (p.max_iterations > 1000000u)
     return fail(ctx, PT_INVALID_ARG, "max_iterations must be <= 1000000");
@@ -137,6 +137,8 @@ Layout layout(const Plan &pl, bool stage) {
 // ---------------------------------------------------------------------------
 int ptk_choose_config(pt_ctx *ctx, const pt_problem *ps, uint32_t n);
 
+pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, pt_report *reports, double *history);
+
 pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
                           pt_report *const *reports, double *const *histories, int force_cfg) {
   if (!ctx) return PT_INVALID_ARG;
@@ -152,6 +154,19 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (fault == 2) return fail(ctx, PT_OOM, "injected: allocation failure");
   if (fault == 3) return fail(ctx, PT_LAUNCH_FAILED, "injected: launch failure");
 
+  const bool mg = n > 0 && (ps[0].flags & PT_FLAG_MULTIGRID);
+  for (uint32_t i = 0; i < n; ++i)
+    if (((ps[i].flags & PT_FLAG_MULTIGRID) != 0) != mg)
+      return fail(ctx, PT_INVALID_ARG, "PT_FLAG_MULTIGRID must agree across a batch");
+  if (mg) {
+    // multigrid-preconditioned CG, one problem at a time (each is already a
+    // sequence of whole-grid launches)
+    for (uint32_t i = 0; i < n; ++i) {
+      const pt_status s = ptk_solve_mg(ctx, ps[i], outs[i], reports[i], histories ? histories[i] : nullptr);
+      if (s != PT_OK) return s;
+    }
+    return PT_OK;
+  }
   const bool devptr = n > 0 && (ps[0].flags & PT_FLAG_DEVICE_POINTERS);
   for (uint32_t i = 0; i < n; ++i)
     if (((ps[i].flags & PT_FLAG_DEVICE_POINTERS) != 0) != devptr)
