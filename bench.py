@@ -12,8 +12,11 @@ Arms:
                      HBM (device pointers); `e2e`: solves/s through the C ABI with
                      pinned host buffers, host<->device copies inside the timed
                      region.
+  multigrid          (N=1) the same inputs through multigrid-preconditioned CG
+                     (PT_FLAG_MULTIGRID, ``multigrid_leg``).
   learned_warm_start (N=1) solves/s of U-Net guess + SOR vs plain SOR on the
-                     same 4096x4096 RGB, 8-polygon inputs (``learned_leg``).
+                     same 4096x4096 RGB, 8-polygon inputs, and of multigrid
+                     with and without the guess (``learned_leg``).
   --workload masks   the 4096x4096 workload's 8 polygon masks (``mask_arm``).
   mask_raster        (N=1) the workloads' polygon masks rasterised on the device
                      (mask.polygon@1 semantics, ``mask_leg``) beside the
@@ -490,6 +493,9 @@ def gpu_arm(args):
     learned = None
     if ws == 1 and not args.no_learned and not args.device_only:
         learned = learned_leg(ctx, dev)  # reported apart; outside the timed region above
+    multigrid = None
+    if ws == 1 and not args.device_only:
+        multigrid = multigrid_leg(ctx, dev, inst)
     mask_raster = None
     if ws == 1 and not args.device_only:
         mask_raster = mask_leg(ctx, dev, peak)
@@ -523,6 +529,7 @@ def gpu_arm(args):
             "clocks": clocks,
             "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
                        "converged": converged, "worst_final_residual": worst_res},
+            "multigrid": multigrid,
             "learned_warm_start": learned,
             "mask_raster": mask_raster,
         }
@@ -710,40 +717,88 @@ def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8):
                              flags, None)
     p_warm = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), 0.0, 100000, 1e-6, 1.8,
                             flags | _lib.PT_FLAG_WARM_START, guess.data_ptr())
+    mgf = _lib.PT_FLAG_DEVICE_POINTERS | _lib.PT_FLAG_MULTIGRID
+    p_mg = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), 0.0, 100000, 1e-6, 1.8, mgf, None)
+    p_mg_warm = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), 0.0, 100000, 1e-6, 1.8,
+                               mgf | _lib.PT_FLAG_WARM_START, guess.data_ptr())
+    problems = {"plain": p_plain, "learned": p_warm, "multigrid": p_mg, "learned_multigrid": p_mg_warm}
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     torch.cuda.synchronize(dev)
 
-    def run(learned: bool):
+    def run(mode: str):
+        learned = mode.startswith("learned")
         if learned:
             st = L.pt_unet_guess(net.h, g.data_ptr(), a.data_ptr(), m.data_ptr(), W, H, C, scale, guess.data_ptr())
             if st != _lib.PT_OK:
                 raise _lib.CudaError(st, ctx.last_error())
-        st = L.pt_poisson_solve(ctx.h, Ct.byref(p_warm if learned else p_plain), out.data_ptr(), reps, None)
+        st = L.pt_poisson_solve(ctx.h, Ct.byref(problems[mode]), out.data_ptr(), reps, None)
         if st != _lib.PT_OK:
             raise _lib.CudaError(st, ctx.last_error())
         return [int(reps[c].iterations) for c in range(C)], all(reps[c].converged for c in range(C)), \
             [bool(reps[c].warm_start) for c in range(C)]
 
     res = {}
-    for learned in (False, True):
+    for mode in problems:
         for _ in range(warmup):
-            run(learned)
+            run(mode)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
-            sweeps, conv, used = run(learned)
+            its, conv, used = run(mode)
         e1.record(stream)
         e1.synchronize()
         sec = e0.elapsed_time(e1) / 1e3 / steps
-        res["learned" if learned else "plain"] = dict(solves_per_s=1.0 / sec, ms_per_solve=sec * 1e3,
-                                                      sweeps=sweeps, converged=conv,
-                                                      **({"guess_used": used} if learned else {}))
+        key = "sweeps" if mode in ("plain", "learned") else "cg_iterations"
+        res[mode] = dict(solves_per_s=1.0 / sec, ms_per_solve=sec * 1e3, **{key: its}, converged=conv,
+                         **({"guess_used": used} if mode.startswith("learned") else {}))
     net.close()
-    return {"workload": "multi_4096: 4096x4096 RGB, 8 polygons 3-10% each, rel-res 1e-6, automatic omega",
+    return {"workload": "multi_4096: 4096x4096 RGB, 8 polygons 3-10% each, rel-res 1e-6, automatic omega for SOR",
             "model": "U-Net 16-32-64-128, bf16, trained on 20,000 256x256 solves; inference pooled x%d" % scale,
             "steps": steps, **res,
-            "speedup": res["learned"]["solves_per_s"] / res["plain"]["solves_per_s"]}
+            "speedup": res["learned"]["solves_per_s"] / res["plain"]["solves_per_s"],
+            "speedup_multigrid": res["multigrid"]["solves_per_s"] / res["plain"]["solves_per_s"],
+            "speedup_learned_multigrid": res["learned_multigrid"]["solves_per_s"] / res["multigrid"]["solves_per_s"]}
+
+
+def multigrid_leg(ctx, dev, inst, steps: int = 3, warmup: int = 1):
+    """The headline workload (same inputs, device pointers) solved by
+    multigrid-preconditioned CG instead of red-black SOR: solves/s (CUDA events
+    on the context stream) and CG iterations per channel."""
+    import ctypes as Ct
+    import torch
+    from paintop_b200 import _lib
+    W, H, C = inst.width, inst.height, inst.channels
+    g = torch.as_tensor(inst.source, device=dev).contiguous()
+    a = torch.as_tensor(inst.target, device=dev).contiguous()
+    m = torch.as_tensor(inst.mask, device=dev).contiguous()
+    out = torch.empty_like(g)
+    reps = (_lib.PtReport * (C + 1))()
+    p = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), WORKLOAD["lam"], WORKLOAD["max_iterations"],
+                       WORKLOAD["tolerance"], WORKLOAD["omega"],
+                       _lib.PT_FLAG_DEVICE_POINTERS | _lib.PT_FLAG_MULTIGRID, None)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    torch.cuda.synchronize(dev)
+
+    def run():
+        st = _lib.lib().pt_poisson_solve(ctx.h, Ct.byref(p), out.data_ptr(), reps, None)
+        if st != _lib.PT_OK:
+            raise _lib.CudaError(st, ctx.last_error())
+    for _ in range(warmup):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        run()
+    e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3 / steps
+    return {"solves_per_s": 1.0 / sec, "ms_per_solve": sec * 1e3,
+            "cg_iterations": [int(reps[c].iterations) for c in range(C)],
+            "refinements": [int(reps[c].refinements) for c in range(C)],
+            "converged": all(reps[c].converged for c in range(C)),
+            "worst_final_residual": max(reps[c].final_residual for c in range(C)),
+            "launches_per_solve": ctx.last_timing()[2]}
 
 
 def main():

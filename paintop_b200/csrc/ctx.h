@@ -26,13 +26,23 @@ struct pt_ctx {
   bool graphs = true;          // capture device-pointer solves into a CUDA graph
   cudaGraphExec_t gexec = nullptr;
   std::string gkey;            // the plan the cached graph was captured for
+  cudaGraphExec_t mgexec[2] = {nullptr, nullptr};  // multigrid-CG iteration: first / later
+  std::string mgkey;           // the problem shape and arena the multigrid graphs were captured for
+  long long mgnodes = 0;       // kernels in one of those iterations
+
+  void drop_graphs() {
+    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }  // they point into the arena
+    gkey.clear();
+    for (auto &g : mgexec)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    mgkey.clear();
+  }
 
   bool reserve(size_t bytes) {
     if (bytes <= arena_cap) return true;
     if (arena) {
       cudaStreamSynchronize(stream);
-      if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }  // it points into the arena
-      gkey.clear();
+      drop_graphs();
       cudaFree(arena);
       arena = nullptr;
       arena_cap = 0;
@@ -53,8 +63,7 @@ struct pt_ctx {
   }
 
   void release() {
-    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
-    gkey.clear();
+    drop_graphs();
     for (auto &e : ev)
       if (e) { cudaEventDestroy(e); e = nullptr; }
     if (arena) cudaFree(arena);

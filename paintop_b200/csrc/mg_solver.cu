@@ -183,6 +183,44 @@ __global__ void k_mg_smooth(int W, int H, const uint8_t *__restrict__ act, const
   }
 }
 
+// The coarsest level (at most kCoarseMax cells): `sweeps` red-black sweeps,
+// then as many in reverse colour order, from e = 0, in shared memory; one
+// block per channel.
+constexpr int kCoarseMax = 64;
+
+__global__ void k_mg_coarse(int W, int H, const uint8_t *__restrict__ act, const float *__restrict__ rhs,
+                            float *__restrict__ e, float s, float d, int sweeps) {
+  __shared__ float se[kCoarseMax], sr[kCoarseMax];
+  __shared__ uint8_t sa[kCoarseMax];
+  const int n = W * H, c = blockIdx.x, t = threadIdx.x;
+  if (t < n) {
+    se[t] = 0.0f;
+    sr[t] = rhs[(long long)c * n + t];
+    sa[t] = act[t];
+  }
+  __syncthreads();
+  const int j = t / max(W, 1), i = t - j * W;
+  for (int k = 0; k < 4 * sweeps; ++k) {
+    // colour order R, B (first half) then B, R (second half)
+    const int half = k / (2 * sweeps), step = k & 1;
+    const int color = half == 0 ? step : 1 - step;
+    float v = 0.0f;
+    const bool mine = t < n && sa[t] && ((i + j) & 1) == color;
+    if (mine) {
+      float nb = 0.0f;
+      if (i > 0) nb += se[t - 1];
+      if (i < W - 1) nb += se[t + 1];
+      if (j > 0) nb += se[t - W];
+      if (j < H - 1) nb += se[t + W];
+      v = (sr[t] + s * nb) / d;
+    }
+    __syncthreads();
+    if (mine) se[t] = v;
+    __syncthreads();
+  }
+  if (t < n) e[(long long)c * n + t] = se[t];
+}
+
 // res = rhs - A_k e at active cells, 0 elsewhere; grid (blocks, C)
 __global__ void k_mg_resid(int W, int H, const uint8_t *__restrict__ act, const float *__restrict__ rhs,
                            const float *__restrict__ e, float s, float d, float *__restrict__ res) {
@@ -306,8 +344,7 @@ __global__ void k_cg_direction(long long N, int C, const float *__restrict__ z, 
 }
 
 __global__ void k_cg_scalars_after_dir(int C, double *__restrict__ sc) {
-  const int c = threadIdx.x;
-  if (c < C) sc[c * S_N + S_RHO] = sc[c * S_N + S_RHO_NEW];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) sc[c * S_N + S_RHO] = sc[c * S_N + S_RHO_NEW];
 }
 
 // x += alpha p, r -= alpha q (alpha = rho / p.q); partial sums of r.r
@@ -381,8 +418,14 @@ void vcycle(Mg &m, size_t rhs0, size_t e0) {
     const size_t rhs = k == 0 ? rhs0 : v.rhs, e = k == 0 ? e0 : v.e;
     const long long N = (long long)v.W * v.H;
     const dim3 gh(blocks((long long)((v.W + 1) / 2) * v.H, sms), m.C), g(blocks(N, sms), m.C);
+    if (k == L - 1) {  // the coarsest level: symmetric sweeps in one block per channel
+      k_mg_coarse<<<m.C, kCoarseMax, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e),
+                                                 v.s, v.d, 24);
+      ++m.launches;
+      break;
+    }
     cudaMemsetAsync(m.at<float>(e), 0, (size_t)N * m.C * sizeof(float), m.st);
-    const int sweeps = k == L - 1 ? 24 : 2;
+    const int sweeps = 2;
     for (int t = 0; t < sweeps; ++t) {
       k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
                                              v.d, 0);
@@ -390,16 +433,6 @@ void vcycle(Mg &m, size_t rhs0, size_t e0) {
                                              v.d, 1);
     }
     m.launches += 1 + 2 * sweeps;
-    if (k == L - 1) {  // the coarsest level: as many sweeps back in reverse colour order
-      for (int t = 0; t < sweeps; ++t) {
-        k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                               v.d, 1);
-        k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                               v.d, 0);
-      }
-      m.launches += 2 * sweeps;
-      break;
-    }
     Level &cl = m.lv[k + 1];
     k_mg_resid<<<g, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
                                          m.at<float>(v.res));
@@ -458,7 +491,7 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
     for (;;) {
       const float s = 1.0f / (float)(1u << (2 * std::min(k, 15)));
       m.lv.push_back(Level{w, h, 0, 0, 0, 0, s, 4.0f * s + (float)p.lambda});
-      if ((long long)w * h <= 64 || (w == 1 && h == 1) || k >= 30) break;
+      if ((long long)w * h <= kCoarseMax || k >= 30) break;
       w = (w + 1) / 2; h = (h + 1) / 2; ++k;
     }
   }
@@ -553,6 +586,57 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
   }
   std::vector<double> hsc(C * S_N, 0.0), hscale(C, 0.0), rr(C);
   const float d0 = m.lv[0].d;
+  // One CG iteration: V-cycle z = M r, rho = r.z, p = z + beta p, q = A p,
+  // alpha = rho / p.q, x += alpha p, r -= alpha q, ||r||^2 (to `red`). Its
+  // launches depend only on the problem's shape and the arena, so they are
+  // captured once into two CUDA graphs (first iteration, later ones) cached on
+  // the context and replayed while shape and arena stay the same.
+  long long per_iteration = 0;
+  auto enqueue_iteration = [&](bool first) -> cudaError_t {
+    const long long l0 = m.launches;
+    vcycle(m, m.r, m.z);
+    k_cg_dot<<<gch, kThreads, 0, m.st>>>(N, r, z, part);
+    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_RHO_NEW, S_N);
+    k_cg_direction<<<gall, kThreads, 0, m.st>>>(N, C, z, pp, sc, first ? 1 : 0);
+    k_cg_scalars_after_dir<<<1, 32, 0, m.st>>>(C, sc);
+    k_cg_apply<<<gch, kThreads, 0, m.st>>>(W, H, act0, pp, d0, q, part);
+    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_PQ, S_N);
+    k_cg_step<<<gch, kThreads, 0, m.st>>>(N, pp, q, x, r, sc, part);
+    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, red, 1);
+    m.launches += 8;
+    per_iteration = m.launches - l0;
+    return cudaGetLastError();
+  };
+  if (ctx->graphs) {
+    std::string key(reinterpret_cast<const char *>(&m.base), sizeof(m.base));
+    const double shape[6] = {(double)W, (double)H, (double)C, p.lambda, (double)m.nb, (double)o};
+    key.append(reinterpret_cast<const char *>(shape), sizeof(shape));
+    if (key != ctx->mgkey || !ctx->mgexec[0] || !ctx->mgexec[1]) {
+      for (auto &ge : ctx->mgexec)
+        if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+      ctx->mgkey.clear();
+      const long long saved = m.launches;
+      for (int g = 0; g < 2 && ce == cudaSuccess; ++g) {
+        cudaGraph_t graph = nullptr;
+        ce = cudaStreamBeginCapture(m.st, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+          const cudaError_t e1 = enqueue_iteration(g == 0);
+          ce = cudaStreamEndCapture(m.st, &graph);
+          if (e1 != cudaSuccess) ce = e1;
+        }
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ctx->mgexec[g], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+      }
+      m.launches = saved;
+      ctx->mgnodes = per_iteration;
+      if (ce != cudaSuccess) {
+        for (auto &ge : ctx->mgexec)
+          if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+        return mfail(ctx, PT_LAUNCH_FAILED, std::string("graph capture: ") + cudaGetErrorString(ce));
+      }
+      ctx->mgkey = key;
+    }
+  }
   int outer = 0;
   while (std::any_of(stop.begin(), stop.end(), [](int s) { return s < 0; })) {
     // scale this outer step's residual to unit norm; channels that stopped get 0
@@ -573,16 +657,14 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
       target[c] = run[c] ? std::max(0.25 * p.tolerance * r0[c] / cur[c], 2e-6) : 1.0;
     }
     for (int it = 0;; ++it) {
-      vcycle(m, m.r, m.z);
-      k_cg_dot<<<gch, kThreads, 0, m.st>>>(N, r, z, part);
-      k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_RHO_NEW, S_N);
-      k_cg_direction<<<gall, kThreads, 0, m.st>>>(N, C, z, pp, sc, it == 0 ? 1 : 0);
-      k_cg_scalars_after_dir<<<1, 32, 0, m.st>>>(C, sc);
-      k_cg_apply<<<gch, kThreads, 0, m.st>>>(W, H, act0, pp, d0, q, part);
-      k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_PQ, S_N);
-      k_cg_step<<<gch, kThreads, 0, m.st>>>(N, pp, q, x, r, sc, part);
-      k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, red, 1);
-      m.launches += 8;
+      const int g = it == 0 ? 0 : 1;
+      if (ctx->mgexec[g]) {
+        ce = cudaGraphLaunch(ctx->mgexec[g], m.st);
+        m.launches += ctx->mgnodes;
+      } else {
+        ce = enqueue_iteration(it == 0);
+      }
+      if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("cg: ") + cudaGetErrorString(ce));
       ce = cudaMemcpyAsync(rr.data(), red, C * 8, cudaMemcpyDeviceToHost, m.st);
       if (ce == cudaSuccess) ce = cudaStreamSynchronize(m.st);
       if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("cg: ") + cudaGetErrorString(ce));
