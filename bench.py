@@ -18,6 +18,8 @@ Arms:
                      same 4096x4096 RGB, 8-polygon inputs, and of multigrid
                      with and without the guess (``learned_leg``).
   --workload masks   the 4096x4096 workload's 8 polygon masks (``mask_arm``).
+  --workload multigrid  the 4096x4096 RGB, 8-polygon solve by multigrid-CG
+                     (``multigrid_arm``).
   mask_raster        (N=1) the workloads' polygon masks rasterised on the device
                      (mask.polygon@1 semantics, ``mask_leg``) beside the
                      oracle's single-core rasteriser.
@@ -342,6 +344,117 @@ def mask_arm(args):
                          "peak_kind": peak_kind, "kernel_us_mean": kernel_s * 1e6,
                          "algorithmic_bytes_per_launch": 4 * W * H},
             "cpu_baseline": cpu, "gpu_launches": P * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def multigrid_arm(args):
+    """Multigrid workload: the 4096x4096 RGB, 8-polygon problem (tolerance 1e-6,
+    lambda 0) solved by multigrid-preconditioned CG (PT_FLAG_MULTIGRID). A step =
+    one solve. `value`: solves/s with inputs in HBM; `e2e`: through the C ABI
+    with pinned host buffers. Every rank solves its own copy (weak scaling)."""
+    import ctypes as Ct
+    import torch
+    from paintop_b200 import _lib, synth
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    L = _lib.lib()
+    ctx = _lib.Context(dev.index)
+    inst = synth.multi_4096(1)
+    W, H, C = inst.width, inst.height, inst.channels
+    hs = torch.from_numpy(inst.source.reshape(-1)).pin_memory()
+    ht = torch.from_numpy(inst.target.reshape(-1)).pin_memory()
+    hm = torch.from_numpy(inst.mask.reshape(-1)).pin_memory()
+    ho = torch.empty_like(hs).pin_memory()
+    g, a, m = hs.to(dev), ht.to(dev), hm.to(dev)
+    out = torch.empty_like(g)
+    reps = (_lib.PtReport * (C + 1))()
+    flags = _lib.PT_FLAG_MULTIGRID
+    p_dev = _lib.PtProblem(W, H, C, g.data_ptr(), a.data_ptr(), m.data_ptr(), 0.0, 100000, 1e-6, 1.8,
+                           flags | _lib.PT_FLAG_DEVICE_POINTERS, None)
+    p_host = _lib.PtProblem(W, H, C, hs.data_ptr(), ht.data_ptr(), hm.data_ptr(), 0.0, 100000, 1e-6, 1.8, flags,
+                            None)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def solve(device):
+        st = L.pt_poisson_solve(ctx.h, Ct.byref(p_dev if device else p_host),
+                                (out if device else ho).data_ptr(), reps, None)
+        if st != _lib.PT_OK:
+            raise _lib.CudaError(st, ctx.last_error())
+        return ctx.last_timing()
+
+    def timed(device):
+        for _ in range(args.warmup):
+            solve(device)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        info = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            info.append(solve(device))
+        e1.record(stream)
+        e1.synchronize()
+        el = e0.elapsed_time(e1) / 1e3
+        if ws > 1:
+            import torch.distributed as dist
+            t = torch.tensor([el], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        return el, info
+
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    elapsed, info = timed(True)
+    clocks = sampler.stop()
+    e2e_elapsed, _ = timed(False)
+    its = [int(reps[c].iterations) for c in range(C)]
+    interior = int((inst.mask[1:-1, 1:-1] > 0.5).sum())
+    # Modelled bytes of one CG iteration per level-0 cell and channel, as the
+    # kernels move them: 8 red-black half-sweeps (rhs 2 B, e 4 + 2 B, mask 1 B
+    # each), residual 13, restriction 4, prolongation 9, zeroing 4, r.z 8,
+    # direction 12, operator 9, update 24 -> 155 B; coarser levels add a third.
+    cells = W * H * C
+    bytes_per_iter = 155.0 * cells * 4.0 / 3.0
+    solve_s = float(np.mean([t[0] for t in info])) / 1e3  # the iterative part (CUDA events)
+    achieved = bytes_per_iter * float(np.mean(its)) / solve_s / 1e9
+    peak, peak_kind = _peaks()
+    if rank == 0:
+        line = {
+            "metric": "multigrid-CG solves/s @ rel-res 1e-6 (4096x4096 RGB, 8 polygons)",
+            "value": ws * args.steps / elapsed, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 residual and refinement)",
+            "data": "synthetic (seeded sinusoid-plus-noise images, 8 random polygons)",
+            "config": {"workload": "multi_4096_multigrid", "width": W, "height": H, "channels": C, "lambda": 0.0,
+                       "tolerance": 1e-6, "interior_px": interior,
+                       "l2": "inputs larger than L2 (201 MB per solve)"},
+            "e2e": {"value": ws * args.steps / e2e_elapsed, "unit": "solves/s",
+                    "h2d_bytes_per_step": 4 * (2 * W * H * C + W * H),
+                    "d2h_bytes_per_step": 4 * W * H * C + 64 * (C + 1)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "multigrid-CG iteration (all kernels)",
+                         "peak_kind": peak_kind, "modelled_bytes_per_iteration": bytes_per_iter,
+                         "iterative_part_ms": solve_s * 1e3},
+            "cpu_baseline": None, "gpu_launches": int(sum(t[2] for t in info)), "clocks": clocks,
+            "solver": {"cg_iterations": its, "refinements": [int(reps[c].refinements) for c in range(C)],
+                       "converged": all(reps[c].converged for c in range(C)),
+                       "worst_final_residual": max(reps[c].final_residual for c in range(C))},
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -810,7 +923,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--device-only", action="store_true",
                     help="time only the device-resident arm (for profiler runs)")
-    ap.add_argument("--workload", default="screened_2048", choices=["screened_2048", "batch_uneven", "masks"])
+    ap.add_argument("--workload", default="screened_2048",
+                    choices=["screened_2048", "batch_uneven", "masks", "multigrid"])
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-warm-start leg (4096x4096 RGB, learned vs plain)")
@@ -823,6 +937,8 @@ def main():
         return batch_arm(args)
     if args.workload == "masks":
         return mask_arm(args)
+    if args.workload == "multigrid":
+        return multigrid_arm(args)
     return gpu_arm(args)
 
 

@@ -90,27 +90,52 @@ __global__ void k_mg_assemble(int W, int H, int C, const float *__restrict__ gui
   }
 }
 
+// Stencil and vector kernels run on 2-D grids: threads (32, 8) over columns
+// and rows, grid.y strides over rows, grid.z is the channel; all index math is
+// 32-bit (a level has at most 2^31 cells). Kernels that reduce write one
+// partial per block, (blockIdx.y * gridDim.x + blockIdx.x), per channel.
+constexpr int kTx = 32, kTy = 8;
+
+__device__ __forceinline__ int block_index() { return blockIdx.y * gridDim.x + blockIdx.x; }
+__device__ __forceinline__ int blocks_per_channel() { return gridDim.x * gridDim.y; }
+
+__device__ __forceinline__ double block_sum2(double v, double *sh) {
+  const int t = threadIdx.y * kTx + threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int o = kTx * kTy / 2; o > 0; o >>= 1) {
+    if (t < o) sh[t] += sh[t + o];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
 // r = fma(lambda + 4, -u, nsum) - b' at interior cells (0 elsewhere) and
-// per-block partial sums of r^2; grid (blocks, C).
-__global__ void k_mg_residual64(int W, int H, const uint8_t *__restrict__ act, const double *__restrict__ u,
-                                const double *__restrict__ bl, double lambda, double *__restrict__ r64,
-                                double *__restrict__ part) {
-  __shared__ double sh[kThreads];
-  const long long N = (long long)W * H;
-  const int c = blockIdx.y;
-  const double *uc = u + (long long)c * N;
+// per-block partial sums of r^2.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(int W, int H, const uint8_t *__restrict__ act,
+                                                             const double *__restrict__ u,
+                                                             const double *__restrict__ bl, double lambda,
+                                                             double *__restrict__ r64, double *__restrict__ part) {
+  __shared__ double sh[kTx * kTy];
+  const int c = blockIdx.z;
+  const size_t N = (size_t)W * H;
+  const double *uc = u + c * N;
+  const int i = blockIdx.x * kTx + threadIdx.x;
   double acc = 0.0;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < N; q += (long long)gridDim.x * blockDim.x) {
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t q = (size_t)j * W + i;
     double r = 0.0;
     if (act[q]) {
       const double nsum = uc[q - 1] + uc[q + 1] + uc[q - W] + uc[q + W];  // L, R, U, D (poisson.rs:275-298)
-      r = fma(lambda + 4.0, -uc[q], nsum) - bl[(long long)c * N + q];
+      r = fma(lambda + 4.0, -uc[q], nsum) - bl[c * N + q];
     }
-    r64[(long long)c * N + q] = r;
+    r64[c * N + q] = r;
     acc += r * r;
   }
-  const double s = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[(long long)c * gridDim.x + blockIdx.x] = s;
+  const double t = block_sum2(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
 }
 
 // out[c * stride] = fixed-order sum of part[c][0 .. n-1]; grid (C)
@@ -123,22 +148,27 @@ __global__ void k_mg_reduce(const double *__restrict__ part, int n, double *__re
 }
 
 // r32 = r64 / scale[c] (0 where the channel is not being corrected)
-__global__ void k_mg_scale(long long N, int C, const double *__restrict__ r64, const double *__restrict__ scale,
-                           float *__restrict__ r32) {
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N * C;
-       p += (long long)gridDim.x * blockDim.x) {
-    const double s = scale[p / N];
-    r32[p] = s > 0.0 ? (float)(r64[p] / s) : 0.0f;
+__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(int W, int H, const double *__restrict__ r64,
+                                                        const double *__restrict__ scale, float *__restrict__ r32) {
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const double s = scale[c];
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t o = c * N + (size_t)j * W + i;
+    r32[o] = s > 0.0 ? (float)(r64[o] / s) : 0.0f;
   }
 }
 
 // u += scale[c] * x at interior cells
-__global__ void k_mg_update(long long N, int C, const uint8_t *__restrict__ act, const float *__restrict__ x,
-                            const double *__restrict__ scale, double *__restrict__ u) {
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N * C;
-       p += (long long)gridDim.x * blockDim.x) {
-    const long long q = p % N;
-    if (act[q]) u[p] = fma(scale[p / N], (double)x[p], u[p]);
+__global__ void __launch_bounds__(kTx * kTy) k_mg_update(int W, int H, const uint8_t *__restrict__ act,
+                                                         const float *__restrict__ x, const double *__restrict__ scale,
+                                                         double *__restrict__ u) {
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const double s = scale[c];
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t q = (size_t)j * W + i;
+    if (act[q]) u[c * N + q] = fma(s, (double)x[c * N + q], u[c * N + q]);
   }
 }
 
@@ -160,19 +190,18 @@ __global__ void k_mg_coarsen(int Wf, int Hf, const uint8_t *__restrict__ af, int
 
 // One colour of red-black Gauss-Seidel on A_k e = rhs: e = (rhs + s * sum of
 // neighbours) / d at active cells of that colour (inactive cells hold 0).
-// Threads index the cells of one colour only; grid (blocks, C).
-__global__ void k_mg_smooth(int W, int H, const uint8_t *__restrict__ act, const float *__restrict__ rhs,
-                            float *__restrict__ e, float s, float d, int color) {
-  const int hw = (W + 1) / 2;
-  const long long N = (long long)W * H, M = (long long)hw * H;
-  const int c = blockIdx.y;
-  float *ec = e + (long long)c * N;
-  const float *rc = rhs + (long long)c * N;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < M; t += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(t / hw);
-    const int i = 2 * (int)(t - (long long)j * hw) + ((j + color) & 1);
+// x threads index the cells of one colour in a row.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(int W, int H, const uint8_t *__restrict__ act,
+                                                         const float *__restrict__ rhs, float *__restrict__ e, float s,
+                                                         float d, int color) {
+  const int c = blockIdx.z, m = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  float *ec = e + c * N;
+  const float *rc = rhs + c * N;
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H; j += gridDim.y * kTy) {
+    const int i = 2 * m + ((j + color) & 1);
     if (i >= W) continue;
-    const long long q = (long long)j * W + i;
+    const size_t q = (size_t)j * W + i;
     if (!act[q]) continue;
     float nb = 0.0f;
     if (i > 0) nb += ec[q - 1];
@@ -221,39 +250,41 @@ __global__ void k_mg_coarse(int W, int H, const uint8_t *__restrict__ act, const
   if (t < n) e[(long long)c * n + t] = se[t];
 }
 
-// res = rhs - A_k e at active cells, 0 elsewhere; grid (blocks, C)
-__global__ void k_mg_resid(int W, int H, const uint8_t *__restrict__ act, const float *__restrict__ rhs,
-                           const float *__restrict__ e, float s, float d, float *__restrict__ res) {
-  const long long N = (long long)W * H;
-  const int c = blockIdx.y;
-  const float *ec = e + (long long)c * N;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < N; q += (long long)gridDim.x * blockDim.x) {
+// res = rhs - A_k e at active cells, 0 elsewhere
+__global__ void __launch_bounds__(kTx * kTy) k_mg_resid(int W, int H, const uint8_t *__restrict__ act,
+                                                        const float *__restrict__ rhs, const float *__restrict__ e,
+                                                        float s, float d, float *__restrict__ res) {
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const float *ec = e + c * N;
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t q = (size_t)j * W + i;
     float r = 0.0f;
     if (act[q]) {
-      const int j = (int)(q / W), i = (int)(q - (long long)j * W);
       float nb = 0.0f;
       if (i > 0) nb += ec[q - 1];
       if (i < W - 1) nb += ec[q + 1];
       if (j > 0) nb += ec[q - W];
       if (j < H - 1) nb += ec[q + W];
-      r = rhs[(long long)c * N + q] - (d * ec[q] - s * nb);
+      r = rhs[c * N + q] - (d * ec[q] - s * nb);
     }
-    res[(long long)c * N + q] = r;
+    res[c * N + q] = r;
   }
 }
 
 __device__ __forceinline__ float pw(int a) { return (a == 0 || a == 1) ? 0.75f : 0.25f; }  // a = fine - 2 * coarse
 
 // rhs_c(I, J) = sum over fine (2I + a, 2J + b), a, b in -1..2, of wx wy res_f / 4
-__global__ void k_mg_restrict(int Wf, int Hf, const float *__restrict__ res, int Wc, int Hc,
-                              const uint8_t *__restrict__ ac, float *__restrict__ rhs) {
-  const long long Nc = (long long)Wc * Hc, Nf = (long long)Wf * Hf;
-  const int c = blockIdx.y;
-  const float *rf = res + (long long)c * Nf;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Nc; q += (long long)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(kTx * kTy) k_mg_restrict(int Wf, int Hf, const float *__restrict__ res, int Wc,
+                                                           int Hc, const uint8_t *__restrict__ ac,
+                                                           float *__restrict__ rhs) {
+  const int c = blockIdx.z, I = blockIdx.x * kTx + threadIdx.x;
+  const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
+  const float *rf = res + c * Nf;
+  for (int J = blockIdx.y * kTy + threadIdx.y; J < Hc && I < Wc; J += gridDim.y * kTy) {
+    const size_t q = (size_t)J * Wc + I;
     float v = 0.0f;
     if (ac[q]) {
-      const int J = (int)(q / Wc), I = (int)(q - (long long)J * Wc);
       for (int b = -1; b <= 2; ++b) {
         const int j = 2 * J + b;
         if (j < 0 || j >= Hf) continue;
@@ -261,85 +292,90 @@ __global__ void k_mg_restrict(int Wf, int Hf, const float *__restrict__ res, int
         for (int a = -1; a <= 2; ++a) {
           const int i = 2 * I + a;
           if (i < 0 || i >= Wf) continue;
-          row += pw(a) * rf[(long long)j * Wf + i];
+          row += pw(a) * rf[(size_t)j * Wf + i];
         }
         v += pw(b) * row;
       }
       v *= 0.25f;
     }
-    rhs[(long long)c * Nc + q] = v;
+    rhs[c * Nc + q] = v;
   }
 }
 
 // e_f += bilinear prolongation of e_c at active fine cells
-__global__ void k_mg_prolong(int Wf, int Hf, const uint8_t *__restrict__ af, float *__restrict__ ef, int Wc, int Hc,
-                             const float *__restrict__ ec) {
-  const long long Nc = (long long)Wc * Hc, Nf = (long long)Wf * Hf;
-  const int c = blockIdx.y;
-  const float *e = ec + (long long)c * Nc;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < Nf; q += (long long)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(int Wf, int Hf, const uint8_t *__restrict__ af,
+                                                          float *__restrict__ ef, int Wc, int Hc,
+                                                          const float *__restrict__ ec) {
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
+  const float *e = ec + c * Nc;
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < Hf && i < Wf; j += gridDim.y * kTy) {
+    const size_t q = (size_t)j * Wf + i;
     if (!af[q]) continue;
-    const int j = (int)(q / Wf), i = (int)(q - (long long)j * Wf);
     const int I0 = i >> 1, J0 = j >> 1;
     const int I1 = (i & 1) ? I0 + 1 : I0 - 1, J1 = (j & 1) ? J0 + 1 : J0 - 1;
     auto at = [&](int I, int J) -> float {
-      return (I >= 0 && I < Wc && J >= 0 && J < Hc) ? e[(long long)J * Wc + I] : 0.0f;
+      return (I >= 0 && I < Wc && J >= 0 && J < Hc) ? e[(size_t)J * Wc + I] : 0.0f;
     };
     const float v = 0.5625f * at(I0, J0) + 0.1875f * (at(I1, J0) + at(I0, J1)) + 0.0625f * at(I1, J1);
-    ef[(long long)c * Nf + q] += v;
+    ef[c * Nf + q] += v;
   }
 }
 
 // ---- conjugate gradients -------------------------------------------------------
-// q = A_0 p at active cells; partial sums of p.q; grid (blocks, C)
-__global__ void k_cg_apply(int W, int H, const uint8_t *__restrict__ act, const float *__restrict__ p, float d,
-                           float *__restrict__ q, double *__restrict__ part) {
-  __shared__ double sh[kThreads];
-  const long long N = (long long)W * H;
-  const int c = blockIdx.y;
-  const float *pc = p + (long long)c * N;
+// q = A_0 p at active cells; partial sums of p.q
+__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(int W, int H, const uint8_t *__restrict__ act,
+                                                        const float *__restrict__ p, float d, float *__restrict__ q,
+                                                        double *__restrict__ part) {
+  __shared__ double sh[kTx * kTy];
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const float *pc = p + c * N;
   double acc = 0.0;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N; k += (long long)gridDim.x * blockDim.x) {
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t k = (size_t)j * W + i;
     float v = 0.0f;
     if (act[k]) {
       // interior cells are never on the border: all four neighbours exist
       v = d * pc[k] - (pc[k - 1] + pc[k + 1] + pc[k - W] + pc[k + W]);
       acc += (double)pc[k] * (double)v;
     }
-    q[(long long)c * N + k] = v;
+    q[c * N + k] = v;
   }
-  const double s = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[(long long)c * gridDim.x + blockIdx.x] = s;
+  const double t = block_sum2(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
 }
 
-// partial sums of a.b; grid (blocks, C)
-__global__ void k_cg_dot(long long N, const float *__restrict__ a, const float *__restrict__ b,
-                         double *__restrict__ part) {
-  __shared__ double sh[kThreads];
-  const int c = blockIdx.y;
+// partial sums of a.b
+__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(int W, int H, const float *__restrict__ a,
+                                                      const float *__restrict__ b, double *__restrict__ part) {
+  __shared__ double sh[kTx * kTy];
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
   double acc = 0.0;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N; k += (long long)gridDim.x * blockDim.x)
-    acc += (double)a[(long long)c * N + k] * (double)b[(long long)c * N + k];
-  const double s = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[(long long)c * gridDim.x + blockIdx.x] = s;
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t o = c * N + (size_t)j * W + i;
+    acc += (double)a[o] * (double)b[o];
+  }
+  const double t = block_sum2(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
 }
 
 // Per-channel scalars: sc[c] = {rho, rho_new, pq, rr, alpha, beta, run}
 enum { S_RHO, S_RHO_NEW, S_PQ, S_RR, S_ALPHA, S_BETA, S_RUN, S_N };
 
-// p = z + beta p (beta = rho_new / rho, or 0 on the first iteration), rho = rho_new
-__global__ void k_cg_direction(long long N, int C, const float *__restrict__ z, float *__restrict__ p,
-                               const double *__restrict__ sc, int first) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N * C;
-       k += (long long)gridDim.x * blockDim.x) {
-    const double *s = sc + (k / N) * S_N;
-    if (s[S_RUN] == 0.0) continue;
-    if (first) {  // p is not read: it holds whatever the arena held
-      p[k] = z[k];
-      continue;
-    }
-    const float beta = (float)(s[S_RHO] != 0.0 ? s[S_RHO_NEW] / s[S_RHO] : 0.0);
-    p[k] = z[k] + beta * p[k];
+// p = z + beta p (beta = rho_new / rho; p = z on the first iteration)
+__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(int W, int H, const float *__restrict__ z,
+                                                            float *__restrict__ p, const double *__restrict__ sc,
+                                                            int first) {
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const double *s = sc + c * S_N;
+  if (s[S_RUN] == 0.0) return;
+  const float beta = first ? 0.0f : (float)(s[S_RHO] != 0.0 ? s[S_RHO_NEW] / s[S_RHO] : 0.0);
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t o = c * N + (size_t)j * W + i;
+    p[o] = first ? z[o] : z[o] + beta * p[o];  // first: p is not read (it holds what the arena held)
   }
 }
 
@@ -348,27 +384,29 @@ __global__ void k_cg_scalars_after_dir(int C, double *__restrict__ sc) {
 }
 
 // x += alpha p, r -= alpha q (alpha = rho / p.q); partial sums of r.r
-__global__ void k_cg_step(long long N, const float *__restrict__ p, const float *__restrict__ q,
-                          float *__restrict__ x, float *__restrict__ r, const double *__restrict__ sc,
-                          double *__restrict__ part) {
-  __shared__ double sh[kThreads];
-  const int c = blockIdx.y;
+__global__ void __launch_bounds__(kTx * kTy) k_cg_step(int W, int H, const float *__restrict__ p,
+                                                       const float *__restrict__ q, float *__restrict__ x,
+                                                       float *__restrict__ r, const double *__restrict__ sc,
+                                                       double *__restrict__ part) {
+  __shared__ double sh[kTx * kTy];
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
   const double *s = sc + c * S_N;
   if (s[S_RUN] == 0.0) {  // a stopped channel: x and r stay (p may never have been written)
-    if (threadIdx.x == 0) part[(long long)c * gridDim.x + blockIdx.x] = 0.0;
+    if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = 0.0;
     return;
   }
   const float alpha = s[S_PQ] > 0.0 ? (float)(s[S_RHO] / s[S_PQ]) : 0.0f;
   double acc = 0.0;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N; k += (long long)gridDim.x * blockDim.x) {
-    const long long o = (long long)c * N + k;
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t o = c * N + (size_t)j * W + i;
     x[o] += alpha * p[o];
     const float rv = r[o] - alpha * q[o];
     r[o] = rv;
     acc += (double)rv * (double)rv;
   }
-  const double t = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[(long long)c * gridDim.x + blockIdx.x] = t;
+  const double t = block_sum2(acc, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
 }
 
 // out = interleave(u) at interior cells, the anchor elsewhere (bit for bit)
@@ -406,6 +444,17 @@ struct Mg {
   template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
 };
 
+// (32, 8) threads over w columns and h rows, channels in z; at most about 8
+// blocks per SM per channel (rows are strided), at most 65535 in y.
+dim3 grid2(int w, int h, int C, int sms) {
+  const int gx = std::max(1, (w + kTx - 1) / kTx);
+  int gy = std::max(1, (h + kTy - 1) / kTy);
+  gy = std::min(gy, std::max(1, sms * 8 / gx));
+  gy = std::min(gy, 65535);
+  return dim3(gx, gy, C);
+}
+const dim3 kBlock2(kTx, kTy);
+
 unsigned blocks(long long n, int sms) {
   return (unsigned)std::max<long long>(1, std::min<long long>((n + kThreads - 1) / kThreads, (long long)sms * 8));
 }
@@ -417,7 +466,7 @@ void vcycle(Mg &m, size_t rhs0, size_t e0) {
     Level &v = m.lv[k];
     const size_t rhs = k == 0 ? rhs0 : v.rhs, e = k == 0 ? e0 : v.e;
     const long long N = (long long)v.W * v.H;
-    const dim3 gh(blocks((long long)((v.W + 1) / 2) * v.H, sms), m.C), g(blocks(N, sms), m.C);
+    const dim3 gh = grid2((v.W + 1) / 2, v.H, m.C, sms), g = grid2(v.W, v.H, m.C, sms);
     if (k == L - 1) {  // the coarsest level: symmetric sweeps in one block per channel
       k_mg_coarse<<<m.C, kCoarseMax, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e),
                                                  v.s, v.d, 24);
@@ -427,31 +476,30 @@ void vcycle(Mg &m, size_t rhs0, size_t e0) {
     cudaMemsetAsync(m.at<float>(e), 0, (size_t)N * m.C * sizeof(float), m.st);
     const int sweeps = 2;
     for (int t = 0; t < sweeps; ++t) {
-      k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
+      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
                                              v.d, 0);
-      k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
+      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
                                              v.d, 1);
     }
     m.launches += 1 + 2 * sweeps;
     Level &cl = m.lv[k + 1];
-    k_mg_resid<<<g, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
+    k_mg_resid<<<g, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
                                          m.at<float>(v.res));
-    const dim3 gc(blocks((long long)cl.W * cl.H, sms), m.C);
-    k_mg_restrict<<<gc, kThreads, 0, m.st>>>(v.W, v.H, m.at<float>(v.res), cl.W, cl.H, m.at<uint8_t>(cl.act),
+    const dim3 gc = grid2(cl.W, cl.H, m.C, sms);
+    k_mg_restrict<<<gc, kBlock2, 0, m.st>>>(v.W, v.H, m.at<float>(v.res), cl.W, cl.H, m.at<uint8_t>(cl.act),
                                              m.at<float>(cl.rhs));
     m.launches += 2;
   }
   for (int k = L - 2; k >= 0; --k) {
     Level &v = m.lv[k], &cl = m.lv[k + 1];
     const size_t rhs = k == 0 ? rhs0 : v.rhs, e = k == 0 ? e0 : v.e;
-    const long long N = (long long)v.W * v.H;
-    const dim3 gh(blocks((long long)((v.W + 1) / 2) * v.H, sms), m.C), g(blocks(N, sms), m.C);
-    k_mg_prolong<<<g, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(e), cl.W, cl.H,
+    const dim3 gh = grid2((v.W + 1) / 2, v.H, m.C, sms), g = grid2(v.W, v.H, m.C, sms);
+    k_mg_prolong<<<g, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(e), cl.W, cl.H,
                                            m.at<float>(cl.e));
     for (int t = 0; t < 2; ++t) {
-      k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
+      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
                                              v.d, 1);
-      k_mg_smooth<<<gh, kThreads, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
+      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
                                              v.d, 0);
     }
     m.launches += 5;
@@ -484,7 +532,8 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
   Mg m;
   m.ctx = ctx; m.st = ctx->stream; m.W = W; m.H = H; m.C = C; m.N = (long long)W * H;
   const long long N = m.N, NC = N * C;
-  m.nb = (int)blocks(N, ctx->sms);
+  const dim3 g0 = grid2(W, H, C, ctx->sms);  // level-0 grid of every reducing kernel
+  m.nb = (int)(g0.x * g0.y);
   // levels: halve (ceil) while the level has more than 64 cells
   {
     int w = W, h = H, k = 0;
@@ -529,7 +578,6 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
   }
   const int sms = ctx->sms;
   const unsigned gall = blocks(NC, sms);
-  const dim3 gch(m.nb, C);
   uint8_t *act0 = m.at<uint8_t>(m.lv[0].act);
   double *u = m.at<double>(m.u), *bl = m.at<double>(m.bl), *r64 = m.at<double>(m.r64), *part = m.at<double>(m.part),
          *red = m.at<double>(m.red), *sc = m.at<double>(m.sc), *scale = m.at<double>(m.scale);
@@ -549,7 +597,7 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
   // FP64 residual norms per channel of the current u -> host
   std::vector<double> nrm(C);
   auto residual = [&](const double *uu) -> cudaError_t {
-    k_mg_residual64<<<gch, kThreads, 0, m.st>>>(W, H, act0, uu, bl, p.lambda, r64, part);
+    k_mg_residual64<<<g0, kBlock2, 0, m.st>>>(W, H, act0, uu, bl, p.lambda, r64, part);
     k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, red, 1);
     m.launches += 2;
     cudaError_t e = cudaMemcpyAsync(nrm.data(), red, C * 8, cudaMemcpyDeviceToHost, m.st);
@@ -595,13 +643,13 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
   auto enqueue_iteration = [&](bool first) -> cudaError_t {
     const long long l0 = m.launches;
     vcycle(m, m.r, m.z);
-    k_cg_dot<<<gch, kThreads, 0, m.st>>>(N, r, z, part);
+    k_cg_dot<<<g0, kBlock2, 0, m.st>>>(W, H, r, z, part);
     k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_RHO_NEW, S_N);
-    k_cg_direction<<<gall, kThreads, 0, m.st>>>(N, C, z, pp, sc, first ? 1 : 0);
+    k_cg_direction<<<g0, kBlock2, 0, m.st>>>(W, H, z, pp, sc, first ? 1 : 0);
     k_cg_scalars_after_dir<<<1, 32, 0, m.st>>>(C, sc);
-    k_cg_apply<<<gch, kThreads, 0, m.st>>>(W, H, act0, pp, d0, q, part);
+    k_cg_apply<<<g0, kBlock2, 0, m.st>>>(W, H, act0, pp, d0, q, part);
     k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_PQ, S_N);
-    k_cg_step<<<gch, kThreads, 0, m.st>>>(N, pp, q, x, r, sc, part);
+    k_cg_step<<<g0, kBlock2, 0, m.st>>>(W, H, pp, q, x, r, sc, part);
     k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, red, 1);
     m.launches += 8;
     per_iteration = m.launches - l0;
@@ -646,7 +694,7 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
     }
     cudaMemcpyAsync(scale, hscale.data(), C * 8, cudaMemcpyHostToDevice, m.st);
     cudaMemcpyAsync(sc, hsc.data(), C * S_N * 8, cudaMemcpyHostToDevice, m.st);
-    k_mg_scale<<<gall, kThreads, 0, m.st>>>(N, C, r64, scale, r);
+    k_mg_scale<<<g0, kBlock2, 0, m.st>>>(W, H, r64, scale, r);
     cudaMemsetAsync(x, 0, NC * 4, m.st);
     m.launches += 1;
     // inner target: well below the bar, or as far as FP32 gets from unit norm
@@ -684,7 +732,7 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
       if (!any) break;
     }
     // u += scale * x, then the FP64 residual decides
-    k_mg_update<<<gall, kThreads, 0, m.st>>>(N, C, act0, x, scale, u);
+    k_mg_update<<<g0, kBlock2, 0, m.st>>>(W, H, act0, x, scale, u);
     ++m.launches;
     const std::vector<double> prev = cur;
     ce = residual(u);
