@@ -212,6 +212,21 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(int W, int H, const uin
   }
 }
 
+// The first half-sweep of a V-cycle level, from e = 0: e = rhs / d at active
+// cells of colour 0 (red), 0 everywhere else -- what zeroing e and one red
+// half-sweep produce, bit for bit (the neighbour sum is 0 and rhs + s * 0 is
+// rhs), in one pass that writes every cell.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth_first(int W, int H, const uint8_t *__restrict__ act,
+                                                               const float *__restrict__ rhs, float *__restrict__ e,
+                                                               float s, float d) {
+  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+    const size_t q = (size_t)j * W + i;
+    e[c * N + q] = (act[q] && ((i + j) & 1) == 0) ? (rhs[c * N + q] + s * 0.0f) / d : 0.0f;
+  }
+}
+
 // The coarsest level (at most kCoarseMax cells): `sweeps` red-black sweeps,
 // then as many in reverse colour order, from e = 0, in shared memory; one
 // block per channel.
@@ -250,37 +265,20 @@ __global__ void k_mg_coarse(int W, int H, const uint8_t *__restrict__ act, const
   if (t < n) e[(long long)c * n + t] = se[t];
 }
 
-// res = rhs - A_k e at active cells, 0 elsewhere
-__global__ void __launch_bounds__(kTx * kTy) k_mg_resid(int W, int H, const uint8_t *__restrict__ act,
-                                                        const float *__restrict__ rhs, const float *__restrict__ e,
-                                                        float s, float d, float *__restrict__ res) {
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
-  const size_t N = (size_t)W * H;
-  const float *ec = e + c * N;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
-    const size_t q = (size_t)j * W + i;
-    float r = 0.0f;
-    if (act[q]) {
-      float nb = 0.0f;
-      if (i > 0) nb += ec[q - 1];
-      if (i < W - 1) nb += ec[q + 1];
-      if (j > 0) nb += ec[q - W];
-      if (j < H - 1) nb += ec[q + W];
-      r = rhs[c * N + q] - (d * ec[q] - s * nb);
-    }
-    res[c * N + q] = r;
-  }
-}
-
 __device__ __forceinline__ float pw(int a) { return (a == 0 || a == 1) ? 0.75f : 0.25f; }  // a = fine - 2 * coarse
 
-// rhs_c(I, J) = sum over fine (2I + a, 2J + b), a, b in -1..2, of wx wy res_f / 4
-__global__ void __launch_bounds__(kTx * kTy) k_mg_restrict(int Wf, int Hf, const float *__restrict__ res, int Wc,
-                                                           int Hc, const uint8_t *__restrict__ ac,
-                                                           float *__restrict__ rhs) {
+// The restriction of the level's residual, rhs_c(I, J) = sum over fine
+// (2I + a, 2J + b), a, b in -1..2, of wx wy res_f / 4 with res_f = rhs - A e at
+// active fine cells (0 elsewhere), evaluated on the fly so the residual is
+// never stored.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(int Wf, int Hf, const uint8_t *__restrict__ af,
+                                                                 const float *__restrict__ rhsf,
+                                                                 const float *__restrict__ ef, float s, float d, int Wc,
+                                                                 int Hc, const uint8_t *__restrict__ ac,
+                                                                 float *__restrict__ rhsc) {
   const int c = blockIdx.z, I = blockIdx.x * kTx + threadIdx.x;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
-  const float *rf = res + c * Nf;
+  const float *e = ef + c * Nf, *rh = rhsf + c * Nf;
   for (int J = blockIdx.y * kTy + threadIdx.y; J < Hc && I < Wc; J += gridDim.y * kTy) {
     const size_t q = (size_t)J * Wc + I;
     float v = 0.0f;
@@ -292,13 +290,23 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_restrict(int Wf, int Hf, const
         for (int a = -1; a <= 2; ++a) {
           const int i = 2 * I + a;
           if (i < 0 || i >= Wf) continue;
-          row += pw(a) * rf[(size_t)j * Wf + i];
+          const size_t f = (size_t)j * Wf + i;
+          float r = 0.0f;
+          if (af[f]) {
+            float nb = 0.0f;
+            if (i > 0) nb += e[f - 1];
+            if (i < Wf - 1) nb += e[f + 1];
+            if (j > 0) nb += e[f - Wf];
+            if (j < Hf - 1) nb += e[f + Wf];
+            r = rh[f] - (d * e[f] - s * nb);
+          }
+          row += pw(a) * r;
         }
         v += pw(b) * row;
       }
       v *= 0.25f;
     }
-    rhs[c * Nc + q] = v;
+    rhsc[c * Nc + q] = v;
   }
 }
 
@@ -424,7 +432,7 @@ __global__ void k_mg_emit(int W, int H, int C, const uint8_t *__restrict__ act, 
 // ---- host ----------------------------------------------------------------------
 struct Level {
   int W, H;
-  size_t act, e, rhs, res;  // arena offsets
+  size_t act, e, rhs;  // arena offsets
   float s, d;
 };
 
@@ -465,7 +473,6 @@ void vcycle(Mg &m, size_t rhs0, size_t e0) {
   for (int k = 0; k < L; ++k) {
     Level &v = m.lv[k];
     const size_t rhs = k == 0 ? rhs0 : v.rhs, e = k == 0 ? e0 : v.e;
-    const long long N = (long long)v.W * v.H;
     const dim3 gh = grid2((v.W + 1) / 2, v.H, m.C, sms), g = grid2(v.W, v.H, m.C, sms);
     if (k == L - 1) {  // the coarsest level: symmetric sweeps in one block per channel
       k_mg_coarse<<<m.C, kCoarseMax, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e),
@@ -473,22 +480,21 @@ void vcycle(Mg &m, size_t rhs0, size_t e0) {
       ++m.launches;
       break;
     }
-    cudaMemsetAsync(m.at<float>(e), 0, (size_t)N * m.C * sizeof(float), m.st);
-    const int sweeps = 2;
-    for (int t = 0; t < sweeps; ++t) {
-      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                             v.d, 0);
-      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                             v.d, 1);
-    }
-    m.launches += 1 + 2 * sweeps;
+    // red, black, red, black from e = 0 (the first red half-sweep writes all of e)
+    k_mg_smooth_first<<<g, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
+                                               v.d);
+    k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
+                                          1);
+    k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
+                                          0);
+    k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
+                                          1);
+    m.launches += 4;
     Level &cl = m.lv[k + 1];
-    k_mg_resid<<<g, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
-                                         m.at<float>(v.res));
     const dim3 gc = grid2(cl.W, cl.H, m.C, sms);
-    k_mg_restrict<<<gc, kBlock2, 0, m.st>>>(v.W, v.H, m.at<float>(v.res), cl.W, cl.H, m.at<uint8_t>(cl.act),
-                                             m.at<float>(cl.rhs));
-    m.launches += 2;
+    k_mg_resid_restrict<<<gc, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e),
+                                                  v.s, v.d, cl.W, cl.H, m.at<uint8_t>(cl.act), m.at<float>(cl.rhs));
+    ++m.launches;
   }
   for (int k = L - 2; k >= 0; --k) {
     Level &v = m.lv[k], &cl = m.lv[k + 1];
@@ -539,7 +545,7 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
     int w = W, h = H, k = 0;
     for (;;) {
       const float s = 1.0f / (float)(1u << (2 * std::min(k, 15)));
-      m.lv.push_back(Level{w, h, 0, 0, 0, 0, s, 4.0f * s + (float)p.lambda});
+      m.lv.push_back(Level{w, h, 0, 0, 0, s, 4.0f * s + (float)p.lambda});
       if ((long long)w * h <= kCoarseMax || k >= 30) break;
       w = (w + 1) / 2; h = (h + 1) / 2; ++k;
     }
@@ -550,7 +556,6 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
     Level &v = m.lv[k];
     const size_t n = (size_t)v.W * v.H;
     v.act = take(n);
-    v.res = take(n * C * sizeof(float));
     if (k > 0) { v.e = take(n * C * sizeof(float)); v.rhs = take(n * C * sizeof(float)); }
   }
   m.u = take(NC * 8); m.bl = take(NC * 8); m.uw = warm ? take(NC * 8) : 0; m.r64 = take(NC * 8);
