@@ -106,12 +106,18 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        # wait for the first sample, then count only samples taken from here on
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.mark = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -126,9 +132,10 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.thread.join(timeout=2)
+        lines = self.lines[getattr(self, "mark", 0):] or self.lines[-1:]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -1030,7 +1037,7 @@ def multigrid_leg(ctx, dev, inst, steps: int = 3, warmup: int = 1):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
