@@ -47,6 +47,7 @@
 namespace {
 
 constexpr int kThreads = 256;
+constexpr double kInnerFloor = 2e-6;  // deepest relative reduction asked of one FP32 CG run
 
 __device__ __forceinline__ double block_sum(double v, double *sh) {
   sh[threadIdx.x] = v;
@@ -702,12 +703,15 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
     k_mg_scale<<<g0, kBlock2, 0, m.st>>>(W, H, r64, scale, r);
     cudaMemsetAsync(x, 0, NC * 4, m.st);
     m.launches += 1;
-    // inner target: well below the bar, or as far as FP32 gets from unit norm
+    // inner target: a quarter of the remaining bar, at most as deep as FP32
+    // goes from a unit residual; a run whose residual stops falling (less than
+    // 30% over 4 iterations: the FP32 floor) hands over to the next outer step
     std::vector<double> target(C), rel(C, 1.0);
+    std::vector<std::vector<double>> seen(C);
     std::vector<int> run(C);
     for (int c = 0; c < C; ++c) {
       run[c] = stop[c] < 0;
-      target[c] = run[c] ? std::max(0.25 * p.tolerance * r0[c] / cur[c], 2e-6) : 1.0;
+      target[c] = run[c] ? std::max(0.25 * p.tolerance * r0[c] / cur[c], kInnerFloor) : 1.0;
     }
     for (int it = 0;; ++it) {
       const int g = it == 0 ? 0 : 1;
@@ -727,7 +731,10 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
         its[c] += 1;
         rel[c] = std::sqrt(rr[c]);  // relative to this outer step's unit residual
         hist[c].push_back(rel[c] * cur[c] / r0[c]);
-        if (rel[c] <= target[c] || its[c] >= (int)p.max_iterations || !std::isfinite(rel[c])) {
+        seen[c].push_back(rel[c]);
+        const size_t n = seen[c].size();
+        const bool stuck = n > 4 && seen[c][n - 1] > 0.7 * seen[c][n - 5];
+        if (rel[c] <= target[c] || stuck || its[c] >= (int)p.max_iterations || !std::isfinite(rel[c])) {
           run[c] = 0;
           hsc[c * S_N + S_RUN] = 0.0;
           cudaMemcpyAsync(sc + c * S_N + S_RUN, &hsc[c * S_N + S_RUN], 8, cudaMemcpyHostToDevice, m.st);
