@@ -20,6 +20,8 @@ Arms:
   --workload masks   the 4096x4096 workload's 8 polygon masks (``mask_arm``).
   --workload multigrid  the 4096x4096 RGB, 8-polygon solve by multigrid-CG
                      (``multigrid_arm``).
+  --workload train    the learned warm start's U-Net training step, batch 64 of
+                     256x256 (``train_arm``).
   --workload clone_512  the reference's CPU-runnable 512x512 RGB clone, seeds
                      1-5, beside the restated op on one core (``clone_arm``).
   mask_raster        (N=1) the workloads' polygon masks rasterised on the device
@@ -569,6 +571,95 @@ def clone_arm(args):
     return 0
 
 
+def train_arm(args):
+    """U-Net training step of the learned warm start: batch 64 of 256x256
+    single-channel instances (seeded, device-generated; the target is the
+    anchor's correction), forward + backward + Adam through pt_unet_train_step.
+    A step = one training step. `value`: samples/s; the roofline is the bf16
+    tensor peak against the convolutions' algorithmic FLOPs. Every rank trains
+    its own replica on its own batch (weak scaling; the data-parallel
+    exchange is timed by the trainer, not here)."""
+    import ctypes as Ct
+    import torch
+    from paintop_b200 import _lib, warmstart as wsm
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    ctx = _lib.Context(dev.index)
+    B, S = 64, 256
+    net = wsm.UNet(ctx, seed=rank)
+    g, a, m = wsm.make_instances(B, S, seed=3 + rank)
+    f = net.features(g, a, m)
+    lm = wsm.interior_mask(m)
+    t = (a - g).contiguous()
+    L = _lib.lib()
+    loss = Ct.c_double()
+
+    def step():
+        st = L.pt_unet_train_step(net.h, f.data_ptr(), t.data_ptr(), lm.data_ptr(), B, S, S, Ct.c_float(1e-3),
+                                  Ct.byref(loss))
+        if st != _lib.PT_OK:
+            raise _lib.CudaError(st, ctx.last_error())
+
+    for _ in range(args.warmup):
+        step()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    el = e0.elapsed_time(e1) / 1e3
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([el], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        el = float(tt.item())
+    flops = wsm.train_flops_per_pixel() * B * S * S
+    step_s = el / args.steps
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+        pk = json.load(fh)
+    peak = float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops")))
+    achieved = flops / step_s / 1e12
+    if rank == 0:
+        line = {
+            "metric": "U-Net training samples/s (batch 64, 256x256, bf16 weights, fp32 accumulate, Adam)",
+            "value": ws * B * args.steps / el, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded sinusoid-plus-noise instances)",
+            "config": {"workload": "unet_train_b64_256", "batch": B, "size": S,
+                       "model": "U-Net 16-32-64-128, 3x3 convs, 14 layers", "flops_per_step": flops,
+                       "l2": "one 16-channel level-0 activation is 134 MB, larger than L2"},
+            "e2e": None,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "whole training step",
+                         "peak_kind": "measured (sustained: a step loop lasts seconds)"},
+            "cpu_baseline": None, "gpu_launches": None, "clocks": clocks, "loss_last": loss.value,
+        }
+        print(json.dumps(line), flush=True)
+    net.close()
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def mask_cpu_baseline():
     """The oracle's mask.polygon (the reference's rasterize(), one host core) on
     the 2048x2048 star."""
@@ -1044,7 +1135,7 @@ def main():
     ap.add_argument("--device-only", action="store_true",
                     help="time only the device-resident arm (for profiler runs)")
     ap.add_argument("--workload", default="screened_2048",
-                    choices=["screened_2048", "batch_uneven", "masks", "multigrid", "clone_512"])
+                    choices=["screened_2048", "batch_uneven", "masks", "multigrid", "clone_512", "train"])
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-warm-start leg (4096x4096 RGB, learned vs plain)")
@@ -1061,6 +1152,8 @@ def main():
         return multigrid_arm(args)
     if args.workload == "clone_512":
         return clone_arm(args)
+    if args.workload == "train":
+        return train_arm(args)
     return gpu_arm(args)
 
 
