@@ -31,7 +31,8 @@
 // refinements = outer steps after the first; omega_used = 1 (Gauss-Seidel
 // smoothing). Stop reasons: converged at the FP64 bar; max-iterations when the
 // CG iterations reach max_iterations; stalled when an outer step fails to
-// lower the FP64 residual.
+// lower the FP64 residual, or at once (0 iterations, interior set to NaN)
+// when a NaN or infinity in the inputs makes the residual non-finite.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -633,12 +634,27 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
   std::vector<int> its(C, 0), stop(C, -1), refines(C, 0);
   std::vector<double> cur = nrm;  // FP64 ||r|| of the current u
   std::vector<std::vector<double>> hist(C);
+  std::vector<double> hsc(C * S_N, 0.0), hscale(C, 0.0), rr(C);
+  bool poisoned = false;
   for (int c = 0; c < C; ++c) {
     if (r0[c] == 0.0) stop[c] = PT_STOP_CONVERGED;  // poisson.rs:178-185
-    else if (cur[c] <= p.tolerance * r0[c]) stop[c] = PT_STOP_CONVERGED;
+    else if (!std::isfinite(cur[c])) {  // (before the bar: inf <= tol * inf would pass it)
+      // a NaN or infinity reached the system: its residual can never improve,
+      // which the reference ends by its stall rule with the region's cells
+      // non-finite; here at once, with the interior set to NaN
+      stop[c] = PT_STOP_STALLED;
+      hscale[c] = std::nan("");
+      poisoned = true;
+    } else if (cur[c] <= p.tolerance * r0[c]) stop[c] = PT_STOP_CONVERGED;
     else if (p.max_iterations == 0) stop[c] = PT_STOP_MAX_ITERATIONS;
   }
-  std::vector<double> hsc(C * S_N, 0.0), hscale(C, 0.0), rr(C);
+  if (poisoned) {  // u = fma(NaN, 0, u) = NaN at interior cells of those channels
+    cudaMemcpyAsync(scale, hscale.data(), C * 8, cudaMemcpyHostToDevice, m.st);
+    cudaMemsetAsync(x, 0, NC * 4, m.st);
+    k_mg_update<<<g0, kBlock2, 0, m.st>>>(W, H, act0, x, scale, u);
+    ++m.launches;
+    std::fill(hscale.begin(), hscale.end(), 0.0);
+  }
   const float d0 = m.lv[0].d;
   // One CG iteration: V-cycle z = M r, rho = r.z, p = z + beta p, q = A p,
   // alpha = rho / p.q, x += alpha p, r -= alpha q, ||r||^2 (to `red`). Its

@@ -426,3 +426,29 @@ def test_report_export_carries_the_convergence_record(ops, tmp_path):
     assert s["iterations"] == s["steps"] == len(s["residual_history"]) > 0
     assert s["residual_history"][-1] == s["final_residual"] <= 1e-6
     assert v["extent"] == {"width": w, "height": h} and v["channels"] == 1 and v["all_finite"]
+
+
+@pytest.mark.parametrize("case", ["nan_source_interior", "inf_target_boundary", "nan_target_outside"])
+def test_non_finite_inputs_follow_the_reference(ctx, oracle, case):
+    """A NaN or infinity that reaches the system makes the residual NaN: the
+    reference stops by its stall rule with a NaN final residual
+    (poisson.rs:219-228); one that no interior cell reads leaves the solve
+    alone. The non-finite output pixels are the reference's."""
+    w = h = 16
+    rng = np.random.default_rng(1)
+    src = rng.random(w * h).astype(np.float32)
+    tgt = rng.random(w * h).astype(np.float32)
+    mask = np.zeros((h, w), np.float32)
+    mask[4:12, 4:12] = 1
+    mask = mask.reshape(-1)
+    if case == "nan_source_interior":
+        src[8 * w + 8] = np.nan
+    elif case == "inf_target_boundary":
+        tgt[3 * w + 8] = np.inf
+    else:
+        tgt[0] = np.nan
+    ref, rworst, _ = oracle.blend_channels(src, tgt, mask, 1, w, h, 2000, 1e-6, 0.0, 1.8)
+    out, per, worst = ctx.solve(src, tgt, mask, w, h, 1, lam=0.0, max_iterations=2000, tolerance=1e-6, omega=1.8)
+    assert worst["stop_reason"] == rworst.stop_reason and worst["converged"] == rworst.converged
+    assert np.isnan(worst["final_residual"]) == np.isnan(rworst.final_residual)
+    assert np.array_equal(~np.isfinite(out), ~np.isfinite(ref))

@@ -149,3 +149,28 @@ def test_multigrid_device_pointers_and_large_regions(ctx, L):
     for c in range(C):
         assert reps[c].converged and reps[c].final_residual <= 1e-6
         assert reps[c].iterations < 100, reps[c].iterations
+
+
+@pytest.mark.parametrize("case", ["nan_source_interior", "inf_target_boundary"])
+def test_multigrid_non_finite_residual_stalls(ctx, L, case):
+    """A NaN residual cannot improve: the multigrid path stops at once as
+    stalled with a NaN final residual and non-finite interior pixels (the
+    reference's outcome for a poisoned system), while non-interior pixels stay
+    the target's."""
+    w = h = 16
+    rng = np.random.default_rng(1)
+    src = rng.random(w * h).astype(np.float32)
+    tgt = rng.random(w * h).astype(np.float32)
+    mask = np.zeros((h, w), np.float32)
+    mask[4:12, 4:12] = 1
+    mask = mask.reshape(-1)
+    if case == "nan_source_interior":
+        src[8 * w + 8] = np.nan
+    else:
+        tgt[3 * w + 8] = np.inf
+    out, per, worst = ctx.solve(src, tgt, mask, w, h, 1, max_iterations=2000, tolerance=1e-6,
+                                flags=L.PT_FLAG_MULTIGRID)
+    assert worst["stop_reason"] == "stalled" and not worst["converged"] and np.isnan(worst["final_residual"])
+    inter = mask.reshape(h, w) > 0.5
+    assert not np.isfinite(out.reshape(h, w)[inter]).any()
+    assert np.array_equal(out.reshape(h, w)[~inter].view(np.uint32), tgt.reshape(h, w)[~inter].view(np.uint32))
