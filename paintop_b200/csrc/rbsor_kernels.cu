@@ -597,11 +597,26 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
     for (int j = 0; j < S; ++j)
       if (j == s - 1) acc[j] += part;
   }
+  // The S tile partials in one pass, each with block_sum's order (a warp's
+  // xor butterfly, then the warps in index order): one barrier instead of two
+  // per sweep. The scratch is the black plane of g, which nothing reads after
+  // the half-sweeps (the pass above reads only the red plane).
+  {
+    double *sr = reinterpret_cast<double *>(sG + G::PLANE);
 #pragma unroll
-  for (int j = 0; j < S; ++j) {
-    if (j >= s) break;
-    const double tot = block_sum(acc[j], sred);
-    if (tid == 0) P.partial[(long long)j * P.ntiles + t] = tot;
+    for (int j = 0; j < S; ++j) {
+      if (j >= s) break;
+      double v = acc[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) sr[j * kWarps + warp] = v;
+    }
+    __syncthreads();
+    if (tid < s) {
+      double tot = 0.0;
+      for (int w = 0; w < kWarps; ++w) tot += sr[tid * kWarps + w];
+      P.partial[(long long)tid * P.ntiles + t] = tot;
+    }
   }
 
   // ---- write the owned cells
