@@ -858,7 +858,9 @@ def gpu_arm(args):
 def batch_arm(args):
     """Batched uneven workload: 256 RGB instances, side log-uniform in [64, 1024],
     aspect in [0.5, 2], ellipse masks covering 20-60%, tol 1e-6, automatic omega,
-    solved in one persistent launch per batch (graph-replayed). A step = the batch."""
+    solved in one persistent launch per batch (graph-replayed). A step = the batch.
+    With --multigrid the same batch goes through multigrid-preconditioned CG
+    (PT_FLAG_MULTIGRID), every instance in each launch."""
     import ctypes as Ct
     import torch
     from paintop_b200 import _lib, synth
@@ -887,7 +889,7 @@ def batch_arm(args):
     outs_h = (Ct.c_void_p * n)()
     rep_arr = [(_lib.PtReport * (i.channels + 1))() for i in insts]
     rep_ptrs = (Ct.POINTER(_lib.PtReport) * n)(*[Ct.cast(r, Ct.POINTER(_lib.PtReport)) for r in rep_arr])
-    flags = _lib.PT_FLAG_OMEGA_AUTO
+    flags = _lib.PT_FLAG_MULTIGRID if args.multigrid else _lib.PT_FLAG_OMEGA_AUTO
     h2d = d2h = 0
     for k, inst in enumerate(insts):
         sh = torch.from_numpy(inst.source.reshape(-1)).pin_memory()
@@ -946,9 +948,14 @@ def batch_arm(args):
     e2e_elapsed, _ = timed(False)
     iters = [[r[c].iterations for c in range(i.channels)] for r, i in zip(rep_arr, insts)]
     conv = all(r[c].converged for r, i in zip(rep_arr, insts) for c in range(i.channels))
-    alg = sum(n_int * (BYTES_PER_SWEEP * sum(it) + BYTES_PER_RESIDUAL * (
-        sum(it) + sum(r[c].refinements for c in range(i.channels))))
-        for n_int, it, r, i in zip([interior_all[k] for k in share], iters, rep_arr, insts))
+    if args.multigrid:
+        # the multigrid model: 155 B per level-0 cell and channel per CG
+        # iteration, a third more for the coarser levels (multigrid_arm)
+        alg = sum(155.0 * 4.0 / 3.0 * i.width * i.height * sum(it) for it, i in zip(iters, insts))
+    else:
+        alg = sum(n_int * (BYTES_PER_SWEEP * sum(it) + BYTES_PER_RESIDUAL * (
+            sum(it) + sum(r[c].refinements for c in range(i.channels))))
+            for n_int, it, r, i in zip([interior_all[k] for k in share], iters, rep_arr, insts))
     total = len(allinst)
     line = None
     if rank == 0:
@@ -961,30 +968,35 @@ def batch_arm(args):
             t0 = time.perf_counter()
             for k in sample:
                 i = insts[k]
-                om = float(rep_arr[k][0].omega_used)
+                om = 1.8 if args.multigrid else float(rep_arr[k][0].omega_used)
                 O.blend_channels(i.source.reshape(-1), i.target.reshape(-1), i.mask.reshape(-1),
                                  i.channels, i.width, i.height, 100000, 1e-6, 0.0, om)
             dt = time.perf_counter() - t0
             cpu = {"value": len(sample) / dt, "unit": "instances/s", "cores": 1, "kind": "port",
                    "sample": f"{len(sample)} instances spread over the size range ({dt:.1f} s), "
-                             "row-major SOR at the omega the GPU chose"}
+                             + ("row-major SOR at the op's omega 1.8" if args.multigrid else
+                                "row-major SOR at the omega the GPU chose")}
         peak, peak_kind = _peaks()
         kmean = float(np.mean(kms))
         line = {
-            "metric": "Poisson instances/s @ rel-res 1e-6 (256 uneven RGB instances, one launch)",
+            "metric": ("Poisson instances/s @ rel-res 1e-6 (256 uneven RGB instances, multigrid-CG, one call)"
+                       if args.multigrid else
+                       "Poisson instances/s @ rel-res 1e-6 (256 uneven RGB instances, one launch)"),
             "value": total * args.steps / elapsed, "unit": "instances/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded sinusoid-plus-noise images, ellipse masks)",
             "config": {"workload": "batch_uneven", "instances": total, "tolerance": 1e-6,
-                       "omega": "automatic (device, per channel)",
-                       "tile_config": ctx.last_config(),
+                       "omega": "smoother 1.25" if args.multigrid else "automatic (device, per channel)",
+                       "solver": "multigrid-CG" if args.multigrid else "red-black SOR",
+                       "tile_config": None if args.multigrid else ctx.last_config(),
                        "l2": "inputs larger than L2"},
             "e2e": {"value": total * args.steps / e2e_elapsed, "unit": "instances/s",
                     "h2d_bytes_per_step": h2d * ws, "d2h_bytes_per_step": d2h * ws},
             "roofline": {"bound": "hbm", "achieved": alg / (kmean / 1e3) / 1e9, "peak": peak,
                          "unit": "GB/s", "frac": alg / (kmean / 1e3) / 1e9 / peak, "traffic": None,
-                         "kernel": "ptk::k_solve", "peak_kind": peak_kind, "kernel_ms_mean": kmean},
+                         "kernel": "multigrid-CG iteration (all kernels, modelled bytes)" if args.multigrid
+                         else "ptk::k_solve", "peak_kind": peak_kind, "kernel_ms_mean": kmean},
             "cpu_baseline": cpu, "gpu_launches": int(args.steps * ctx.last_timing()[2]),
             "clocks": clocks,
             "solver": {"converged": conv, "max_iterations": int(max(max(x) for x in iters)),
@@ -1142,6 +1154,8 @@ def main():
     ap.add_argument("--workload", default="screened_2048",
                     choices=["screened_2048", "batch_uneven", "masks", "multigrid", "clone_512", "train"])
     ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--multigrid", action="store_true",
+                    help="batch_uneven: solve by multigrid-preconditioned CG instead of red-black SOR")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-warm-start leg (4096x4096 RGB, learned vs plain)")
     args = ap.parse_args()

@@ -20,9 +20,17 @@
 // active fine cells and restriction its transpose / 4; smoothing is red-black
 // Gauss-Seidel, red then black before the coarse correction and black then
 // red after it, so the V-cycle is a symmetric operator and a valid CG
-// preconditioner. All channels of an image share the level masks and are
-// processed by the same launches. Every reduction is a fixed-order tree, so a
-// rerun is byte-identical.
+// preconditioner. Every reduction is a fixed-order tree, so a rerun is
+// byte-identical.
+//
+// Batches: every problem of a call (pt_poisson_solve_batch) keeps its own
+// level hierarchy, its own CG scalars per channel and its own stopping, but
+// all of them share each launch. A launch walks a table of blocks, each block
+// one 32 x 8 tile of one instance's plane, laid out per instance exactly as a
+// call with that instance alone lays it out, so partial sums, their
+// reduction order and hence every result of an instance are bit for bit what
+// it gets when solved alone. An (instance, channel) pair whose run has
+// stopped skips the V-cycle and the vector kernels.
 //
 // Report (pt_report): iterations = preconditioned CG iterations (each one
 // V-cycle and one operator application); history[k] = relative residual after
@@ -62,44 +70,30 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return r;
 }
 
-// ---- assembly ----------------------------------------------------------------
-// interior flag, u = anchor (or the warm guess at interior cells), b' =
-// fma(lambda, -anchor, laplacian(guidance)) at interior cells, all channels.
-__global__ void k_mg_assemble(int W, int H, int C, const float *__restrict__ guid, const float *__restrict__ anchor,
-                              const float *__restrict__ mask, const float *__restrict__ guess, double lambda,
-                              uint8_t *__restrict__ act, double *__restrict__ u, double *__restrict__ bl,
-                              double *__restrict__ uw) {
-  const long long N = (long long)W * H;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N * C;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(p / N);
-    const long long q = p - (long long)c * N;
-    const int j = (int)(q / W), i = (int)(q - (long long)j * W);
-    const bool in = W >= 3 && H >= 3 && i > 0 && j > 0 && i < W - 1 && j < H - 1 && mask[q] > 0.5f;
-    if (c == 0) act[q] = in ? 1 : 0;
-    const double a = (double)anchor[q * C + c];
-    u[p] = a;
-    double b = 0.0;
-    if (in) {
-      // poisson.rs:364-373: L, R, U, D, then fma(4, -centre, sum)
-      const double ctr = (double)guid[q * C + c];
-      const double s = (double)guid[(q - 1) * C + c] + (double)guid[(q + 1) * C + c] + (double)guid[(q - W) * C + c] +
-                       (double)guid[(q + W) * C + c];
-      b = fma(4.0, -ctr, s);
-    }
-    bl[p] = in ? fma(lambda, -a, b) : 0.0;
-    if (uw) uw[p] = (in && guess) ? (double)guess[q * C + c] : a;
-  }
-}
-
-// Stencil and vector kernels run on 2-D grids: threads (32, 8) over columns
-// and rows, grid.y strides over rows, grid.z is the channel; all index math is
-// 32-bit (a level has at most 2^31 cells). Kernels that reduce write one
-// partial per block, (blockIdx.y * gridDim.x + blockIdx.x), per channel.
+// Stencil and vector kernels run on tiles of (32, 8) threads over columns and
+// rows; a tile strides over the rows of its instance's plane, grid.z is the
+// channel. Kernels that reduce write one partial per tile and channel.
 constexpr int kTx = 32, kTy = 8;
 
-__device__ __forceinline__ int block_index() { return blockIdx.y * gridDim.x + blockIdx.x; }
-__device__ __forceinline__ int blocks_per_channel() { return gridDim.x * gridDim.y; }
+// One instance's plane as one launch tiles it. The blocks of a launch are the
+// instances' tiles one after another; bmap[blockIdx.x] names the entry.
+struct Geo {
+  int W, H;           // the tiled plane (restriction: the coarse one)
+  int gx, gy;         // tiles: gx across W (a half-sweep: across (W + 1) / 2), gy striding the rows
+  int blk0;           // the instance's first block in the launch
+  int C;              // its channels
+  int unit0;          // its first (instance, channel) unit: CG scalars, scales, run flags, reductions
+  int pad;
+  long long part0;    // its first partial sum (level-0 reductions): C * gx * gy of them, channel-major
+  long long o, oc;    // the plane's first cell in its level's one-channel (interior flags) and C-channel arrays
+  long long o2, oc2;  // the same for the other plane of a two-level kernel
+  int W2, H2;         // that plane (restriction: the fine level; prolongation: the coarse level)
+  float s, d;         // the level's 4^-k and diagonal 4^(1-k) + lambda (restriction: the fine level's)
+  double lambda;
+};
+
+// Where a block of a tiled launch works: its entry, tile column and row
+__device__ __forceinline__ int tile_b(const Geo &g) { return (int)blockIdx.x - g.blk0; }
 
 __device__ __forceinline__ double block_sum2(double v, double *sh) {
   const int t = threadIdx.y * kTx + threadIdx.x;
@@ -114,63 +108,136 @@ __device__ __forceinline__ double block_sum2(double v, double *sh) {
   return r;
 }
 
-// r = fma(lambda + 4, -u, nsum) - b' at interior cells (0 elsewhere) and
-// per-block partial sums of r^2.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(int W, int H, const uint8_t *__restrict__ act,
-                                                             const double *__restrict__ u,
-                                                             const double *__restrict__ bl, double lambda,
-                                                             double *__restrict__ r64, double *__restrict__ part) {
-  __shared__ double sh[kTx * kTy];
-  const int c = blockIdx.z;
+// Per-unit CG scalars: sc[unit] = {rho, rho_new, pq, rr, alpha, beta}
+enum { S_RHO, S_RHO_NEW, S_PQ, S_RR, S_ALPHA, S_BETA, S_N };
+
+// The caller-side buffers of one instance (device memory: the caller's, or
+// the staged copies of host buffers)
+struct Io {
+  const float *guid, *anchor, *mask, *guess;
+  float *out;
+};
+
+// ---- assembly ----------------------------------------------------------------
+// interior flag, u = anchor (or the warm guess at interior cells), b' =
+// fma(lambda, -anchor, laplacian(guidance)) at interior cells; level-0 tiles.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                           const Io *__restrict__ io, uint8_t *__restrict__ act,
+                                                           double *__restrict__ u, double *__restrict__ bl,
+                                                           double *__restrict__ uw) {
+  const int gi = bmap[blockIdx.x];
+  const Geo &g = geo[gi];
+  const int c = blockIdx.z, C = g.C;
+  if (c >= C) return;
+  const Io f = io[gi];
+  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
-  const double *uc = u + c * N;
-  const int i = blockIdx.x * kTx + threadIdx.x;
+  uint8_t *a = act + g.o;
+  double *uc = u + g.oc + c * N, *bc = bl + g.oc + c * N, *wc = uw ? uw + g.oc + c * N : nullptr;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
+    const size_t q = (size_t)j * W + i;
+    const bool in = W >= 3 && H >= 3 && i > 0 && j > 0 && i < W - 1 && j < H - 1 && f.mask[q] > 0.5f;
+    if (c == 0) a[q] = in ? 1 : 0;
+    const double av = (double)f.anchor[q * C + c];
+    uc[q] = av;
+    double bv = 0.0;
+    if (in) {
+      // poisson.rs:364-373: L, R, U, D, then fma(4, -centre, sum)
+      const float *gd = f.guid;
+      const double ctr = (double)gd[q * C + c];
+      const double s = (double)gd[(q - 1) * C + c] + (double)gd[(q + 1) * C + c] + (double)gd[(q - W) * C + c] +
+                       (double)gd[(q + W) * C + c];
+      bv = fma(4.0, -ctr, s);
+    }
+    bc[q] = in ? fma(g.lambda, -av, bv) : 0.0;
+    if (wc) wc[q] = (in && f.guess) ? (double)f.guess[q * C + c] : av;
+  }
+}
+
+// r = fma(lambda + 4, -u, nsum) - b' at interior cells (0 elsewhere) and
+// per-tile partial sums of r^2.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                             const uint8_t *__restrict__ act,
+                                                             const double *__restrict__ u,
+                                                             const double *__restrict__ bl, double *__restrict__ r64,
+                                                             double *__restrict__ part) {
+  __shared__ double sh[kTx * kTy];
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C) return;
+  const int W = g.W, H = g.H, gx = g.gx, gy = g.gy, b = tile_b(g), i = (b % gx) * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const uint8_t *a = act + g.o;
+  const double *uc = u + g.oc + c * N, *bc = bl + g.oc + c * N;
+  double *rc = r64 + g.oc + c * N;
+  const double lambda = g.lambda;
   double acc = 0.0;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
     const size_t q = (size_t)j * W + i;
     double r = 0.0;
-    if (act[q]) {
+    if (a[q]) {
       const double nsum = uc[q - 1] + uc[q + 1] + uc[q - W] + uc[q + W];  // L, R, U, D (poisson.rs:275-298)
-      r = fma(lambda + 4.0, -uc[q], nsum) - bl[c * N + q];
+      r = fma(lambda + 4.0, -uc[q], nsum) - bc[q];
     }
-    r64[c * N + q] = r;
+    rc[q] = r;
     acc += r * r;
   }
   const double t = block_sum2(acc, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
 }
 
-// out[c * stride] = fixed-order sum of part[c][0 .. n-1]; grid (C)
-__global__ void k_mg_reduce(const double *__restrict__ part, int n, double *__restrict__ out, int stride) {
+// A unit's partial sums: part[start .. start + n - 1]
+struct Red {
+  long long start, n;
+};
+
+// out[unit * stride] = fixed-order sum of the unit's partials; grid (units)
+__global__ void k_mg_reduce(const double *__restrict__ part, const Red *__restrict__ rtab, double *__restrict__ out,
+                            int stride) {
   __shared__ double sh[kThreads];
+  const Red rt = rtab[blockIdx.x];
   double acc = 0.0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) acc += part[(long long)blockIdx.x * n + k];
+  for (long long k = threadIdx.x; k < rt.n; k += blockDim.x) acc += part[rt.start + k];
   const double s = block_sum(acc, sh);
   if (threadIdx.x == 0) out[(long long)blockIdx.x * stride] = s;
 }
 
-// r32 = r64 / scale[c] (0 where the channel is not being corrected)
-__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(int W, int H, const double *__restrict__ r64,
+// r32 = r64 / scale[unit] (0 where the unit is not being corrected)
+__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                        const double *__restrict__ r64,
                                                         const double *__restrict__ scale, float *__restrict__ r32) {
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C) return;
+  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
-  const double s = scale[c];
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
-    const size_t o = c * N + (size_t)j * W + i;
-    r32[o] = s > 0.0 ? (float)(r64[o] / s) : 0.0f;
+  const double s = scale[g.unit0 + c];
+  const double *rc = r64 + g.oc + c * N;
+  float *oc = r32 + g.oc + c * N;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
+    const size_t q = (size_t)j * W + i;
+    oc[q] = s > 0.0 ? (float)(rc[q] / s) : 0.0f;
   }
 }
 
-// u += scale[c] * x at interior cells
-__global__ void __launch_bounds__(kTx * kTy) k_mg_update(int W, int H, const uint8_t *__restrict__ act,
-                                                         const float *__restrict__ x, const double *__restrict__ scale,
-                                                         double *__restrict__ u) {
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+// u += scale[unit] * x at interior cells; a unit with scale 0 (not being
+// corrected) is left as it is, bit for bit
+__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                         const uint8_t *__restrict__ act, const float *__restrict__ x,
+                                                         const double *__restrict__ scale, double *__restrict__ u) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C) return;
+  const double s = scale[g.unit0 + c];
+  if (s == 0.0) return;
+  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
-  const double s = scale[c];
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+  const uint8_t *a = act + g.o;
+  const float *xc = x + g.oc + c * N;
+  double *uc = u + g.oc + c * N;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
     const size_t q = (size_t)j * W + i;
-    if (act[q]) u[c * N + q] = fma(s, (double)x[c * N + q], u[c * N + q]);
+    if (a[q]) uc[q] = fma(s, (double)xc[q], uc[q]);
   }
 }
 
@@ -188,35 +255,46 @@ constexpr int kCoarseRule = 3;
 // the same four masks; the coarsest level keeps plain Gauss-Seidel.
 constexpr float kSmoothOmega = 1.25f;
 
-__global__ void k_mg_coarsen(int Wf, int Hf, const uint8_t *__restrict__ af, int Wc, int Hc, uint8_t *__restrict__ ac) {
-  const long long N = (long long)Wc * Hc;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < N; q += (long long)gridDim.x * blockDim.x) {
-    const int J = (int)(q / Wc), I = (int)(q - (long long)J * Wc);
+// Coarse interior flags from the fine ones; tiles of the coarse plane (the
+// fine plane is the entry's second).
+__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                          const uint8_t *__restrict__ af, uint8_t *__restrict__ ac) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int Wc = g.W, Hc = g.H, Wf = g.W2, Hf = g.H2, b = tile_b(g), I = (b % g.gx) * kTx + threadIdx.x;
+  const uint8_t *f = af + g.o2;
+  uint8_t *cc = ac + g.o;
+  for (int J = (b / g.gx) * kTy + threadIdx.y; J < Hc && I < Wc; J += g.gy * kTy) {
     int n = 0;
     for (int dy = 0; dy < 2; ++dy)
       for (int dx = 0; dx < 2; ++dx) {
         const int i = 2 * I + dx, j = 2 * J + dy;
-        if (i < Wf && j < Hf) n += af[(long long)j * Wf + i];
+        if (i < Wf && j < Hf) n += f[(size_t)j * Wf + i];
       }
-    ac[q] = n >= kCoarseRule ? 1 : 0;
+    cc[(size_t)J * Wc + I] = n >= kCoarseRule ? 1 : 0;
   }
 }
 
 // One colour of red-black Gauss-Seidel on A_k e = rhs: e = (rhs + s * sum of
 // neighbours) / d at active cells of that colour (inactive cells hold 0).
-// x threads index the cells of one colour in a row.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(int W, int H, const uint8_t *__restrict__ act,
-                                                         const float *__restrict__ rhs, float *__restrict__ e, float s,
-                                                         float d, int color) {
-  const int c = blockIdx.z, m = blockIdx.x * kTx + threadIdx.x;
+// x threads index the cells of one colour in a row (half-sweep tiles).
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                         const uint8_t *__restrict__ act,
+                                                         const float *__restrict__ rhs, float *__restrict__ e,
+                                                         const double *__restrict__ run, int color) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  const int W = g.W, H = g.H, b = tile_b(g), m = (b % g.gx) * kTx + threadIdx.x;
+  const float s = g.s, d = g.d;
   const size_t N = (size_t)W * H;
-  float *ec = e + c * N;
-  const float *rc = rhs + c * N;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H; j += gridDim.y * kTy) {
+  const uint8_t *a = act + g.o;
+  float *ec = e + g.oc + c * N;
+  const float *rc = rhs + g.oc + c * N;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H; j += g.gy * kTy) {
     const int i = 2 * m + ((j + color) & 1);
     if (i >= W) continue;
     const size_t q = (size_t)j * W + i;
-    if (!act[q]) continue;
+    if (!a[q]) continue;
     float nb = 0.0f;
     if (i > 0) nb += ec[q - 1];
     if (i < W - 1) nb += ec[q + 1];
@@ -231,32 +309,48 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(int W, int H, const uin
 // cells of colour 0 (red), 0 everywhere else, relaxed by kSmoothOmega -- what
 // zeroing e and one red half-sweep produce, bit for bit, in one pass that
 // writes every cell.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth_first(int W, int H, const uint8_t *__restrict__ act,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth_first(const Geo *__restrict__ geo,
+                                                               const int *__restrict__ bmap,
+                                                               const uint8_t *__restrict__ act,
                                                                const float *__restrict__ rhs, float *__restrict__ e,
-                                                               float s, float d) {
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+                                                               const double *__restrict__ run) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
+  const float s = g.s, d = g.d;
   const size_t N = (size_t)W * H;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+  const uint8_t *a = act + g.o;
+  float *ec = e + g.oc + c * N;
+  const float *rc = rhs + g.oc + c * N;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
     const size_t q = (size_t)j * W + i;
-    const float gs = (rhs[c * N + q] + s * 0.0f) / d;
-    e[c * N + q] = (act[q] && ((i + j) & 1) == 0) ? 0.0f + kSmoothOmega * (gs - 0.0f) : 0.0f;
+    const float gs = (rc[q] + s * 0.0f) / d;
+    ec[q] = (a[q] && ((i + j) & 1) == 0) ? 0.0f + kSmoothOmega * (gs - 0.0f) : 0.0f;
   }
 }
 
 // The coarsest level (at most kCoarseMax cells): `sweeps` red-black sweeps,
 // then as many in reverse colour order, from e = 0, in shared memory; one
-// block per channel.
+// block per instance (blockIdx.x = its entry) and channel (blockIdx.z).
 constexpr int kCoarseMax = 64;
 
-__global__ void k_mg_coarse(int W, int H, const uint8_t *__restrict__ act, const float *__restrict__ rhs,
-                            float *__restrict__ e, float s, float d, int sweeps) {
+__global__ void k_mg_coarse(const Geo *__restrict__ geo, const uint8_t *__restrict__ act,
+                            const float *__restrict__ rhs, float *__restrict__ e, const double *__restrict__ run,
+                            int sweeps) {
   __shared__ float se[kCoarseMax], sr[kCoarseMax];
   __shared__ uint8_t sa[kCoarseMax];
-  const int n = W * H, c = blockIdx.x, t = threadIdx.x;
+  const Geo &g = geo[blockIdx.x];
+  const int c = blockIdx.z;
+  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  const int W = g.W, H = g.H, n = W * H, t = threadIdx.x;
+  const float s = g.s, d = g.d;
+  const float *rc = rhs + g.oc + (long long)c * n;
+  float *ecp = e + g.oc + (long long)c * n;
   if (t < n) {
     se[t] = 0.0f;
-    sr[t] = rhs[(long long)c * n + t];
-    sa[t] = act[t];
+    sr[t] = rc[t];
+    sa[t] = act[g.o + t];
   }
   __syncthreads();
   const int j = t / max(W, 1), i = t - j * W;
@@ -278,7 +372,7 @@ __global__ void k_mg_coarse(int W, int H, const uint8_t *__restrict__ act, const
     if (mine) se[t] = v;
     __syncthreads();
   }
-  if (t < n) e[(long long)c * n + t] = se[t];
+  if (t < n) ecp[t] = se[t];
 }
 
 __device__ __forceinline__ float pw(int a) { return (a == 0 || a == 1) ? 0.75f : 0.25f; }  // a = fine - 2 * coarse
@@ -286,29 +380,38 @@ __device__ __forceinline__ float pw(int a) { return (a == 0 || a == 1) ? 0.75f :
 // The restriction of the level's residual, rhs_c(I, J) = sum over fine
 // (2I + a, 2J + b), a, b in -1..2, of wx wy res_f / 4 with res_f = rhs - A e at
 // active fine cells (0 elsewhere), evaluated on the fly so the residual is
-// never stored.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(int Wf, int Hf, const uint8_t *__restrict__ af,
+// never stored. Tiles of the coarse plane; the fine plane is the second.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(const Geo *__restrict__ geo,
+                                                                 const int *__restrict__ bmap,
+                                                                 const uint8_t *__restrict__ af,
                                                                  const float *__restrict__ rhsf,
-                                                                 const float *__restrict__ ef, float s, float d, int Wc,
-                                                                 int Hc, const uint8_t *__restrict__ ac,
-                                                                 float *__restrict__ rhsc) {
-  const int c = blockIdx.z, I = blockIdx.x * kTx + threadIdx.x;
+                                                                 const float *__restrict__ ef,
+                                                                 const uint8_t *__restrict__ ac,
+                                                                 float *__restrict__ rhsc,
+                                                                 const double *__restrict__ run) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  const int Wc = g.W, Hc = g.H, Wf = g.W2, Hf = g.H2, b = tile_b(g), I = (b % g.gx) * kTx + threadIdx.x;
+  const float s = g.s, d = g.d;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
-  const float *e = ef + c * Nf, *rh = rhsf + c * Nf;
-  for (int J = blockIdx.y * kTy + threadIdx.y; J < Hc && I < Wc; J += gridDim.y * kTy) {
+  const float *e = ef + g.oc2 + c * Nf, *rh = rhsf + g.oc2 + c * Nf;
+  const uint8_t *fa = af + g.o2, *ca = ac + g.o;
+  float *out = rhsc + g.oc + c * Nc;
+  for (int J = (b / g.gx) * kTy + threadIdx.y; J < Hc && I < Wc; J += g.gy * kTy) {
     const size_t q = (size_t)J * Wc + I;
     float v = 0.0f;
-    if (ac[q]) {
-      for (int b = -1; b <= 2; ++b) {
-        const int j = 2 * J + b;
+    if (ca[q]) {
+      for (int bb = -1; bb <= 2; ++bb) {
+        const int j = 2 * J + bb;
         if (j < 0 || j >= Hf) continue;
         float row = 0.0f;
-        for (int a = -1; a <= 2; ++a) {
-          const int i = 2 * I + a;
+        for (int aa = -1; aa <= 2; ++aa) {
+          const int i = 2 * I + aa;
           if (i < 0 || i >= Wf) continue;
           const size_t f = (size_t)j * Wf + i;
           float r = 0.0f;
-          if (af[f]) {
+          if (fa[f]) {
             float nb = 0.0f;
             if (i > 0) nb += e[f - 1];
             if (i < Wf - 1) nb += e[f + 1];
@@ -316,213 +419,310 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(int Wf, int Hf,
             if (j < Hf - 1) nb += e[f + Wf];
             r = rh[f] - (d * e[f] - s * nb);
           }
-          row += pw(a) * r;
+          row += pw(aa) * r;
         }
-        v += pw(b) * row;
+        v += pw(bb) * row;
       }
       v *= 0.25f;
     }
-    rhsc[c * Nc + q] = v;
+    out[q] = v;
   }
 }
 
-// e_f += bilinear prolongation of e_c at active fine cells
-__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(int Wf, int Hf, const uint8_t *__restrict__ af,
-                                                          float *__restrict__ ef, int Wc, int Hc,
-                                                          const float *__restrict__ ec) {
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+// e_f += bilinear prolongation of e_c at active fine cells; tiles of the fine
+// plane, the coarse plane is the second.
+__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                          const uint8_t *__restrict__ af, float *__restrict__ ef,
+                                                          const float *__restrict__ ec,
+                                                          const double *__restrict__ run) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  const int Wf = g.W, Hf = g.H, Wc = g.W2, Hc = g.H2, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
-  const float *e = ec + c * Nc;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < Hf && i < Wf; j += gridDim.y * kTy) {
+  const float *e = ec + g.oc2 + c * Nc;
+  float *out = ef + g.oc + c * Nf;
+  const uint8_t *fa = af + g.o;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < Hf && i < Wf; j += g.gy * kTy) {
     const size_t q = (size_t)j * Wf + i;
-    if (!af[q]) continue;
+    if (!fa[q]) continue;
     const int I0 = i >> 1, J0 = j >> 1;
     const int I1 = (i & 1) ? I0 + 1 : I0 - 1, J1 = (j & 1) ? J0 + 1 : J0 - 1;
     auto at = [&](int I, int J) -> float {
       return (I >= 0 && I < Wc && J >= 0 && J < Hc) ? e[(size_t)J * Wc + I] : 0.0f;
     };
     const float v = 0.5625f * at(I0, J0) + 0.1875f * (at(I1, J0) + at(I0, J1)) + 0.0625f * at(I1, J1);
-    ef[c * Nf + q] += v;
+    out[q] += v;
   }
 }
 
-// ---- conjugate gradients -------------------------------------------------------
+// ---- conjugate gradients (level-0 tiles) ---------------------------------------
+__device__ __forceinline__ void zero_partial(const Geo &g, int c, double *part) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * g.gx * g.gy + tile_b(g)] = 0.0;
+}
+
 // q = A_0 p at active cells; partial sums of p.q
-__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(int W, int H, const uint8_t *__restrict__ act,
-                                                        const float *__restrict__ p, float d, float *__restrict__ q,
-                                                        double *__restrict__ part) {
+__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                        const uint8_t *__restrict__ act, const float *__restrict__ p,
+                                                        float *__restrict__ q, double *__restrict__ part,
+                                                        const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C) return;
+  if (run[g.unit0 + c] == 0.0) {  // a stopped unit: its p.q is never read
+    zero_partial(g, c, part);
+    return;
+  }
+  const int W = g.W, H = g.H, gx = g.gx, gy = g.gy, b = tile_b(g), i = (b % gx) * kTx + threadIdx.x;
+  const float d = g.d;
   const size_t N = (size_t)W * H;
-  const float *pc = p + c * N;
+  const uint8_t *a = act + g.o;
+  const float *pc = p + g.oc + c * N;
+  float *qc = q + g.oc + c * N;
   double acc = 0.0;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
+  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
     const size_t k = (size_t)j * W + i;
     float v = 0.0f;
-    if (act[k]) {
+    if (a[k]) {
       // interior cells are never on the border: all four neighbours exist
       v = d * pc[k] - (pc[k - 1] + pc[k + 1] + pc[k - W] + pc[k + W]);
       acc += (double)pc[k] * (double)v;
     }
-    q[c * N + k] = v;
+    qc[k] = v;
   }
   const double t = block_sum2(acc, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
 }
 
 // partial sums of a.b
-__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(int W, int H, const float *__restrict__ a,
-                                                      const float *__restrict__ b, double *__restrict__ part) {
+__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                      const float *__restrict__ x, const float *__restrict__ y,
+                                                      double *__restrict__ part, const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C) return;
+  if (run[g.unit0 + c] == 0.0) {  // a stopped unit: its rho is never read
+    zero_partial(g, c, part);
+    return;
+  }
+  const int W = g.W, H = g.H, gx = g.gx, gy = g.gy, b = tile_b(g), i = (b % gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
+  const float *xc = x + g.oc + c * N, *yc = y + g.oc + c * N;
   double acc = 0.0;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
-    const size_t o = c * N + (size_t)j * W + i;
-    acc += (double)a[o] * (double)b[o];
+  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
+    const size_t o = (size_t)j * W + i;
+    acc += (double)xc[o] * (double)yc[o];
   }
   const double t = block_sum2(acc, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
 }
 
-// Per-channel scalars: sc[c] = {rho, rho_new, pq, rr, alpha, beta, run}
-enum { S_RHO, S_RHO_NEW, S_PQ, S_RR, S_ALPHA, S_BETA, S_RUN, S_N };
-
 // p = z + beta p (beta = rho_new / rho; p = z on the first iteration)
-__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(int W, int H, const float *__restrict__ z,
-                                                            float *__restrict__ p, const double *__restrict__ sc,
-                                                            int first) {
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
-  const size_t N = (size_t)W * H;
-  const double *s = sc + c * S_N;
-  if (s[S_RUN] == 0.0) return;
+__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                            const float *__restrict__ z, float *__restrict__ p,
+                                                            const double *__restrict__ sc,
+                                                            const double *__restrict__ run, int first) {
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  const double *s = sc + (long long)(g.unit0 + c) * S_N;
   const float beta = first ? 0.0f : (float)(s[S_RHO] != 0.0 ? s[S_RHO_NEW] / s[S_RHO] : 0.0);
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
-    const size_t o = c * N + (size_t)j * W + i;
-    p[o] = first ? z[o] : z[o] + beta * p[o];  // first: p is not read (it holds what the arena held)
+  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const float *zc = z + g.oc + c * N;
+  float *pc = p + g.oc + c * N;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
+    const size_t o = (size_t)j * W + i;
+    pc[o] = first ? zc[o] : zc[o] + beta * pc[o];  // first: p is not read (it holds what the arena held)
   }
 }
 
-__global__ void k_cg_scalars_after_dir(int C, double *__restrict__ sc) {
-  for (int c = threadIdx.x; c < C; c += blockDim.x) sc[c * S_N + S_RHO] = sc[c * S_N + S_RHO_NEW];
+__global__ void k_cg_scalars_after_dir(int U, double *__restrict__ sc) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < U; k += gridDim.x * blockDim.x)
+    sc[(long long)k * S_N + S_RHO] = sc[(long long)k * S_N + S_RHO_NEW];
 }
 
 // x += alpha p, r -= alpha q (alpha = rho / p.q); partial sums of r.r
-__global__ void __launch_bounds__(kTx * kTy) k_cg_step(int W, int H, const float *__restrict__ p,
-                                                       const float *__restrict__ q, float *__restrict__ x,
-                                                       float *__restrict__ r, const double *__restrict__ sc,
-                                                       double *__restrict__ part) {
+__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                       const float *__restrict__ p, const float *__restrict__ q,
+                                                       float *__restrict__ x, float *__restrict__ r,
+                                                       const double *__restrict__ sc, double *__restrict__ part,
+                                                       const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const int c = blockIdx.z, i = blockIdx.x * kTx + threadIdx.x;
-  const size_t N = (size_t)W * H;
-  const double *s = sc + c * S_N;
-  if (s[S_RUN] == 0.0) {  // a stopped channel: x and r stay (p may never have been written)
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = 0.0;
+  const Geo &g = geo[bmap[blockIdx.x]];
+  const int c = blockIdx.z;
+  if (c >= g.C) return;
+  if (run[g.unit0 + c] == 0.0) {  // a stopped unit: x and r stay (p may never have been written)
+    zero_partial(g, c, part);
     return;
   }
+  const double *s = sc + (long long)(g.unit0 + c) * S_N;
   const float alpha = s[S_PQ] > 0.0 ? (float)(s[S_RHO] / s[S_PQ]) : 0.0f;
+  const int W = g.W, H = g.H, gx = g.gx, gy = g.gy, b = tile_b(g), i = (b % gx) * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const float *pc = p + g.oc + c * N, *qc = q + g.oc + c * N;
+  float *xc = x + g.oc + c * N, *rc = r + g.oc + c * N;
   double acc = 0.0;
-  for (int j = blockIdx.y * kTy + threadIdx.y; j < H && i < W; j += gridDim.y * kTy) {
-    const size_t o = c * N + (size_t)j * W + i;
-    x[o] += alpha * p[o];
-    const float rv = r[o] - alpha * q[o];
-    r[o] = rv;
+  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
+    const size_t o = (size_t)j * W + i;
+    xc[o] += alpha * pc[o];
+    const float rv = rc[o] - alpha * qc[o];
+    rc[o] = rv;
     acc += (double)rv * (double)rv;
   }
   const double t = block_sum2(acc, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0) part[(size_t)c * blocks_per_channel() + block_index()] = t;
+  if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
 }
 
 // out = interleave(u) at interior cells, the anchor elsewhere (bit for bit)
-__global__ void k_mg_emit(int W, int H, int C, const uint8_t *__restrict__ act, const double *__restrict__ u,
-                          const float *__restrict__ anchor, float *__restrict__ out) {
-  const long long N = (long long)W * H;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N * C;
-       k += (long long)gridDim.x * blockDim.x) {
-    const long long q = k / C;
-    const int c = (int)(k - q * C);
-    out[k] = act[q] ? (float)u[(long long)c * N + q] : anchor[k];
+__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+                                                       const Io *__restrict__ io, const uint8_t *__restrict__ act,
+                                                       const double *__restrict__ u) {
+  const int gi = bmap[blockIdx.x];
+  const Geo &g = geo[gi];
+  const int c = blockIdx.z, C = g.C;
+  if (c >= C) return;
+  const Io f = io[gi];
+  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
+  const size_t N = (size_t)W * H;
+  const uint8_t *a = act + g.o;
+  const double *uc = u + g.oc + c * N;
+  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
+    const size_t q = (size_t)j * W + i;
+    f.out[q * C + c] = a[q] ? (float)uc[q] : f.anchor[q * C + c];
   }
 }
 
 // ---- host ----------------------------------------------------------------------
-struct Level {
-  int W, H;
-  size_t act, e, rhs;  // arena offsets
-  float s, d;
+size_t aup(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// (32, 8)-thread tiles over w columns and h rows of one instance: at most
+// about 8 tiles per SM per channel (rows are strided), at most 65535 rows of
+// tiles.
+void tiles2(int w, int h, int sms, int &gx, int &gy) {
+  gx = std::max(1, (w + kTx - 1) / kTx);
+  gy = std::max(1, (h + kTy - 1) / kTy);
+  gy = std::min(gy, std::max(1, sms * 8 / gx));
+  gy = std::min(gy, 65535);
+}
+const dim3 kBlock2(kTx, kTy);
+
+float level_s(int k) { return 1.0f / (float)(1u << (2 * std::min(k, 15))); }
+
+// A call is cut into groups of at most this many level-0 tiles (and units);
+// every launch of a group then has fewer blocks.
+constexpr long long kGroupTiles = 1ll << 22;
+
+// One instance (a problem with channels) of a group
+struct Inst {
+  int idx;                       // its index in the caller's arrays
+  int W, H, C, L;                // extent, channels, levels
+  double lambda;
+  std::vector<int> w, h;         // level extents
+  std::vector<long long> o, oc;  // level offsets in the one-channel and C-channel arrays
+  int unit0 = 0;                 // first (instance, channel) unit
+  long long part0 = 0;           // first level-0 partial sum
+  int gx = 1, gy = 1;            // level-0 tiles
+  bool dev = false, warm = false;
+  size_t in = 0, mask = 0, guess = 0, out = 0;  // staged copies of host buffers
 };
 
-size_t aup(size_t b) { return (b + 255) & ~(size_t)255; }
+// One kind of launch at one level: its table entries and blocks
+struct Launch {
+  size_t geo = 0, bmap = 0;  // byte offsets of the tables in the table area
+  int n = 0;                 // entries (instances)
+  long long blocks = 0;
+};
+
+struct LevelArr {
+  size_t act = 0, e = 0, rhs = 0;
+};
+
+// Tables built on the host and uploaded in one copy
+struct Blob {
+  std::vector<unsigned char> b;
+  size_t put(const void *p, size_t n) {
+    const size_t o = (b.size() + 15) & ~(size_t)15;
+    b.resize(o + n);
+    if (n) std::memcpy(b.data() + o, p, n);
+    return o;
+  }
+};
+
+Launch make_launch(Blob &blob, std::vector<Geo> &gs) {
+  Launch l;
+  l.n = (int)gs.size();
+  std::vector<int> bm;
+  long long blk = 0;
+  for (size_t k = 0; k < gs.size(); ++k) {
+    gs[k].blk0 = (int)blk;
+    const long long nb = (long long)gs[k].gx * gs[k].gy;
+    bm.insert(bm.end(), (size_t)nb, (int)k);
+    blk += nb;
+  }
+  l.blocks = blk;
+  l.geo = blob.put(gs.data(), gs.size() * sizeof(Geo));
+  l.bmap = blob.put(bm.data(), bm.size() * sizeof(int));
+  return l;
+}
 
 struct Mg {
   pt_ctx *ctx;
   cudaStream_t st;
   char *base = nullptr;
-  int W, H, C;
-  long long N;
-  std::vector<Level> lv;
-  size_t u, bl, uw, r64, part, red, sc, scale, x, r, z, p, q;
-  size_t in, mask, guess, out;  // staged inputs (host buffers)
-  int nb;                        // blocks per channel of the reductions
+  unsigned Cmax = 1;
+  int U = 0;
+  std::vector<Inst> in;
+  std::vector<LevelArr> lv;
+  Launch all0;
+  std::vector<Launch> full, half, restr, coarse;  // per level
+  size_t tab = 0, rtab = 0, io = 0;
+  size_t u = 0, bl = 0, uw = 0, r64 = 0, part = 0, red = 0, sc = 0, scale = 0, run = 0, x = 0, r = 0, z = 0, p = 0,
+         q = 0;
   long long launches = 0;
   template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
+  const Geo *geo(const Launch &l) { return at<Geo>(tab + l.geo); }
+  const int *bmap(const Launch &l) { return at<int>(tab + l.bmap); }
+  dim3 grid(const Launch &l, unsigned z) { return dim3((unsigned)l.blocks, 1, z); }
 };
 
-// (32, 8) threads over w columns and h rows, channels in z; at most about 8
-// blocks per SM per channel (rows are strided), at most 65535 in y.
-dim3 grid2(int w, int h, int C, int sms) {
-  const int gx = std::max(1, (w + kTx - 1) / kTx);
-  int gy = std::max(1, (h + kTy - 1) / kTy);
-  gy = std::min(gy, std::max(1, sms * 8 / gx));
-  gy = std::min(gy, 65535);
-  return dim3(gx, gy, C);
-}
-const dim3 kBlock2(kTx, kTy);
-
-unsigned blocks(long long n, int sms) {
-  return (unsigned)std::max<long long>(1, std::min<long long>((n + kThreads - 1) / kThreads, (long long)sms * 8));
-}
-
-void vcycle(Mg &m, size_t rhs0, size_t e0) {
+void vcycle(Mg &m, float *rhs0, float *e0) {
   const int L = (int)m.lv.size();
-  const int sms = m.ctx->sms;
+  const double *run = m.at<double>(m.run);
+  const unsigned Cz = m.Cmax;
   for (int k = 0; k < L; ++k) {
-    Level &v = m.lv[k];
-    const size_t rhs = k == 0 ? rhs0 : v.rhs, e = k == 0 ? e0 : v.e;
-    const dim3 gh = grid2((v.W + 1) / 2, v.H, m.C, sms), g = grid2(v.W, v.H, m.C, sms);
-    if (k == L - 1) {  // the coarsest level: symmetric sweeps in one block per channel
-      k_mg_coarse<<<m.C, kCoarseMax, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e),
-                                                 v.s, v.d, 24);
+    const LevelArr &v = m.lv[k];
+    float *rhs = k == 0 ? rhs0 : m.at<float>(v.rhs), *e = k == 0 ? e0 : m.at<float>(v.e);
+    const uint8_t *act = m.at<uint8_t>(v.act);
+    const Launch &K = m.coarse[k];
+    if (K.n) {  // instances whose coarsest level this is: symmetric sweeps in one block per channel
+      k_mg_coarse<<<dim3((unsigned)K.n, 1, Cz), kCoarseMax, 0, m.st>>>(m.geo(K), act, rhs, e, run, 24);
       ++m.launches;
-      break;
     }
+    const Launch &F = m.full[k], &Hh = m.half[k], &R = m.restr[k];
+    if (!F.n) continue;
     // red, black, red, black from e = 0 (the first red half-sweep writes all of e)
-    k_mg_smooth_first<<<g, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                               v.d);
-    k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
-                                          1);
-    k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
-                                          0);
-    k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s, v.d,
-                                          1);
-    m.launches += 4;
-    Level &cl = m.lv[k + 1];
-    const dim3 gc = grid2(cl.W, cl.H, m.C, sms);
-    k_mg_resid_restrict<<<gc, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e),
-                                                  v.s, v.d, cl.W, cl.H, m.at<uint8_t>(cl.act), m.at<float>(cl.rhs));
-    ++m.launches;
+    k_mg_smooth_first<<<m.grid(F, Cz), kBlock2, 0, m.st>>>(m.geo(F), m.bmap(F), act, rhs, e, run);
+    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 1);
+    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 0);
+    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 1);
+    const LevelArr &cl = m.lv[k + 1];
+    k_mg_resid_restrict<<<m.grid(R, Cz), kBlock2, 0, m.st>>>(m.geo(R), m.bmap(R), act, rhs, e,
+                                                              m.at<uint8_t>(cl.act), m.at<float>(cl.rhs), run);
+    m.launches += 5;
   }
   for (int k = L - 2; k >= 0; --k) {
-    Level &v = m.lv[k], &cl = m.lv[k + 1];
-    const size_t rhs = k == 0 ? rhs0 : v.rhs, e = k == 0 ? e0 : v.e;
-    const dim3 gh = grid2((v.W + 1) / 2, v.H, m.C, sms), g = grid2(v.W, v.H, m.C, sms);
-    k_mg_prolong<<<g, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(e), cl.W, cl.H,
-                                           m.at<float>(cl.e));
+    const Launch &F = m.full[k], &Hh = m.half[k];
+    if (!F.n) continue;
+    const LevelArr &v = m.lv[k], &cl = m.lv[k + 1];
+    float *rhs = k == 0 ? rhs0 : m.at<float>(v.rhs), *e = k == 0 ? e0 : m.at<float>(v.e);
+    const uint8_t *act = m.at<uint8_t>(v.act);
+    k_mg_prolong<<<m.grid(F, Cz), kBlock2, 0, m.st>>>(m.geo(F), m.bmap(F), act, e, m.at<float>(cl.e), run);
     for (int t = 0; t < 2; ++t) {
-      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                             v.d, 1);
-      k_mg_smooth<<<gh, kBlock2, 0, m.st>>>(v.W, v.H, m.at<uint8_t>(v.act), m.at<float>(rhs), m.at<float>(e), v.s,
-                                             v.d, 0);
+      k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 1);
+      k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 0);
     }
     m.launches += 5;
   }
@@ -533,168 +733,274 @@ pt_status mfail(pt_ctx *ctx, pt_status s, const std::string &msg) {
   return s;
 }
 
-}  // namespace
-
-// One problem through multigrid-preconditioned CG (called by pt_poisson_solve
-// and pt_poisson_solve_batch for problems with PT_FLAG_MULTIGRID).
-pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, pt_report *reports, double *history) {
-  const int W = (int)p.width, H = (int)p.height, C = (int)p.channels;
-  const bool dev = (p.flags & PT_FLAG_DEVICE_POINTERS) != 0, warm = (p.flags & PT_FLAG_WARM_START) != 0;
-  if (C == 0) {
-    pt_report r{};
-    r.converged = 1; r.stop_reason = PT_STOP_CONVERGED; r.tolerance = p.tolerance; r.channel = -1;
-    reports[0] = r;
-    return PT_OK;
-  }
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  cudaError_t ce = cudaSetDevice(ctx->device);
-  if (ce != cudaSuccess) return mfail(ctx, PT_NO_DEVICE, cudaGetErrorString(ce));
-  for (auto &e : ctx->ev)
-    if (!e && cudaEventCreate(&e) != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, "event create");
+// One group of instances (ids: indices into ps, all with channels > 0)
+pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> &ids, float *const *outs,
+                      pt_report *const *reports, double *const *histories, double &solve_ms, double &call_ms,
+                      long long &launches) {
+  const int sms = ctx->sms;
   Mg m;
-  m.ctx = ctx; m.st = ctx->stream; m.W = W; m.H = H; m.C = C; m.N = (long long)W * H;
-  const long long N = m.N, NC = N * C;
-  const dim3 g0 = grid2(W, H, C, ctx->sms);  // level-0 grid of every reducing kernel
-  m.nb = (int)(g0.x * g0.y);
-  // levels: halve (ceil) while the level has more than 64 cells
-  {
-    int w = W, h = H, k = 0;
+  m.ctx = ctx;
+  m.st = ctx->stream;
+  // instances, their levels (halve, ceil, while a level has more than
+  // kCoarseMax cells), units and level-0 partial sums
+  int Lmax = 0;
+  long long P = 0;
+  bool any_warm = false;
+  for (int id : ids) {
+    const pt_problem &p = ps[id];
+    Inst I;
+    I.idx = id; I.W = (int)p.width; I.H = (int)p.height; I.C = (int)p.channels; I.lambda = p.lambda;
+    I.dev = (p.flags & PT_FLAG_DEVICE_POINTERS) != 0;
+    I.warm = (p.flags & PT_FLAG_WARM_START) != 0;
+    int w = I.W, h = I.H, k = 0;
     for (;;) {
-      const float s = 1.0f / (float)(1u << (2 * std::min(k, 15)));
-      m.lv.push_back(Level{w, h, 0, 0, 0, s, 4.0f * s + (float)p.lambda});
+      I.w.push_back(w);
+      I.h.push_back(h);
       if ((long long)w * h <= kCoarseMax || k >= 30) break;
       w = (w + 1) / 2; h = (h + 1) / 2; ++k;
     }
+    I.L = (int)I.w.size();
+    tiles2(I.W, I.H, sms, I.gx, I.gy);
+    I.unit0 = m.U;
+    m.U += I.C;
+    I.part0 = P;
+    P += (long long)I.C * I.gx * I.gy;
+    Lmax = std::max(Lmax, I.L);
+    m.Cmax = std::max(m.Cmax, (unsigned)I.C);
+    any_warm |= I.warm;
+    m.in.push_back(std::move(I));
   }
+  const int U = m.U;
+  std::vector<long long> cells(Lmax, 0), ccells(Lmax, 0);
+  for (Inst &I : m.in)
+    for (int k = 0; k < I.L; ++k) {
+      I.o.push_back(cells[k]);
+      I.oc.push_back(ccells[k]);
+      cells[k] += (long long)I.w[k] * I.h[k];
+      ccells[k] += (long long)I.C * I.w[k] * I.h[k];
+    }
+
+  // launch tables
+  Blob blob;
+  auto geo_at = [&](const Inst &I, int k, int tw, int th) {
+    Geo g{};
+    g.W = I.w[k]; g.H = I.h[k];
+    tiles2(tw, th, sms, g.gx, g.gy);
+    g.C = I.C; g.unit0 = I.unit0; g.part0 = I.part0;
+    g.o = I.o[k]; g.oc = I.oc[k];
+    g.s = level_s(k);
+    g.d = 4.0f * g.s + (float)I.lambda;
+    g.lambda = I.lambda;
+    return g;
+  };
+  auto second = [](Geo &g, const Inst &I, int k) {
+    g.W2 = I.w[k]; g.H2 = I.h[k]; g.o2 = I.o[k]; g.oc2 = I.oc[k];
+  };
+  {
+    std::vector<Geo> g0;
+    for (const Inst &I : m.in) g0.push_back(geo_at(I, 0, I.W, I.H));
+    m.all0 = make_launch(blob, g0);
+  }
+  m.full.resize(Lmax); m.half.resize(Lmax); m.restr.resize(Lmax); m.coarse.resize(Lmax);
+  for (int k = 0; k < Lmax; ++k) {
+    std::vector<Geo> gf, gh, gr, gk;
+    for (const Inst &I : m.in) {
+      if (k == I.L - 1) {
+        gk.push_back(geo_at(I, k, 1, 1));
+      } else if (k < I.L - 1) {
+        Geo f = geo_at(I, k, I.w[k], I.h[k]);
+        second(f, I, k + 1);
+        gf.push_back(f);
+        gh.push_back(geo_at(I, k, (I.w[k] + 1) / 2, I.h[k]));
+        Geo r = geo_at(I, k + 1, I.w[k + 1], I.h[k + 1]);  // coarse tiles, the fine level's operator
+        r.s = level_s(k);
+        r.d = 4.0f * r.s + (float)I.lambda;
+        second(r, I, k);
+        gr.push_back(r);
+      }
+    }
+    m.full[k] = make_launch(blob, gf);
+    m.half[k] = make_launch(blob, gh);
+    m.restr[k] = make_launch(blob, gr);
+    m.coarse[k] = make_launch(blob, gk);
+  }
+  {
+    std::vector<Red> rt;
+    for (const Inst &I : m.in)
+      for (int c = 0; c < I.C; ++c)
+        rt.push_back(Red{I.part0 + (long long)c * I.gx * I.gy, (long long)I.gx * I.gy});
+    m.rtab = blob.put(rt.data(), rt.size() * sizeof(Red));
+  }
+
+  // arena: tables, levels, level-0 vectors, then the staged host buffers
   size_t o = 0;
   auto take = [&](size_t b) { size_t r = o; o = aup(o + std::max<size_t>(b, 1)); return r; };
-  for (size_t k = 0; k < m.lv.size(); ++k) {
-    Level &v = m.lv[k];
-    const size_t n = (size_t)v.W * v.H;
-    v.act = take(n);
-    if (k > 0) { v.e = take(n * C * sizeof(float)); v.rhs = take(n * C * sizeof(float)); }
+  m.tab = take(blob.b.size());
+  m.io = take(m.in.size() * sizeof(Io));
+  m.lv.resize(Lmax);
+  for (int k = 0; k < Lmax; ++k) {
+    m.lv[k].act = take((size_t)cells[k]);
+    if (k > 0) {
+      m.lv[k].e = take((size_t)ccells[k] * sizeof(float));
+      m.lv[k].rhs = take((size_t)ccells[k] * sizeof(float));
+    }
   }
-  m.u = take(NC * 8); m.bl = take(NC * 8); m.uw = warm ? take(NC * 8) : 0; m.r64 = take(NC * 8);
-  m.part = take((size_t)m.nb * C * 8); m.red = take((size_t)C * 8); m.sc = take((size_t)C * S_N * 8);
-  m.scale = take((size_t)C * 8);
+  const size_t NC = (size_t)ccells[0];
+  m.u = take(NC * 8); m.bl = take(NC * 8); m.uw = any_warm ? take(NC * 8) : 0; m.r64 = take(NC * 8);
+  m.part = take((size_t)P * 8); m.red = take((size_t)U * 8); m.sc = take((size_t)U * S_N * 8);
+  m.scale = take((size_t)U * 8); m.run = take((size_t)U * 8);
   m.x = take(NC * 4); m.r = take(NC * 4); m.z = take(NC * 4); m.p = take(NC * 4); m.q = take(NC * 4);
-  if (!dev) {
-    m.in = take(NC * 2 * 4); m.mask = take(N * 4); m.guess = warm ? take(NC * 4) : 0; m.out = take(NC * 4);
+  for (Inst &I : m.in) {
+    if (I.dev) continue;
+    const size_t n = (size_t)I.W * I.H, nc = n * I.C;
+    I.in = take(nc * 2 * 4); I.mask = take(n * 4); I.guess = I.warm ? take(nc * 4) : 0; I.out = take(nc * 4);
   }
   if (!ctx->reserve(o)) return mfail(ctx, PT_OOM, "device arena allocation failed");
   m.base = static_cast<char *>(ctx->arena);
   cudaEventRecord(ctx->ev[0], m.st);
 
-  const float *guid = p.source_or_guidance, *anc = p.target_or_anchor, *msk = p.mask, *gs = p.initial_guess;
-  float *out = out_candidate;
-  if (!dev) {
-    float *in = m.at<float>(m.in);
-    ce = cudaMemcpyAsync(in, guid, NC * 4, cudaMemcpyHostToDevice, m.st);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(in + NC, anc, NC * 4, cudaMemcpyHostToDevice, m.st);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(m.at<float>(m.mask), msk, N * 4, cudaMemcpyHostToDevice, m.st);
-    if (ce == cudaSuccess && warm) ce = cudaMemcpyAsync(m.at<float>(m.guess), gs, NC * 4, cudaMemcpyHostToDevice, m.st);
-    if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("input upload: ") + cudaGetErrorString(ce));
-    guid = in; anc = in + NC; msk = m.at<float>(m.mask); gs = warm ? m.at<float>(m.guess) : nullptr;
-    out = m.at<float>(m.out);
+  // tables and inputs
+  cudaError_t ce = cudaMemcpyAsync(m.base + m.tab, blob.b.data(), blob.b.size(), cudaMemcpyHostToDevice, m.st);
+  std::vector<Io> io(m.in.size());
+  for (size_t k = 0; k < m.in.size() && ce == cudaSuccess; ++k) {
+    const Inst &I = m.in[k];
+    const pt_problem &p = ps[I.idx];
+    const size_t n = (size_t)I.W * I.H, nc = n * I.C;
+    if (I.dev) {
+      io[k] = Io{p.source_or_guidance, p.target_or_anchor, p.mask, I.warm ? p.initial_guess : nullptr, outs[I.idx]};
+      continue;
+    }
+    float *in = m.at<float>(I.in);
+    ce = cudaMemcpyAsync(in, p.source_or_guidance, nc * 4, cudaMemcpyHostToDevice, m.st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(in + nc, p.target_or_anchor, nc * 4, cudaMemcpyHostToDevice, m.st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(m.at<float>(I.mask), p.mask, n * 4, cudaMemcpyHostToDevice, m.st);
+    if (ce == cudaSuccess && I.warm)
+      ce = cudaMemcpyAsync(m.at<float>(I.guess), p.initial_guess, nc * 4, cudaMemcpyHostToDevice, m.st);
+    io[k] = Io{in, in + nc, m.at<float>(I.mask), I.warm ? m.at<float>(I.guess) : nullptr, m.at<float>(I.out)};
   }
-  const int sms = ctx->sms;
-  const unsigned gall = blocks(NC, sms);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(m.base + m.io, io.data(), io.size() * sizeof(Io), cudaMemcpyHostToDevice, m.st);
+  if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("input upload: ") + cudaGetErrorString(ce));
+
+  const Io *iod = m.at<Io>(m.io);
+  const Launch &A = m.all0;
+  const Geo *g0 = m.geo(A);
+  const int *b0 = m.bmap(A);
+  const dim3 ga = m.grid(A, m.Cmax);
+  const Red *rtab = m.at<Red>(m.tab + m.rtab);
   uint8_t *act0 = m.at<uint8_t>(m.lv[0].act);
   double *u = m.at<double>(m.u), *bl = m.at<double>(m.bl), *r64 = m.at<double>(m.r64), *part = m.at<double>(m.part),
-         *red = m.at<double>(m.red), *sc = m.at<double>(m.sc), *scale = m.at<double>(m.scale);
+         *red = m.at<double>(m.red), *sc = m.at<double>(m.sc), *scale = m.at<double>(m.scale),
+         *run = m.at<double>(m.run);
   float *x = m.at<float>(m.x), *r = m.at<float>(m.r), *z = m.at<float>(m.z), *pp = m.at<float>(m.p),
         *q = m.at<float>(m.q);
-  k_mg_assemble<<<gall, kThreads, 0, m.st>>>(W, H, C, guid, anc, msk, gs, p.lambda, act0, u, bl,
-                                             warm ? m.at<double>(m.uw) : nullptr);
+  k_mg_assemble<<<ga, kBlock2, 0, m.st>>>(g0, b0, iod, act0, u, bl, any_warm ? m.at<double>(m.uw) : nullptr);
   m.launches = 1;
-  for (size_t k = 1; k < m.lv.size(); ++k) {
-    const Level &f = m.lv[k - 1], &v = m.lv[k];
-    k_mg_coarsen<<<blocks((long long)v.W * v.H, sms), kThreads, 0, m.st>>>(f.W, f.H, m.at<uint8_t>(f.act), v.W, v.H,
-                                                                           m.at<uint8_t>(v.act));
+  for (int k = 0; k + 1 < Lmax; ++k) {
+    const Launch &R = m.restr[k];
+    if (!R.n) continue;
+    k_mg_coarsen<<<m.grid(R, 1), kBlock2, 0, m.st>>>(m.geo(R), m.bmap(R), m.at<uint8_t>(m.lv[k].act),
+                                                     m.at<uint8_t>(m.lv[k + 1].act));
     ++m.launches;
   }
   cudaEventRecord(ctx->ev[1], m.st);
 
-  // FP64 residual norms per channel of the current u -> host
-  std::vector<double> nrm(C);
+  // per-unit facts
+  std::vector<int> uinst(U), maxit(U);
+  std::vector<double> tol(U);
+  for (size_t k = 0; k < m.in.size(); ++k)
+    for (int c = 0; c < m.in[k].C; ++c) {
+      const int un = m.in[k].unit0 + c;
+      uinst[un] = (int)k;
+      tol[un] = ps[m.in[k].idx].tolerance;
+      maxit[un] = (int)ps[m.in[k].idx].max_iterations;
+    }
+
+  // FP64 residual norms per unit of the current u -> host
+  std::vector<double> nrm(U);
   auto residual = [&](const double *uu) -> cudaError_t {
-    k_mg_residual64<<<g0, kBlock2, 0, m.st>>>(W, H, act0, uu, bl, p.lambda, r64, part);
-    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, red, 1);
+    k_mg_residual64<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, uu, bl, r64, part);
+    k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, red, 1);
     m.launches += 2;
-    cudaError_t e = cudaMemcpyAsync(nrm.data(), red, C * 8, cudaMemcpyDeviceToHost, m.st);
+    cudaError_t e = cudaMemcpyAsync(nrm.data(), red, (size_t)U * 8, cudaMemcpyDeviceToHost, m.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(m.st);
     for (double &v : nrm) v = std::sqrt(v);
     return e;
   };
   ce = residual(u);
   if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("residual: ") + cudaGetErrorString(ce));
-  const std::vector<double> r0 = nrm;  // ||r(anchor)|| per channel: the bar is tolerance * r0
-  std::vector<int> warm_used(C, 0);
-  if (warm) {
+  const std::vector<double> r0 = nrm;  // ||r(anchor)|| per unit: the bar is tolerance * r0
+  std::vector<int> warm_used(U, 0);
+  if (any_warm) {
     double *uw = m.at<double>(m.uw);
     ce = residual(uw);
     if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("residual: ") + cudaGetErrorString(ce));
     // a guess is used per channel only if its residual is finite and below the anchor's
-    for (int c = 0; c < C; ++c)
-      if (std::isfinite(nrm[c]) && nrm[c] < r0[c]) {
-        warm_used[c] = 1;
-        cudaMemcpyAsync(u + (long long)c * N, uw + (long long)c * N, N * 8, cudaMemcpyDeviceToDevice, m.st);
-      }
+    for (int un = 0; un < U; ++un) {
+      const Inst &I = m.in[uinst[un]];
+      if (!I.warm || !(std::isfinite(nrm[un]) && nrm[un] < r0[un])) continue;
+      warm_used[un] = 1;
+      const size_t n = (size_t)I.W * I.H, off = (size_t)I.oc[0] + (size_t)(un - I.unit0) * n;
+      cudaMemcpyAsync(u + off, uw + off, n * 8, cudaMemcpyDeviceToDevice, m.st);
+    }
     ce = residual(u);
     if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("residual: ") + cudaGetErrorString(ce));
   }
 
-  // per-channel state
-  std::vector<int> its(C, 0), stop(C, -1), refines(C, 0);
+  // per-unit state
+  std::vector<int> its(U, 0), stop(U, -1), refines(U, 0);
   std::vector<double> cur = nrm;  // FP64 ||r|| of the current u
-  std::vector<std::vector<double>> hist(C);
-  std::vector<double> hsc(C * S_N, 0.0), hscale(C, 0.0), rr(C);
+  std::vector<std::vector<double>> hist(U);
+  std::vector<double> hscale(U, 0.0), hrun(U, 0.0), rr(U);
   bool poisoned = false;
-  for (int c = 0; c < C; ++c) {
-    if (r0[c] == 0.0) stop[c] = PT_STOP_CONVERGED;  // poisson.rs:178-185
-    else if (!std::isfinite(cur[c])) {  // (before the bar: inf <= tol * inf would pass it)
+  for (int un = 0; un < U; ++un) {
+    if (r0[un] == 0.0) stop[un] = PT_STOP_CONVERGED;  // poisson.rs:178-185
+    else if (!std::isfinite(cur[un])) {  // (before the bar: inf <= tol * inf would pass it)
       // a NaN or infinity reached the system: its residual can never improve,
       // which the reference ends by its stall rule with the region's cells
       // non-finite; here at once, with the interior set to NaN
-      stop[c] = PT_STOP_STALLED;
-      hscale[c] = std::nan("");
+      stop[un] = PT_STOP_STALLED;
+      hscale[un] = std::nan("");
       poisoned = true;
-    } else if (cur[c] <= p.tolerance * r0[c]) stop[c] = PT_STOP_CONVERGED;
-    else if (p.max_iterations == 0) stop[c] = PT_STOP_MAX_ITERATIONS;
+    } else if (cur[un] <= tol[un] * r0[un]) stop[un] = PT_STOP_CONVERGED;
+    else if (maxit[un] == 0) stop[un] = PT_STOP_MAX_ITERATIONS;
   }
-  if (poisoned) {  // u = fma(NaN, 0, u) = NaN at interior cells of those channels
-    cudaMemcpyAsync(scale, hscale.data(), C * 8, cudaMemcpyHostToDevice, m.st);
+  if (poisoned) {  // u = fma(NaN, 0, u) = NaN at interior cells of those units
+    cudaMemcpyAsync(scale, hscale.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
     cudaMemsetAsync(x, 0, NC * 4, m.st);
-    k_mg_update<<<g0, kBlock2, 0, m.st>>>(W, H, act0, x, scale, u);
+    k_mg_update<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, x, scale, u);
     ++m.launches;
     std::fill(hscale.begin(), hscale.end(), 0.0);
   }
-  const float d0 = m.lv[0].d;
   // One CG iteration: V-cycle z = M r, rho = r.z, p = z + beta p, q = A p,
   // alpha = rho / p.q, x += alpha p, r -= alpha q, ||r||^2 (to `red`). Its
-  // launches depend only on the problem's shape and the arena, so they are
+  // launches depend only on the group's shapes and the arena, so they are
   // captured once into two CUDA graphs (first iteration, later ones) cached on
-  // the context and replayed while shape and arena stay the same.
+  // the context and replayed while shapes and arena stay the same.
   long long per_iteration = 0;
+  const unsigned gsc = (unsigned)std::max(1, std::min((U + kThreads - 1) / kThreads, sms * 4));
   auto enqueue_iteration = [&](bool first) -> cudaError_t {
     const long long l0 = m.launches;
-    vcycle(m, m.r, m.z);
-    k_cg_dot<<<g0, kBlock2, 0, m.st>>>(W, H, r, z, part);
-    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_RHO_NEW, S_N);
-    k_cg_direction<<<g0, kBlock2, 0, m.st>>>(W, H, z, pp, sc, first ? 1 : 0);
-    k_cg_scalars_after_dir<<<1, 32, 0, m.st>>>(C, sc);
-    k_cg_apply<<<g0, kBlock2, 0, m.st>>>(W, H, act0, pp, d0, q, part);
-    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, sc + S_PQ, S_N);
-    k_cg_step<<<g0, kBlock2, 0, m.st>>>(W, H, pp, q, x, r, sc, part);
-    k_mg_reduce<<<C, kThreads, 0, m.st>>>(part, m.nb, red, 1);
+    vcycle(m, r, z);
+    k_cg_dot<<<ga, kBlock2, 0, m.st>>>(g0, b0, r, z, part, run);
+    k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, sc + S_RHO_NEW, S_N);
+    k_cg_direction<<<ga, kBlock2, 0, m.st>>>(g0, b0, z, pp, sc, run, first ? 1 : 0);
+    k_cg_scalars_after_dir<<<gsc, kThreads, 0, m.st>>>(U, sc);
+    k_cg_apply<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, pp, q, part, run);
+    k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, sc + S_PQ, S_N);
+    k_cg_step<<<ga, kBlock2, 0, m.st>>>(g0, b0, pp, q, x, r, sc, part, run);
+    k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, red, 1);
     m.launches += 8;
     per_iteration = m.launches - l0;
     return cudaGetLastError();
   };
   if (ctx->graphs) {
+    // the graphs' arguments are arena offsets and the tables' contents
     std::string key(reinterpret_cast<const char *>(&m.base), sizeof(m.base));
-    const double shape[6] = {(double)W, (double)H, (double)C, p.lambda, (double)m.nb, (double)o};
-    key.append(reinterpret_cast<const char *>(shape), sizeof(shape));
+    std::vector<size_t> offs = {o, m.tab, m.rtab, m.part, m.red, m.sc, m.run, m.x, m.r, m.z, m.p, m.q,
+                                (size_t)m.Cmax, (size_t)U};
+    for (const LevelArr &v : m.lv) offs.insert(offs.end(), {v.act, v.e, v.rhs});
+    key.append(reinterpret_cast<const char *>(offs.data()), offs.size() * sizeof(size_t));
+    key.append(reinterpret_cast<const char *>(blob.b.data()), blob.b.size());
     if (key != ctx->mgkey || !ctx->mgexec[0] || !ctx->mgexec[1]) {
       for (auto &ge : ctx->mgexec)
         if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
@@ -718,30 +1024,31 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
           if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
         return mfail(ctx, PT_LAUNCH_FAILED, std::string("graph capture: ") + cudaGetErrorString(ce));
       }
-      ctx->mgkey = key;
+      ctx->mgkey = std::move(key);
     }
   }
   int outer = 0;
   while (std::any_of(stop.begin(), stop.end(), [](int s) { return s < 0; })) {
-    // scale this outer step's residual to unit norm; channels that stopped get 0
-    for (int c = 0; c < C; ++c) {
-      hscale[c] = stop[c] < 0 ? cur[c] : 0.0;
-      hsc[c * S_N + S_RUN] = stop[c] < 0 ? 1.0 : 0.0;
+    // scale this outer step's residual to unit norm; units that stopped get 0
+    for (int un = 0; un < U; ++un) {
+      hscale[un] = stop[un] < 0 ? cur[un] : 0.0;
+      hrun[un] = stop[un] < 0 ? 1.0 : 0.0;
     }
-    cudaMemcpyAsync(scale, hscale.data(), C * 8, cudaMemcpyHostToDevice, m.st);
-    cudaMemcpyAsync(sc, hsc.data(), C * S_N * 8, cudaMemcpyHostToDevice, m.st);
-    k_mg_scale<<<g0, kBlock2, 0, m.st>>>(W, H, r64, scale, r);
+    cudaMemcpyAsync(scale, hscale.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
+    cudaMemcpyAsync(run, hrun.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
+    cudaMemsetAsync(sc, 0, (size_t)U * S_N * 8, m.st);
+    k_mg_scale<<<ga, kBlock2, 0, m.st>>>(g0, b0, r64, scale, r);
     cudaMemsetAsync(x, 0, NC * 4, m.st);
     m.launches += 1;
     // inner target: a quarter of the remaining bar, at most as deep as FP32
     // goes from a unit residual; a run whose residual stops falling (less than
     // 30% over 4 iterations: the FP32 floor) hands over to the next outer step
-    std::vector<double> target(C), rel(C, 1.0);
-    std::vector<std::vector<double>> seen(C);
-    std::vector<int> run(C);
-    for (int c = 0; c < C; ++c) {
-      run[c] = stop[c] < 0;
-      target[c] = run[c] ? std::max(0.25 * p.tolerance * r0[c] / cur[c], kInnerFloor) : 1.0;
+    std::vector<double> target(U), rel(U, 1.0);
+    std::vector<std::vector<double>> seen(U);
+    std::vector<int> going(U);
+    for (int un = 0; un < U; ++un) {
+      going[un] = stop[un] < 0;
+      target[un] = going[un] ? std::max(0.25 * tol[un] * r0[un] / cur[un], kInnerFloor) : 1.0;
     }
     for (int it = 0;; ++it) {
       const int g = it == 0 ? 0 : 1;
@@ -752,56 +1059,65 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
         ce = enqueue_iteration(it == 0);
       }
       if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("cg: ") + cudaGetErrorString(ce));
-      ce = cudaMemcpyAsync(rr.data(), red, C * 8, cudaMemcpyDeviceToHost, m.st);
+      ce = cudaMemcpyAsync(rr.data(), red, (size_t)U * 8, cudaMemcpyDeviceToHost, m.st);
       if (ce == cudaSuccess) ce = cudaStreamSynchronize(m.st);
       if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("cg: ") + cudaGetErrorString(ce));
-      bool any = false;
-      for (int c = 0; c < C; ++c) {
-        if (!run[c]) continue;
-        its[c] += 1;
-        rel[c] = std::sqrt(rr[c]);  // relative to this outer step's unit residual
-        hist[c].push_back(rel[c] * cur[c] / r0[c]);
-        seen[c].push_back(rel[c]);
-        const size_t n = seen[c].size();
-        const bool stuck = n > 4 && seen[c][n - 1] > 0.7 * seen[c][n - 5];
-        if (rel[c] <= target[c] || stuck || its[c] >= (int)p.max_iterations || !std::isfinite(rel[c])) {
-          run[c] = 0;
-          hsc[c * S_N + S_RUN] = 0.0;
-          cudaMemcpyAsync(sc + c * S_N + S_RUN, &hsc[c * S_N + S_RUN], 8, cudaMemcpyHostToDevice, m.st);
+      bool any = false, changed = false;
+      for (int un = 0; un < U; ++un) {
+        if (!going[un]) continue;
+        its[un] += 1;
+        rel[un] = std::sqrt(rr[un]);  // relative to this outer step's unit residual
+        hist[un].push_back(rel[un] * cur[un] / r0[un]);
+        seen[un].push_back(rel[un]);
+        const size_t n = seen[un].size();
+        const bool stuck = n > 4 && seen[un][n - 1] > 0.7 * seen[un][n - 5];
+        if (rel[un] <= target[un] || stuck || its[un] >= maxit[un] || !std::isfinite(rel[un])) {
+          going[un] = 0;
+          hrun[un] = 0.0;
+          changed = true;
         }
-        any |= run[c] != 0;
+        any |= going[un] != 0;
       }
       if (!any) break;
+      if (changed) cudaMemcpyAsync(run, hrun.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
     }
     // u += scale * x, then the FP64 residual decides
-    k_mg_update<<<g0, kBlock2, 0, m.st>>>(W, H, act0, x, scale, u);
+    k_mg_update<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, x, scale, u);
     ++m.launches;
     const std::vector<double> prev = cur;
     ce = residual(u);
     if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("residual: ") + cudaGetErrorString(ce));
-    for (int c = 0; c < C; ++c) {
-      if (stop[c] >= 0) continue;
-      cur[c] = nrm[c];
-      if (!hist[c].empty()) hist[c].back() = cur[c] / r0[c];
-      if (outer > 0) refines[c] += 1;
-      if (cur[c] <= p.tolerance * r0[c]) stop[c] = PT_STOP_CONVERGED;
-      else if (its[c] >= (int)p.max_iterations) stop[c] = PT_STOP_MAX_ITERATIONS;
-      else if (!(cur[c] < prev[c] * (1.0 - 1e-12))) stop[c] = PT_STOP_STALLED;
+    for (int un = 0; un < U; ++un) {
+      if (stop[un] >= 0) continue;
+      cur[un] = nrm[un];
+      if (!hist[un].empty()) hist[un].back() = cur[un] / r0[un];
+      if (outer > 0) refines[un] += 1;
+      if (cur[un] <= tol[un] * r0[un]) stop[un] = PT_STOP_CONVERGED;
+      else if (its[un] >= maxit[un]) stop[un] = PT_STOP_MAX_ITERATIONS;
+      else if (!(cur[un] < prev[un] * (1.0 - 1e-12))) stop[un] = PT_STOP_STALLED;
     }
     ++outer;
   }
   cudaEventRecord(ctx->ev[2], m.st);
-  k_mg_emit<<<gall, kThreads, 0, m.st>>>(W, H, C, act0, u, anc, out);
+  k_mg_emit<<<ga, kBlock2, 0, m.st>>>(g0, b0, iod, act0, u);
   ++m.launches;
-  if (!dev) ce = cudaMemcpyAsync(out_candidate, out, NC * 4, cudaMemcpyDeviceToHost, m.st);
-  if (ce == cudaSuccess && history)
-    for (int c = 0; c < C; ++c) {
-      const size_t n = std::min<size_t>(hist[c].size(), p.max_iterations);
+  ce = cudaSuccess;
+  for (size_t k = 0; k < m.in.size() && ce == cudaSuccess; ++k) {
+    const Inst &I = m.in[k];
+    if (!I.dev)
+      ce = cudaMemcpyAsync(outs[I.idx], m.at<float>(I.out), (size_t)I.W * I.H * I.C * 4, cudaMemcpyDeviceToHost,
+                           m.st);
+    double *hp = histories ? histories[I.idx] : nullptr;
+    if (!hp) continue;
+    const uint32_t cap = ps[I.idx].max_iterations;
+    for (int c = 0; c < I.C && ce == cudaSuccess; ++c) {
+      const std::vector<double> &h = hist[I.unit0 + c];
+      const size_t n = std::min<size_t>(h.size(), cap);
       if (!n) continue;
-      ce = cudaMemcpyAsync(history + (size_t)c * p.max_iterations, hist[c].data(), n * 8,
-                           dev ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost, m.st);
-      if (ce != cudaSuccess) break;
+      ce = cudaMemcpyAsync(hp + (size_t)c * cap, h.data(), n * 8,
+                           I.dev ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost, m.st);
     }
+  }
   if (ce == cudaSuccess) ce = cudaEventRecord(ctx->ev[3], m.st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(m.st);
   if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("result download: ") + cudaGetErrorString(ce));
@@ -810,34 +1126,92 @@ pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, p
     if (cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]) != cudaSuccess) a = -1.f;
     if (cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]) != cudaSuccess) b = -1.f;
     cudaGetLastError();
-    ctx->last_solve_ms = a;
-    ctx->last_call_ms = b;
-    ctx->last_launches = m.launches;
+    solve_ms += a;
+    call_ms += b;
+    launches += m.launches;
   }
-  int worst = -1;
-  for (int c = 0; c < C; ++c) {
-    pt_report rep{};
-    rep.iterations = (uint32_t)its[c];
-    rep.stop_reason = stop[c];
-    rep.converged = stop[c] == PT_STOP_CONVERGED;
-    rep.tolerance = p.tolerance;
-    rep.final_residual = r0[c] == 0.0 ? cur[c] : cur[c] / r0[c];
-    rep.history_len = (uint32_t)std::min<size_t>(hist[c].size(), p.max_iterations);
-    rep.omega_used = kSmoothOmega;
-    rep.refinements = (uint32_t)refines[c];
-    rep.channel = c;
-    rep.initial_residual = r0[c];
-    rep.warm_start = warm_used[c];
-    reports[c] = rep;
-    // worse_of (poisson_blend.rs:240-246)
-    if (worst < 0) worst = c;
-    else {
-      const pt_report &a = reports[worst];
-      const bool b_worse = (rep.iterations != a.iterations) ? (rep.iterations > a.iterations)
-                                                            : (rep.final_residual > a.final_residual);
-      if (b_worse) worst = c;
+  for (const Inst &I : m.in) {
+    pt_report *reps = reports[I.idx];
+    const pt_problem &p = ps[I.idx];
+    int worst = -1;
+    for (int c = 0; c < I.C; ++c) {
+      const int un = I.unit0 + c;
+      pt_report rep{};
+      rep.iterations = (uint32_t)its[un];
+      rep.stop_reason = stop[un];
+      rep.converged = stop[un] == PT_STOP_CONVERGED;
+      rep.tolerance = p.tolerance;
+      rep.final_residual = r0[un] == 0.0 ? cur[un] : cur[un] / r0[un];
+      rep.history_len = (uint32_t)std::min<size_t>(hist[un].size(), p.max_iterations);
+      rep.omega_used = kSmoothOmega;
+      rep.refinements = (uint32_t)refines[un];
+      rep.channel = c;
+      rep.initial_residual = r0[un];
+      rep.warm_start = warm_used[un];
+      reps[c] = rep;
+      // worse_of (poisson_blend.rs:240-246)
+      if (worst < 0) worst = c;
+      else {
+        const pt_report &a = reps[worst];
+        const bool b_worse = (rep.iterations != a.iterations) ? (rep.iterations > a.iterations)
+                                                              : (rep.final_residual > a.final_residual);
+        if (b_worse) worst = c;
+      }
     }
+    reps[I.C] = reps[worst];
   }
-  reports[C] = reports[worst];
+  return PT_OK;
+}
+
+}  // namespace
+
+// Problems with PT_FLAG_MULTIGRID (pt_poisson_solve, pt_poisson_solve_batch):
+// all of a call's instances share each launch, in groups of at most
+// kGroupTiles level-0 tiles.
+pt_status ptk_solve_mg_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
+                             pt_report *const *reports, double *const *histories) {
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return mfail(ctx, PT_NO_DEVICE, cudaGetErrorString(ce));
+  for (auto &e : ctx->ev)
+    if (!e && cudaEventCreate(&e) != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, "event create");
+  double solve_ms = 0.0, call_ms = 0.0;
+  long long launches = 0, tiles = 0, units = 0;
+  bool ran = false;
+  std::vector<int> ids;
+  auto flush = [&]() -> pt_status {
+    if (ids.empty()) return PT_OK;
+    const pt_status s = solve_group(ctx, ps, ids, outs, reports, histories, solve_ms, call_ms, launches);
+    ids.clear();
+    tiles = units = 0;
+    ran = true;
+    return s;
+  };
+  for (uint32_t i = 0; i < n; ++i) {
+    const pt_problem &p = ps[i];
+    if (p.channels == 0) {
+      pt_report r{};
+      r.converged = 1; r.stop_reason = PT_STOP_CONVERGED; r.tolerance = p.tolerance; r.channel = -1;
+      reports[i][0] = r;
+      continue;
+    }
+    int gx, gy;
+    tiles2((int)p.width, (int)p.height, ctx->sms, gx, gy);
+    const long long t = (long long)gx * gy;
+    if (!ids.empty() && (tiles + t > kGroupTiles || units + p.channels > kGroupTiles)) {
+      const pt_status s = flush();
+      if (s != PT_OK) return s;
+    }
+    ids.push_back((int)i);
+    tiles += t;
+    units += p.channels;
+  }
+  const pt_status s = flush();
+  if (s != PT_OK) return s;
+  if (ran) {
+    ctx->last_solve_ms = solve_ms;
+    ctx->last_call_ms = call_ms;
+    ctx->last_launches = launches;
+  }
   return PT_OK;
 }

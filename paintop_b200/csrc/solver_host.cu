@@ -137,7 +137,8 @@ Layout layout(const Plan &pl, bool stage) {
 // ---------------------------------------------------------------------------
 int ptk_choose_config(pt_ctx *ctx, const pt_problem *ps, uint32_t n);
 
-pt_status ptk_solve_mg(pt_ctx *ctx, const pt_problem &p, float *out_candidate, pt_report *reports, double *history);
+pt_status ptk_solve_mg_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
+                             pt_report *const *reports, double *const *histories);
 
 pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
                           pt_report *const *reports, double *const *histories, int force_cfg) {
@@ -158,15 +159,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   for (uint32_t i = 0; i < n; ++i)
     if (((ps[i].flags & PT_FLAG_MULTIGRID) != 0) != mg)
       return fail(ctx, PT_INVALID_ARG, "PT_FLAG_MULTIGRID must agree across a batch");
-  if (mg) {
-    // multigrid-preconditioned CG, one problem at a time (each is already a
-    // sequence of whole-grid launches)
-    for (uint32_t i = 0; i < n; ++i) {
-      const pt_status s = ptk_solve_mg(ctx, ps[i], outs[i], reports[i], histories ? histories[i] : nullptr);
-      if (s != PT_OK) return s;
-    }
-    return PT_OK;
-  }
+  if (mg) return ptk_solve_mg_batch(ctx, ps, n, outs, reports, histories);  // every instance in each launch
   const bool devptr = n > 0 && (ps[0].flags & PT_FLAG_DEVICE_POINTERS);
   for (uint32_t i = 0; i < n; ++i)
     if (((ps[i].flags & PT_FLAG_DEVICE_POINTERS) != 0) != devptr)

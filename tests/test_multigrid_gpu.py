@@ -174,3 +174,58 @@ def test_multigrid_non_finite_residual_stalls(ctx, L, case):
     inter = mask.reshape(h, w) > 0.5
     assert not np.isfinite(out.reshape(h, w)[inter]).any()
     assert np.array_equal(out.reshape(h, w)[~inter].view(np.uint32), tgt.reshape(h, w)[~inter].view(np.uint32))
+
+
+def test_multigrid_mixed_batch_equals_solving_alone(ctx, oracle, L):
+    """A batch of unlike problems shares every launch -- one to three channels,
+    lambda, tolerance and iteration cap per problem, an image no larger than
+    the coarsest level (8 x 8), no interior (2 x 40), no channels, a warm start
+    and a NaN -- and each problem's output, reports and residual history are
+    bit for bit those of solving it alone."""
+    specs = [  # seed, w, h, c, lambda, tolerance, cap, kind
+        (31, 150, 90, 3, 0.0, 1e-8, 300, None),
+        (32, 8, 8, 1, 0.0, 1e-9, 300, None),
+        (33, 2, 40, 2, 0.0, 1e-6, 300, None),
+        (34, 257, 129, 2, 0.05, 1e-7, 300, None),
+        (35, 60, 30, 1, 0.0, 1e-12, 3, None),
+        (36, 40, 50, 0, 0.0, 1e-6, 300, None),
+        (37, 120, 100, 2, 0.1, 1e-9, 300, "warm"),
+        (38, 16, 16, 1, 0.0, 1e-6, 300, "nan"),
+        (39, 33, 500, 3, 0.01, 1e-6, 300, None),
+    ]
+    probs = []
+    for seed, w, h, c, lam, tol, cap, kind in specs:
+        if c == 0:
+            s = t = np.zeros(0, np.float32)
+            m = np.ones(w * h, np.float32)
+        else:
+            s, t, m = random_problem(seed, w, h, c)
+        pr = dict(source=s, target=t, mask=m, width=w, height=h, channels=c, lam=lam, max_iterations=cap,
+                  tolerance=tol, flags=L.PT_FLAG_MULTIGRID)
+        if kind == "warm":
+            cg, _ = oracle.cg_blend_channels(s, t, m, c, w, h, lam=lam, rel_tol=1e-13)
+            pr["initial_guess"] = cg.astype(np.float32)
+        if kind == "nan":
+            s[8 * w + 8] = np.nan
+        probs.append(pr)
+    res = ctx.solve_batch(probs, want_history=True)
+    for pr, (out, per, worst), spec in zip(probs, res, specs):
+        c = pr["channels"]
+        if c == 0:
+            assert worst["converged"] and worst["iterations"] == 0
+            continue
+        one, per1, worst1 = ctx.solve(pr["source"], pr["target"], pr["mask"], pr["width"], pr["height"], c,
+                                      lam=pr["lam"], max_iterations=pr["max_iterations"], tolerance=pr["tolerance"],
+                                      flags=pr["flags"], initial_guess=pr.get("initial_guess"))
+        assert np.array_equal(np.asarray(out).view(np.uint32), one.view(np.uint32)), spec
+        for a, b in zip(per, per1):
+            for key in ("iterations", "stop_reason", "converged", "refinements", "warm_start"):
+                assert a[key] == b[key], (spec, key)
+            assert np.array_equal(np.float64(a["final_residual"]), np.float64(b["final_residual"]), equal_nan=True)
+            assert np.array_equal(np.asarray(a["residual_history"]), np.asarray(b["residual_history"]),
+                                  equal_nan=True), spec
+    by_kind = {sp[7]: r for sp, r in zip(specs, res)}
+    assert all(r["warm_start"] == 1 and r["converged"] for r in by_kind["warm"][1])
+    assert by_kind["nan"][2]["stop_reason"] == "stalled"
+    assert res[4][2]["stop_reason"] == "max-iterations" and res[4][2]["iterations"] == 3
+    assert all(r["converged"] for k in (0, 1, 2, 3, 8) for r in res[k][1])
