@@ -121,12 +121,13 @@ struct Io {
 // ---- assembly ----------------------------------------------------------------
 // interior flag, u = anchor (or the warm guess at interior cells), b' =
 // fma(lambda, -anchor, laplacian(guidance)) at interior cells; level-0 tiles.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                            const Io *__restrict__ io, uint8_t *__restrict__ act,
                                                            double *__restrict__ u, double *__restrict__ bl,
                                                            double *__restrict__ uw) {
-  const int gi = bmap[blockIdx.x];
-  const Geo &g = geo[gi];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const int gi = bt.x;
+  const Geo g = geo[gi];
   const int c = blockIdx.z, C = g.C;
   if (c >= C) return;
   const Io f = io[gi];
@@ -156,15 +157,16 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict
 
 // r = fma(lambda + 4, -u, nsum) - b' at interior cells (0 elsewhere) and
 // per-tile partial sums of r^2.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                              const uint8_t *__restrict__ act,
                                                              const double *__restrict__ u,
                                                              const double *__restrict__ bl, double *__restrict__ r64,
                                                              double *__restrict__ part) {
   __shared__ double sh[kTx * kTy];
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C) return;
+  if (c >= bt.z) return;
   const int W = g.W, H = g.H, gx = g.gx, gy = g.gy, b = tile_b(g), i = (b % gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
   const uint8_t *a = act + g.o;
@@ -203,12 +205,13 @@ __global__ void k_mg_reduce(const double *__restrict__ part, const Red *__restri
 }
 
 // r32 = r64 / scale[unit] (0 where the unit is not being corrected)
-__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                         const double *__restrict__ r64,
                                                         const double *__restrict__ scale, float *__restrict__ r32) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C) return;
+  if (c >= bt.z) return;
   const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
   const double s = scale[g.unit0 + c];
@@ -222,12 +225,13 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ 
 
 // u += scale[unit] * x at interior cells; a unit with scale 0 (not being
 // corrected) is left as it is, bit for bit
-__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                          const uint8_t *__restrict__ act, const float *__restrict__ x,
                                                          const double *__restrict__ scale, double *__restrict__ u) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C) return;
+  if (c >= bt.z) return;
   const double s = scale[g.unit0 + c];
   if (s == 0.0) return;
   const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
@@ -257,9 +261,10 @@ constexpr float kSmoothOmega = 1.25f;
 
 // Coarse interior flags from the fine ones; tiles of the coarse plane (the
 // fine plane is the entry's second).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                           const uint8_t *__restrict__ af, uint8_t *__restrict__ ac) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int Wc = g.W, Hc = g.H, Wf = g.W2, Hf = g.H2, b = tile_b(g), I = (b % g.gx) * kTx + threadIdx.x;
   const uint8_t *f = af + g.o2;
   uint8_t *cc = ac + g.o;
@@ -277,13 +282,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict_
 // One colour of red-black Gauss-Seidel on A_k e = rhs: e = (rhs + s * sum of
 // neighbours) / d at active cells of that colour (inactive cells hold 0).
 // x threads index the cells of one colour in a row (half-sweep tiles).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                          const uint8_t *__restrict__ act,
                                                          const float *__restrict__ rhs, float *__restrict__ e,
                                                          const double *__restrict__ run, int color) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  if (c >= bt.z || run[bt.y + c] == 0.0) return;
   const int W = g.W, H = g.H, b = tile_b(g), m = (b % g.gx) * kTx + threadIdx.x;
   const float s = g.s, d = g.d;
   const size_t N = (size_t)W * H;
@@ -310,13 +316,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__
 // zeroing e and one red half-sweep produce, bit for bit, in one pass that
 // writes every cell.
 __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth_first(const Geo *__restrict__ geo,
-                                                               const int *__restrict__ bmap,
+                                                               const int4 *__restrict__ bmap,
                                                                const uint8_t *__restrict__ act,
                                                                const float *__restrict__ rhs, float *__restrict__ e,
                                                                const double *__restrict__ run) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  if (c >= bt.z || run[bt.y + c] == 0.0) return;
   const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const float s = g.s, d = g.d;
   const size_t N = (size_t)W * H;
@@ -382,16 +389,17 @@ __device__ __forceinline__ float pw(int a) { return (a == 0 || a == 1) ? 0.75f :
 // active fine cells (0 elsewhere), evaluated on the fly so the residual is
 // never stored. Tiles of the coarse plane; the fine plane is the second.
 __global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(const Geo *__restrict__ geo,
-                                                                 const int *__restrict__ bmap,
+                                                                 const int4 *__restrict__ bmap,
                                                                  const uint8_t *__restrict__ af,
                                                                  const float *__restrict__ rhsf,
                                                                  const float *__restrict__ ef,
                                                                  const uint8_t *__restrict__ ac,
                                                                  float *__restrict__ rhsc,
                                                                  const double *__restrict__ run) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  if (c >= bt.z || run[bt.y + c] == 0.0) return;
   const int Wc = g.W, Hc = g.H, Wf = g.W2, Hf = g.H2, b = tile_b(g), I = (b % g.gx) * kTx + threadIdx.x;
   const float s = g.s, d = g.d;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
@@ -431,13 +439,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(const Geo *__re
 
 // e_f += bilinear prolongation of e_c at active fine cells; tiles of the fine
 // plane, the coarse plane is the second.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                           const uint8_t *__restrict__ af, float *__restrict__ ef,
                                                           const float *__restrict__ ec,
                                                           const double *__restrict__ run) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  if (c >= bt.z || run[bt.y + c] == 0.0) return;
   const int Wf = g.W, Hf = g.H, Wc = g.W2, Hc = g.H2, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
   const float *e = ec + g.oc2 + c * Nc;
@@ -462,15 +471,16 @@ __device__ __forceinline__ void zero_partial(const Geo &g, int c, double *part) 
 }
 
 // q = A_0 p at active cells; partial sums of p.q
-__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                         const uint8_t *__restrict__ act, const float *__restrict__ p,
                                                         float *__restrict__ q, double *__restrict__ part,
                                                         const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C) return;
-  if (run[g.unit0 + c] == 0.0) {  // a stopped unit: its p.q is never read
+  if (c >= bt.z) return;
+  if (run[bt.y + c] == 0.0) {  // a stopped unit: its p.q is never read
     zero_partial(g, c, part);
     return;
   }
@@ -496,14 +506,15 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ 
 }
 
 // partial sums of a.b
-__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                       const float *__restrict__ x, const float *__restrict__ y,
                                                       double *__restrict__ part, const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C) return;
-  if (run[g.unit0 + c] == 0.0) {  // a stopped unit: its rho is never read
+  if (c >= bt.z) return;
+  if (run[bt.y + c] == 0.0) {  // a stopped unit: its rho is never read
     zero_partial(g, c, part);
     return;
   }
@@ -520,13 +531,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ ge
 }
 
 // p = z + beta p (beta = rho_new / rho; p = z on the first iteration)
-__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                             const float *__restrict__ z, float *__restrict__ p,
                                                             const double *__restrict__ sc,
                                                             const double *__restrict__ run, int first) {
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  if (c >= bt.z || run[bt.y + c] == 0.0) return;
   const double *s = sc + (long long)(g.unit0 + c) * S_N;
   const float beta = first ? 0.0f : (float)(s[S_RHO] != 0.0 ? s[S_RHO_NEW] / s[S_RHO] : 0.0);
   const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
@@ -545,16 +557,17 @@ __global__ void k_cg_scalars_after_dir(int U, double *__restrict__ sc) {
 }
 
 // x += alpha p, r -= alpha q (alpha = rho / p.q); partial sums of r.r
-__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                        const float *__restrict__ p, const float *__restrict__ q,
                                                        float *__restrict__ x, float *__restrict__ r,
                                                        const double *__restrict__ sc, double *__restrict__ part,
                                                        const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const Geo &g = geo[bmap[blockIdx.x]];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const Geo g = geo[bt.x];
   const int c = blockIdx.z;
-  if (c >= g.C) return;
-  if (run[g.unit0 + c] == 0.0) {  // a stopped unit: x and r stay (p may never have been written)
+  if (c >= bt.z) return;
+  if (run[bt.y + c] == 0.0) {  // a stopped unit: x and r stay (p may never have been written)
     zero_partial(g, c, part);
     return;
   }
@@ -577,11 +590,12 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ g
 }
 
 // out = interleave(u) at interior cells, the anchor elsewhere (bit for bit)
-__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
                                                        const Io *__restrict__ io, const uint8_t *__restrict__ act,
                                                        const double *__restrict__ u) {
-  const int gi = bmap[blockIdx.x];
-  const Geo &g = geo[gi];
+  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const int gi = bt.x;
+  const Geo g = geo[gi];
   const int c = blockIdx.z, C = g.C;
   if (c >= C) return;
   const Io f = io[gi];
@@ -599,12 +613,17 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ g
 size_t aup(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // (32, 8)-thread tiles over w columns and h rows of one instance: at most
-// about 8 tiles per SM per channel (rows are strided), at most 65535 rows of
-// tiles.
+// about 8 tiles per SM per channel, at least kMinBands bands of 8 rows per
+// tile where the instance has them (a tile's first loads -- its table entry,
+// geometry and run flag -- then serve several bands), at most 65535 rows of
+// tiles. The choice depends on the instance alone, so its partial sums are
+// the same in any batch.
+constexpr int kMinBands = 4;
 void tiles2(int w, int h, int sms, int &gx, int &gy) {
   gx = std::max(1, (w + kTx - 1) / kTx);
-  gy = std::max(1, (h + kTy - 1) / kTy);
-  gy = std::min(gy, std::max(1, sms * 8 / gx));
+  const int bands = std::max(1, (h + kTy - 1) / kTy);
+  gy = std::min(bands, std::max(1, sms * 8 / gx));
+  gy = std::min(gy, (bands + kMinBands - 1) / kMinBands);
   gy = std::min(gy, 65535);
 }
 const dim3 kBlock2(kTx, kTy);
@@ -654,17 +673,17 @@ struct Blob {
 Launch make_launch(Blob &blob, std::vector<Geo> &gs) {
   Launch l;
   l.n = (int)gs.size();
-  std::vector<int> bm;
+  std::vector<int4> bm;
   long long blk = 0;
   for (size_t k = 0; k < gs.size(); ++k) {
     gs[k].blk0 = (int)blk;
     const long long nb = (long long)gs[k].gx * gs[k].gy;
-    bm.insert(bm.end(), (size_t)nb, (int)k);
+    bm.insert(bm.end(), (size_t)nb, make_int4((int)k, gs[k].unit0, gs[k].C, 0));
     blk += nb;
   }
   l.blocks = blk;
   l.geo = blob.put(gs.data(), gs.size() * sizeof(Geo));
-  l.bmap = blob.put(bm.data(), bm.size() * sizeof(int));
+  l.bmap = blob.put(bm.data(), bm.size() * sizeof(int4));
   return l;
 }
 
@@ -684,7 +703,7 @@ struct Mg {
   long long launches = 0;
   template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
   const Geo *geo(const Launch &l) { return at<Geo>(tab + l.geo); }
-  const int *bmap(const Launch &l) { return at<int>(tab + l.bmap); }
+  const int4 *bmap(const Launch &l) { return at<int4>(tab + l.bmap); }
   dim3 grid(const Launch &l, unsigned z) { return dim3((unsigned)l.blocks, 1, z); }
 };
 
@@ -884,7 +903,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
   const Io *iod = m.at<Io>(m.io);
   const Launch &A = m.all0;
   const Geo *g0 = m.geo(A);
-  const int *b0 = m.bmap(A);
+  const int4 *b0 = m.bmap(A);
   const dim3 ga = m.grid(A, m.Cmax);
   const Red *rtab = m.at<Red>(m.tab + m.rtab);
   uint8_t *act0 = m.at<uint8_t>(m.lv[0].act);
