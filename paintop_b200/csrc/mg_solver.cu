@@ -296,18 +296,42 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__
   const uint8_t *a = act + g.o;
   float *ec = e + g.oc + c * N;
   const float *rc = rhs + g.oc + c * N;
-  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H; j += g.gy * kTy) {
-    const int i = 2 * m + ((j + color) & 1);
-    if (i >= W) continue;
-    const size_t q = (size_t)j * W + i;
-    if (!a[q]) continue;
-    float nb = 0.0f;
-    if (i > 0) nb += ec[q - 1];
-    if (i < W - 1) nb += ec[q + 1];
-    if (j > 0) nb += ec[q - W];
-    if (j < H - 1) nb += ec[q + W];
-    const float gs = (rc[q] + s * nb) / d;
-    ec[q] = ec[q] + kSmoothOmega * (gs - ec[q]);
+  // Two of the tile's rows per pass, both rows' loads before either update:
+  // the neighbours read are of the other colour, which this half-sweep does
+  // not write, so the two rows' accesses are independent and the loads of the
+  // second row need not wait for the first row's store.
+  const int step = g.gy * kTy;
+  for (int j0 = (b / g.gx) * kTy + threadIdx.y; j0 < H; j0 += 2 * step) {
+    const int j1 = j0 + step;
+    const int i0 = 2 * m + ((j0 + color) & 1), i1 = 2 * m + ((j1 + color) & 1);
+    const size_t q0 = (size_t)j0 * W + i0, q1 = (size_t)j1 * W + i1;
+    const bool v0 = i0 < W && a[q0];
+    const bool v1 = j1 < H && i1 < W && a[q1];
+    float nb0 = 0.0f, e0 = 0.0f, r0 = 0.0f, nb1 = 0.0f, e1 = 0.0f, r1 = 0.0f;
+    if (v0) {
+      if (i0 > 0) nb0 += ec[q0 - 1];
+      if (i0 < W - 1) nb0 += ec[q0 + 1];
+      if (j0 > 0) nb0 += ec[q0 - W];
+      if (j0 < H - 1) nb0 += ec[q0 + W];
+      e0 = ec[q0];
+      r0 = rc[q0];
+    }
+    if (v1) {
+      if (i1 > 0) nb1 += ec[q1 - 1];
+      if (i1 < W - 1) nb1 += ec[q1 + 1];
+      if (j1 > 0) nb1 += ec[q1 - W];
+      if (j1 < H - 1) nb1 += ec[q1 + W];
+      e1 = ec[q1];
+      r1 = rc[q1];
+    }
+    if (v0) {
+      const float gs = (r0 + s * nb0) / d;
+      ec[q0] = e0 + kSmoothOmega * (gs - e0);
+    }
+    if (v1) {
+      const float gs = (r1 + s * nb1) / d;
+      ec[q1] = e1 + kSmoothOmega * (gs - e1);
+    }
   }
 }
 
