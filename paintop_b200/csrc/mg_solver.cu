@@ -26,11 +26,13 @@
 // Batches: every problem of a call (pt_poisson_solve_batch) keeps its own
 // level hierarchy, its own CG scalars per channel and its own stopping, but
 // all of them share each launch. A launch walks a table of blocks, each block
-// one 32 x 8 tile of one instance's plane, laid out per instance exactly as a
-// call with that instance alone lays it out, so partial sums, their
-// reduction order and hence every result of an instance are bit for bit what
-// it gets when solved alone. An (instance, channel) pair whose run has
-// stopped skips the V-cycle and the vector kernels.
+// one 32 x 8 tile of one instance's plane. The level-0 tiles, whose partial
+// sums are reduced, are laid out per instance exactly as a call with that
+// instance alone lays them out; every other kernel computes each cell from
+// values no other block of the launch writes, so its result does not depend
+// on the tiling. An instance's results are therefore bit for bit what it gets
+// when solved alone. An (instance, channel) pair whose run has stopped skips
+// the vector kernels and, in a call with several instances, the V-cycle.
 //
 // Report (pt_report): iterations = preconditioned CG iterations (each one
 // V-cycle and one operator application); history[k] = relative residual after
@@ -92,7 +94,14 @@ struct Geo {
   double lambda;
 };
 
-// Where a block of a tiled launch works: its entry, tile column and row
+// The block's entry, the entry's first unit and its channels: from the block
+// table, or -- a launch over one instance, bmap null -- from the kernel's own
+// parameter `one`, with no load before the block's first data.
+__device__ __forceinline__ int4 entry_of(const int4 *__restrict__ bmap, const Geo &one) {
+  return bmap ? bmap[blockIdx.x] : make_int4(0, one.unit0, one.C, 0);
+}
+
+// Which tile of its instance a block works on
 __device__ __forceinline__ int tile_b(const Geo &g) { return (int)blockIdx.x - g.blk0; }
 
 __device__ __forceinline__ double block_sum2(double v, double *sh) {
@@ -121,13 +130,13 @@ struct Io {
 // ---- assembly ----------------------------------------------------------------
 // interior flag, u = anchor (or the warm guess at interior cells), b' =
 // fma(lambda, -anchor, laplacian(guidance)) at interior cells; level-0 tiles.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                            const Io *__restrict__ io, uint8_t *__restrict__ act,
                                                            double *__restrict__ u, double *__restrict__ bl,
                                                            double *__restrict__ uw) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const int4 bt = entry_of(bmap, one);
   const int gi = bt.x;
-  const Geo g = geo[gi];
+  const Geo g = bmap ? geo[gi] : one;
   const int c = blockIdx.z, C = g.C;
   if (c >= C) return;
   const Io f = io[gi];
@@ -157,14 +166,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict
 
 // r = fma(lambda + 4, -u, nsum) - b' at interior cells (0 elsewhere) and
 // per-tile partial sums of r^2.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                              const uint8_t *__restrict__ act,
                                                              const double *__restrict__ u,
                                                              const double *__restrict__ bl, double *__restrict__ r64,
                                                              double *__restrict__ part) {
   __shared__ double sh[kTx * kTy];
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z) return;
   const int W = g.W, H = g.H, gx = g.gx, gy = g.gy, b = tile_b(g), i = (b % gx) * kTx + threadIdx.x;
@@ -205,11 +214,11 @@ __global__ void k_mg_reduce(const double *__restrict__ part, const Red *__restri
 }
 
 // r32 = r64 / scale[unit] (0 where the unit is not being corrected)
-__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                         const double *__restrict__ r64,
                                                         const double *__restrict__ scale, float *__restrict__ r32) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z) return;
   const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
@@ -225,11 +234,11 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ 
 
 // u += scale[unit] * x at interior cells; a unit with scale 0 (not being
 // corrected) is left as it is, bit for bit
-__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                          const uint8_t *__restrict__ act, const float *__restrict__ x,
                                                          const double *__restrict__ scale, double *__restrict__ u) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z) return;
   const double s = scale[g.unit0 + c];
@@ -261,10 +270,10 @@ constexpr float kSmoothOmega = 1.25f;
 
 // Coarse interior flags from the fine ones; tiles of the coarse plane (the
 // fine plane is the entry's second).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                           const uint8_t *__restrict__ af, uint8_t *__restrict__ ac) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int Wc = g.W, Hc = g.H, Wf = g.W2, Hf = g.H2, b = tile_b(g), I = (b % g.gx) * kTx + threadIdx.x;
   const uint8_t *f = af + g.o2;
   uint8_t *cc = ac + g.o;
@@ -279,17 +288,20 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict_
   }
 }
 
+// V-cycle kernels return at once for a unit whose run flag is 0 (run null:
+// no unit is skipped).
+//
 // One colour of red-black Gauss-Seidel on A_k e = rhs: e = (rhs + s * sum of
 // neighbours) / d at active cells of that colour (inactive cells hold 0).
 // x threads index the cells of one colour in a row (half-sweep tiles).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                          const uint8_t *__restrict__ act,
                                                          const float *__restrict__ rhs, float *__restrict__ e,
                                                          const double *__restrict__ run, int color) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
-  if (c >= bt.z || run[bt.y + c] == 0.0) return;
+  if (c >= bt.z || (run && run[bt.y + c] == 0.0)) return;
   const int W = g.W, H = g.H, b = tile_b(g), m = (b % g.gx) * kTx + threadIdx.x;
   const float s = g.s, d = g.d;
   const size_t N = (size_t)W * H;
@@ -340,14 +352,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__
 // zeroing e and one red half-sweep produce, bit for bit, in one pass that
 // writes every cell.
 __global__ void __launch_bounds__(kTx * kTy) k_mg_smooth_first(const Geo *__restrict__ geo,
-                                                               const int4 *__restrict__ bmap,
+                                                               const int4 *__restrict__ bmap, const Geo one,
                                                                const uint8_t *__restrict__ act,
                                                                const float *__restrict__ rhs, float *__restrict__ e,
                                                                const double *__restrict__ run) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
-  if (c >= bt.z || run[bt.y + c] == 0.0) return;
+  if (c >= bt.z || (run && run[bt.y + c] == 0.0)) return;
   const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const float s = g.s, d = g.d;
   const size_t N = (size_t)W * H;
@@ -373,7 +385,7 @@ __global__ void k_mg_coarse(const Geo *__restrict__ geo, const uint8_t *__restri
   __shared__ uint8_t sa[kCoarseMax];
   const Geo &g = geo[blockIdx.x];
   const int c = blockIdx.z;
-  if (c >= g.C || run[g.unit0 + c] == 0.0) return;
+  if (c >= g.C || (run && run[g.unit0 + c] == 0.0)) return;
   const int W = g.W, H = g.H, n = W * H, t = threadIdx.x;
   const float s = g.s, d = g.d;
   const float *rc = rhs + g.oc + (long long)c * n;
@@ -413,17 +425,17 @@ __device__ __forceinline__ float pw(int a) { return (a == 0 || a == 1) ? 0.75f :
 // active fine cells (0 elsewhere), evaluated on the fly so the residual is
 // never stored. Tiles of the coarse plane; the fine plane is the second.
 __global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(const Geo *__restrict__ geo,
-                                                                 const int4 *__restrict__ bmap,
+                                                                 const int4 *__restrict__ bmap, const Geo one,
                                                                  const uint8_t *__restrict__ af,
                                                                  const float *__restrict__ rhsf,
                                                                  const float *__restrict__ ef,
                                                                  const uint8_t *__restrict__ ac,
                                                                  float *__restrict__ rhsc,
                                                                  const double *__restrict__ run) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
-  if (c >= bt.z || run[bt.y + c] == 0.0) return;
+  if (c >= bt.z || (run && run[bt.y + c] == 0.0)) return;
   const int Wc = g.W, Hc = g.H, Wf = g.W2, Hf = g.H2, b = tile_b(g), I = (b % g.gx) * kTx + threadIdx.x;
   const float s = g.s, d = g.d;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
@@ -463,14 +475,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(const Geo *__re
 
 // e_f += bilinear prolongation of e_c at active fine cells; tiles of the fine
 // plane, the coarse plane is the second.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                           const uint8_t *__restrict__ af, float *__restrict__ ef,
                                                           const float *__restrict__ ec,
                                                           const double *__restrict__ run) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
-  if (c >= bt.z || run[bt.y + c] == 0.0) return;
+  if (c >= bt.z || (run && run[bt.y + c] == 0.0)) return;
   const int Wf = g.W, Hf = g.H, Wc = g.W2, Hc = g.H2, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t Nc = (size_t)Wc * Hc, Nf = (size_t)Wf * Hf;
   const float *e = ec + g.oc2 + c * Nc;
@@ -495,13 +507,13 @@ __device__ __forceinline__ void zero_partial(const Geo &g, int c, double *part) 
 }
 
 // q = A_0 p at active cells; partial sums of p.q
-__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                         const uint8_t *__restrict__ act, const float *__restrict__ p,
                                                         float *__restrict__ q, double *__restrict__ part,
                                                         const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z) return;
   if (run[bt.y + c] == 0.0) {  // a stopped unit: its p.q is never read
@@ -530,12 +542,12 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ 
 }
 
 // partial sums of a.b
-__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                       const float *__restrict__ x, const float *__restrict__ y,
                                                       double *__restrict__ part, const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z) return;
   if (run[bt.y + c] == 0.0) {  // a stopped unit: its rho is never read
@@ -555,12 +567,12 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ ge
 }
 
 // p = z + beta p (beta = rho_new / rho; p = z on the first iteration)
-__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                             const float *__restrict__ z, float *__restrict__ p,
                                                             const double *__restrict__ sc,
                                                             const double *__restrict__ run, int first) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z || run[bt.y + c] == 0.0) return;
   const double *s = sc + (long long)(g.unit0 + c) * S_N;
@@ -581,14 +593,14 @@ __global__ void k_cg_scalars_after_dir(int U, double *__restrict__ sc) {
 }
 
 // x += alpha p, r -= alpha q (alpha = rho / p.q); partial sums of r.r
-__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                        const float *__restrict__ p, const float *__restrict__ q,
                                                        float *__restrict__ x, float *__restrict__ r,
                                                        const double *__restrict__ sc, double *__restrict__ part,
                                                        const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
-  const Geo g = geo[bt.x];
+  const int4 bt = entry_of(bmap, one);
+  const Geo g = bmap ? geo[bt.x] : one;
   const int c = blockIdx.z;
   if (c >= bt.z) return;
   if (run[bt.y + c] == 0.0) {  // a stopped unit: x and r stay (p may never have been written)
@@ -614,12 +626,12 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ g
 }
 
 // out = interleave(u) at interior cells, the anchor elsewhere (bit for bit)
-__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int4 *__restrict__ bmap,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                        const Io *__restrict__ io, const uint8_t *__restrict__ act,
                                                        const double *__restrict__ u) {
-  const int4 bt = bmap[blockIdx.x];  // entry, its first unit, its channels
+  const int4 bt = entry_of(bmap, one);
   const int gi = bt.x;
-  const Geo g = geo[gi];
+  const Geo g = bmap ? geo[gi] : one;
   const int c = blockIdx.z, C = g.C;
   if (c >= C) return;
   const Io f = io[gi];
@@ -637,17 +649,25 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ g
 size_t aup(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // (32, 8)-thread tiles over w columns and h rows of one instance: at most
-// about 8 tiles per SM per channel, at least kMinBands bands of 8 rows per
+// about 8 tiles per SM per channel, at least min_bands bands of 8 rows per
 // tile where the instance has them (a tile's first loads -- its table entry,
 // geometry and run flag -- then serve several bands), at most 65535 rows of
-// tiles. The choice depends on the instance alone, so its partial sums are
-// the same in any batch.
+// tiles.
+//
+// Level-0 launches, whose tiles write the partial sums, take kMinBands: a
+// choice that depends on the instance alone, so its partial sums and their
+// order are the same in any batch. A V-cycle launch reduces nothing and its
+// result does not depend on the tiling; it takes kMinBands only when its
+// instances have many tiles (more than kManyWaves waves of 8 per SM at one
+// band each), and one band otherwise, so that the small launches of a single
+// image's coarse levels keep their parallelism.
 constexpr int kMinBands = 4;
-void tiles2(int w, int h, int sms, int &gx, int &gy) {
+constexpr long long kManyWaves = 4;
+void tiles2(int w, int h, int sms, int min_bands, int &gx, int &gy) {
   gx = std::max(1, (w + kTx - 1) / kTx);
   const int bands = std::max(1, (h + kTy - 1) / kTy);
   gy = std::min(bands, std::max(1, sms * 8 / gx));
-  gy = std::min(gy, (bands + kMinBands - 1) / kMinBands);
+  gy = std::min(gy, (bands + min_bands - 1) / min_bands);
   gy = std::min(gy, 65535);
 }
 const dim3 kBlock2(kTx, kTy);
@@ -677,6 +697,7 @@ struct Launch {
   size_t geo = 0, bmap = 0;  // byte offsets of the tables in the table area
   int n = 0;                 // entries (instances)
   long long blocks = 0;
+  Geo one{};                 // the entry of a launch over one instance (passed by value)
 };
 
 struct LevelArr {
@@ -706,6 +727,7 @@ Launch make_launch(Blob &blob, std::vector<Geo> &gs) {
     blk += nb;
   }
   l.blocks = blk;
+  if (gs.size() == 1) l.one = gs[0];
   l.geo = blob.put(gs.data(), gs.size() * sizeof(Geo));
   l.bmap = blob.put(bm.data(), bm.size() * sizeof(int4));
   return l;
@@ -727,13 +749,16 @@ struct Mg {
   long long launches = 0;
   template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
   const Geo *geo(const Launch &l) { return at<Geo>(tab + l.geo); }
-  const int4 *bmap(const Launch &l) { return at<int4>(tab + l.bmap); }
+  const int4 *bmap(const Launch &l) { return l.n == 1 ? nullptr : at<int4>(tab + l.bmap); }
   dim3 grid(const Launch &l, unsigned z) { return dim3((unsigned)l.blocks, 1, z); }
 };
 
 void vcycle(Mg &m, float *rhs0, float *e0) {
   const int L = (int)m.lv.size();
-  const double *run = m.at<double>(m.run);
+  // Units whose run has stopped skip the V-cycle in a batch; a single image's
+  // channels do the work regardless (their z is not read) and so spare every
+  // block a load before its first data.
+  const double *run = m.in.size() > 1 ? m.at<double>(m.run) : nullptr;
   const unsigned Cz = m.Cmax;
   for (int k = 0; k < L; ++k) {
     const LevelArr &v = m.lv[k];
@@ -747,12 +772,12 @@ void vcycle(Mg &m, float *rhs0, float *e0) {
     const Launch &F = m.full[k], &Hh = m.half[k], &R = m.restr[k];
     if (!F.n) continue;
     // red, black, red, black from e = 0 (the first red half-sweep writes all of e)
-    k_mg_smooth_first<<<m.grid(F, Cz), kBlock2, 0, m.st>>>(m.geo(F), m.bmap(F), act, rhs, e, run);
-    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 1);
-    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 0);
-    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 1);
+    k_mg_smooth_first<<<m.grid(F, Cz), kBlock2, 0, m.st>>>(m.geo(F), m.bmap(F), F.one, act, rhs, e, run);
+    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), Hh.one, act, rhs, e, run, 1);
+    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), Hh.one, act, rhs, e, run, 0);
+    k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), Hh.one, act, rhs, e, run, 1);
     const LevelArr &cl = m.lv[k + 1];
-    k_mg_resid_restrict<<<m.grid(R, Cz), kBlock2, 0, m.st>>>(m.geo(R), m.bmap(R), act, rhs, e,
+    k_mg_resid_restrict<<<m.grid(R, Cz), kBlock2, 0, m.st>>>(m.geo(R), m.bmap(R), R.one, act, rhs, e,
                                                               m.at<uint8_t>(cl.act), m.at<float>(cl.rhs), run);
     m.launches += 5;
   }
@@ -762,10 +787,10 @@ void vcycle(Mg &m, float *rhs0, float *e0) {
     const LevelArr &v = m.lv[k], &cl = m.lv[k + 1];
     float *rhs = k == 0 ? rhs0 : m.at<float>(v.rhs), *e = k == 0 ? e0 : m.at<float>(v.e);
     const uint8_t *act = m.at<uint8_t>(v.act);
-    k_mg_prolong<<<m.grid(F, Cz), kBlock2, 0, m.st>>>(m.geo(F), m.bmap(F), act, e, m.at<float>(cl.e), run);
+    k_mg_prolong<<<m.grid(F, Cz), kBlock2, 0, m.st>>>(m.geo(F), m.bmap(F), F.one, act, e, m.at<float>(cl.e), run);
     for (int t = 0; t < 2; ++t) {
-      k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 1);
-      k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), act, rhs, e, run, 0);
+      k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), Hh.one, act, rhs, e, run, 1);
+      k_mg_smooth<<<m.grid(Hh, Cz), kBlock2, 0, m.st>>>(m.geo(Hh), m.bmap(Hh), Hh.one, act, rhs, e, run, 0);
     }
     m.launches += 5;
   }
@@ -803,7 +828,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
       w = (w + 1) / 2; h = (h + 1) / 2; ++k;
     }
     I.L = (int)I.w.size();
-    tiles2(I.W, I.H, sms, I.gx, I.gy);
+    tiles2(I.W, I.H, sms, kMinBands, I.gx, I.gy);
     I.unit0 = m.U;
     m.U += I.C;
     I.part0 = P;
@@ -825,10 +850,10 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
 
   // launch tables
   Blob blob;
-  auto geo_at = [&](const Inst &I, int k, int tw, int th) {
+  auto geo_at = [&](const Inst &I, int k, int tw, int th, int mb) {
     Geo g{};
     g.W = I.w[k]; g.H = I.h[k];
-    tiles2(tw, th, sms, g.gx, g.gy);
+    tiles2(tw, th, sms, mb, g.gx, g.gy);
     g.C = I.C; g.unit0 = I.unit0; g.part0 = I.part0;
     g.o = I.o[k]; g.oc = I.oc[k];
     g.s = level_s(k);
@@ -841,21 +866,29 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
   };
   {
     std::vector<Geo> g0;
-    for (const Inst &I : m.in) g0.push_back(geo_at(I, 0, I.W, I.H));
+    for (const Inst &I : m.in) g0.push_back(geo_at(I, 0, I.W, I.H, kMinBands));
     m.all0 = make_launch(blob, g0);
   }
   m.full.resize(Lmax); m.half.resize(Lmax); m.restr.resize(Lmax); m.coarse.resize(Lmax);
   for (int k = 0; k < Lmax; ++k) {
+    long long many = 0;  // the level's tiles at one band each, all channels
+    for (const Inst &I : m.in)
+      if (k < I.L - 1) {
+        int gx, gy;
+        tiles2(I.w[k], I.h[k], sms, 1, gx, gy);
+        many += (long long)I.C * gx * gy;
+      }
+    const int mb = many > kManyWaves * 8 * sms ? kMinBands : 1;
     std::vector<Geo> gf, gh, gr, gk;
     for (const Inst &I : m.in) {
       if (k == I.L - 1) {
-        gk.push_back(geo_at(I, k, 1, 1));
+        gk.push_back(geo_at(I, k, 1, 1, 1));
       } else if (k < I.L - 1) {
-        Geo f = geo_at(I, k, I.w[k], I.h[k]);
+        Geo f = geo_at(I, k, I.w[k], I.h[k], mb);
         second(f, I, k + 1);
         gf.push_back(f);
-        gh.push_back(geo_at(I, k, (I.w[k] + 1) / 2, I.h[k]));
-        Geo r = geo_at(I, k + 1, I.w[k + 1], I.h[k + 1]);  // coarse tiles, the fine level's operator
+        gh.push_back(geo_at(I, k, (I.w[k] + 1) / 2, I.h[k], mb));
+        Geo r = geo_at(I, k + 1, I.w[k + 1], I.h[k + 1], mb);  // coarse tiles, the fine level's operator
         r.s = level_s(k);
         r.d = 4.0f * r.s + (float)I.lambda;
         second(r, I, k);
@@ -936,12 +969,12 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
          *run = m.at<double>(m.run);
   float *x = m.at<float>(m.x), *r = m.at<float>(m.r), *z = m.at<float>(m.z), *pp = m.at<float>(m.p),
         *q = m.at<float>(m.q);
-  k_mg_assemble<<<ga, kBlock2, 0, m.st>>>(g0, b0, iod, act0, u, bl, any_warm ? m.at<double>(m.uw) : nullptr);
+  k_mg_assemble<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u, bl, any_warm ? m.at<double>(m.uw) : nullptr);
   m.launches = 1;
   for (int k = 0; k + 1 < Lmax; ++k) {
     const Launch &R = m.restr[k];
     if (!R.n) continue;
-    k_mg_coarsen<<<m.grid(R, 1), kBlock2, 0, m.st>>>(m.geo(R), m.bmap(R), m.at<uint8_t>(m.lv[k].act),
+    k_mg_coarsen<<<m.grid(R, 1), kBlock2, 0, m.st>>>(m.geo(R), m.bmap(R), R.one, m.at<uint8_t>(m.lv[k].act),
                                                      m.at<uint8_t>(m.lv[k + 1].act));
     ++m.launches;
   }
@@ -961,7 +994,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
   // FP64 residual norms per unit of the current u -> host
   std::vector<double> nrm(U);
   auto residual = [&](const double *uu) -> cudaError_t {
-    k_mg_residual64<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, uu, bl, r64, part);
+    k_mg_residual64<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, act0, uu, bl, r64, part);
     k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, red, 1);
     m.launches += 2;
     cudaError_t e = cudaMemcpyAsync(nrm.data(), red, (size_t)U * 8, cudaMemcpyDeviceToHost, m.st);
@@ -1010,7 +1043,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
   if (poisoned) {  // u = fma(NaN, 0, u) = NaN at interior cells of those units
     cudaMemcpyAsync(scale, hscale.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
     cudaMemsetAsync(x, 0, NC * 4, m.st);
-    k_mg_update<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, x, scale, u);
+    k_mg_update<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, act0, x, scale, u);
     ++m.launches;
     std::fill(hscale.begin(), hscale.end(), 0.0);
   }
@@ -1024,13 +1057,13 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
   auto enqueue_iteration = [&](bool first) -> cudaError_t {
     const long long l0 = m.launches;
     vcycle(m, r, z);
-    k_cg_dot<<<ga, kBlock2, 0, m.st>>>(g0, b0, r, z, part, run);
+    k_cg_dot<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, r, z, part, run);
     k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, sc + S_RHO_NEW, S_N);
-    k_cg_direction<<<ga, kBlock2, 0, m.st>>>(g0, b0, z, pp, sc, run, first ? 1 : 0);
+    k_cg_direction<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, z, pp, sc, run, first ? 1 : 0);
     k_cg_scalars_after_dir<<<gsc, kThreads, 0, m.st>>>(U, sc);
-    k_cg_apply<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, pp, q, part, run);
+    k_cg_apply<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, act0, pp, q, part, run);
     k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, sc + S_PQ, S_N);
-    k_cg_step<<<ga, kBlock2, 0, m.st>>>(g0, b0, pp, q, x, r, sc, part, run);
+    k_cg_step<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, pp, q, x, r, sc, part, run);
     k_mg_reduce<<<U, kThreads, 0, m.st>>>(part, rtab, red, 1);
     m.launches += 8;
     per_iteration = m.launches - l0;
@@ -1080,7 +1113,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
     cudaMemcpyAsync(scale, hscale.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
     cudaMemcpyAsync(run, hrun.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
     cudaMemsetAsync(sc, 0, (size_t)U * S_N * 8, m.st);
-    k_mg_scale<<<ga, kBlock2, 0, m.st>>>(g0, b0, r64, scale, r);
+    k_mg_scale<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, r64, scale, r);
     cudaMemsetAsync(x, 0, NC * 4, m.st);
     m.launches += 1;
     // inner target: a quarter of the remaining bar, at most as deep as FP32
@@ -1125,7 +1158,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
       if (changed) cudaMemcpyAsync(run, hrun.data(), (size_t)U * 8, cudaMemcpyHostToDevice, m.st);
     }
     // u += scale * x, then the FP64 residual decides
-    k_mg_update<<<ga, kBlock2, 0, m.st>>>(g0, b0, act0, x, scale, u);
+    k_mg_update<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, act0, x, scale, u);
     ++m.launches;
     const std::vector<double> prev = cur;
     ce = residual(u);
@@ -1142,7 +1175,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
     ++outer;
   }
   cudaEventRecord(ctx->ev[2], m.st);
-  k_mg_emit<<<ga, kBlock2, 0, m.st>>>(g0, b0, iod, act0, u);
+  k_mg_emit<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u);
   ++m.launches;
   ce = cudaSuccess;
   for (size_t k = 0; k < m.in.size() && ce == cudaSuccess; ++k) {
@@ -1239,7 +1272,7 @@ pt_status ptk_solve_mg_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, floa
       continue;
     }
     int gx, gy;
-    tiles2((int)p.width, (int)p.height, ctx->sms, gx, gy);
+    tiles2((int)p.width, (int)p.height, ctx->sms, kMinBands, gx, gy);
     const long long t = (long long)gx * gy;
     if (!ids.empty() && (tiles + t > kGroupTiles || units + p.channels > kGroupTiles)) {
       const pt_status s = flush();
