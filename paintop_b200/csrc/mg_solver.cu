@@ -129,7 +129,8 @@ struct Io {
 
 // ---- assembly ----------------------------------------------------------------
 // interior flag, u = anchor (or the warm guess at interior cells), b' =
-// fma(lambda, -anchor, laplacian(guidance)) at interior cells; level-0 tiles.
+// fma(lambda, -anchor, laplacian(guidance)) at interior cells; level-0 tiles,
+// grid.z 1 (each thread does all channels of its cells).
 __global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                            const Io *__restrict__ io, uint8_t *__restrict__ act,
                                                            double *__restrict__ u, double *__restrict__ bl,
@@ -137,30 +138,30 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict
   const int4 bt = entry_of(bmap, one);
   const int gi = bt.x;
   const Geo g = bmap ? geo[gi] : one;
-  const int c = blockIdx.z, C = g.C;
-  if (c >= C) return;
   const Io f = io[gi];
-  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
+  const int C = g.C, W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
   uint8_t *a = act + g.o;
-  double *uc = u + g.oc + c * N, *bc = bl + g.oc + c * N, *wc = uw ? uw + g.oc + c * N : nullptr;
+  double *u0 = u + g.oc, *b0 = bl + g.oc, *w0 = uw ? uw + g.oc : nullptr;
   for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
     const size_t q = (size_t)j * W + i;
     const bool in = W >= 3 && H >= 3 && i > 0 && j > 0 && i < W - 1 && j < H - 1 && f.mask[q] > 0.5f;
-    if (c == 0) a[q] = in ? 1 : 0;
-    const double av = (double)f.anchor[q * C + c];
-    uc[q] = av;
-    double bv = 0.0;
-    if (in) {
-      // poisson.rs:364-373: L, R, U, D, then fma(4, -centre, sum)
-      const float *gd = f.guid;
-      const double ctr = (double)gd[q * C + c];
-      const double s = (double)gd[(q - 1) * C + c] + (double)gd[(q + 1) * C + c] + (double)gd[(q - W) * C + c] +
-                       (double)gd[(q + W) * C + c];
-      bv = fma(4.0, -ctr, s);
+    a[q] = in ? 1 : 0;
+    for (int c = 0; c < C; ++c) {  // a thread's channels are adjacent in the interleaved inputs
+      const double av = (double)f.anchor[q * C + c];
+      u0[c * N + q] = av;
+      double bv = 0.0;
+      if (in) {
+        // poisson.rs:364-373: L, R, U, D, then fma(4, -centre, sum)
+        const float *gd = f.guid;
+        const double ctr = (double)gd[q * C + c];
+        const double s = (double)gd[(q - 1) * C + c] + (double)gd[(q + 1) * C + c] + (double)gd[(q - W) * C + c] +
+                         (double)gd[(q + W) * C + c];
+        bv = fma(4.0, -ctr, s);
+      }
+      b0[c * N + q] = in ? fma(g.lambda, -av, bv) : 0.0;
+      if (w0) w0[c * N + q] = (in && f.guess) ? (double)f.guess[q * C + c] : av;
     }
-    bc[q] = in ? fma(g.lambda, -av, bv) : 0.0;
-    if (wc) wc[q] = (in && f.guess) ? (double)f.guess[q * C + c] : av;
   }
 }
 
@@ -625,23 +626,24 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ g
   if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
 }
 
-// out = interleave(u) at interior cells, the anchor elsewhere (bit for bit)
+// out = interleave(u) at interior cells, the anchor elsewhere (bit for bit);
+// level-0 tiles, grid.z 1
 __global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
                                                        const Io *__restrict__ io, const uint8_t *__restrict__ act,
                                                        const double *__restrict__ u) {
   const int4 bt = entry_of(bmap, one);
   const int gi = bt.x;
   const Geo g = bmap ? geo[gi] : one;
-  const int c = blockIdx.z, C = g.C;
-  if (c >= C) return;
   const Io f = io[gi];
-  const int W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
+  const int C = g.C, W = g.W, H = g.H, b = tile_b(g), i = (b % g.gx) * kTx + threadIdx.x;
   const size_t N = (size_t)W * H;
   const uint8_t *a = act + g.o;
-  const double *uc = u + g.oc + c * N;
+  const double *u0 = u + g.oc;
   for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
     const size_t q = (size_t)j * W + i;
-    f.out[q * C + c] = a[q] ? (float)uc[q] : f.anchor[q * C + c];
+    const bool in = a[q] != 0;
+    for (int c = 0; c < C; ++c)  // a warp writes 32 whole pixels: C * 32 adjacent floats
+      f.out[q * C + c] = in ? (float)u0[c * N + q] : f.anchor[q * C + c];
   }
 }
 
@@ -969,7 +971,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
          *run = m.at<double>(m.run);
   float *x = m.at<float>(m.x), *r = m.at<float>(m.r), *z = m.at<float>(m.z), *pp = m.at<float>(m.p),
         *q = m.at<float>(m.q);
-  k_mg_assemble<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u, bl, any_warm ? m.at<double>(m.uw) : nullptr);
+  k_mg_assemble<<<m.grid(A, 1), kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u, bl, any_warm ? m.at<double>(m.uw) : nullptr);
   m.launches = 1;
   for (int k = 0; k + 1 < Lmax; ++k) {
     const Launch &R = m.restr[k];
@@ -1175,7 +1177,7 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
     ++outer;
   }
   cudaEventRecord(ctx->ev[2], m.st);
-  k_mg_emit<<<ga, kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u);
+  k_mg_emit<<<m.grid(A, 1), kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u);
   ++m.launches;
   ce = cudaSuccess;
   for (size_t k = 0; k < m.in.size() && ce == cudaSuccess; ++k) {
