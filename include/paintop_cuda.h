@@ -128,7 +128,12 @@ pt_status pt_poisson_solve(pt_ctx *ctx, const pt_problem *p, float *out_candidat
 
 /* Solve n independent images in one persistent launch. outs[i], reports[i]
  * (channels_i + 1 entries) and histories[i] (channels_i * max_iterations_i, or
- * NULL; `histories` itself may be NULL) follow pt_poisson_solve. */
+ * NULL; `histories` itself may be NULL) follow pt_poisson_solve. Without
+ * PT_FLAG_MULTIGRID, PT_FLAG_DEVICE_POINTERS must agree across the batch. With
+ * PT_FLAG_MULTIGRID (on every problem), all images share each launch of the
+ * multigrid-CG iteration, may mix host and device buffers, extents, channels,
+ * lambda, tolerance and caps, and each image's output, reports and history are
+ * bit for bit those of pt_poisson_solve on it alone. */
 pt_status pt_poisson_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n,
                                  float *const *outs, pt_report *const *reports,
                                  double *const *histories);

@@ -131,7 +131,8 @@ struct Io {
 // interior flag, u = anchor (or the warm guess at interior cells), b' =
 // fma(lambda, -anchor, laplacian(guidance)) at interior cells; level-0 tiles,
 // grid.z 1 (each thread does all channels of its cells).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict__ geo,
+                                                           const int4 *__restrict__ bmap, const Geo one,
                                                            const Io *__restrict__ io, uint8_t *__restrict__ act,
                                                            double *__restrict__ u, double *__restrict__ bl,
                                                            double *__restrict__ uw) {
@@ -167,7 +168,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_assemble(const Geo *__restrict
 
 // r = fma(lambda + 4, -u, nsum) - b' at interior cells (0 elsewhere) and
 // per-tile partial sums of r^2.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_residual64(const Geo *__restrict__ geo,
+                                                             const int4 *__restrict__ bmap, const Geo one,
                                                              const uint8_t *__restrict__ act,
                                                              const double *__restrict__ u,
                                                              const double *__restrict__ bl, double *__restrict__ r64,
@@ -215,7 +217,8 @@ __global__ void k_mg_reduce(const double *__restrict__ part, const Red *__restri
 }
 
 // r32 = r64 / scale[unit] (0 where the unit is not being corrected)
-__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ geo,
+                                                        const int4 *__restrict__ bmap, const Geo one,
                                                         const double *__restrict__ r64,
                                                         const double *__restrict__ scale, float *__restrict__ r32) {
   const int4 bt = entry_of(bmap, one);
@@ -235,7 +238,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_scale(const Geo *__restrict__ 
 
 // u += scale[unit] * x at interior cells; a unit with scale 0 (not being
 // corrected) is left as it is, bit for bit
-__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_update(const Geo *__restrict__ geo,
+                                                         const int4 *__restrict__ bmap, const Geo one,
                                                          const uint8_t *__restrict__ act, const float *__restrict__ x,
                                                          const double *__restrict__ scale, double *__restrict__ u) {
   const int4 bt = entry_of(bmap, one);
@@ -271,7 +275,8 @@ constexpr float kSmoothOmega = 1.25f;
 
 // Coarse interior flags from the fine ones; tiles of the coarse plane (the
 // fine plane is the entry's second).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict__ geo,
+                                                          const int4 *__restrict__ bmap, const Geo one,
                                                           const uint8_t *__restrict__ af, uint8_t *__restrict__ ac) {
   const int4 bt = entry_of(bmap, one);
   const Geo g = bmap ? geo[bt.x] : one;
@@ -295,7 +300,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_coarsen(const Geo *__restrict_
 // One colour of red-black Gauss-Seidel on A_k e = rhs: e = (rhs + s * sum of
 // neighbours) / d at active cells of that colour (inactive cells hold 0).
 // x threads index the cells of one colour in a row (half-sweep tiles).
-__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_smooth(const Geo *__restrict__ geo,
+                                                         const int4 *__restrict__ bmap, const Geo one,
                                                          const uint8_t *__restrict__ act,
                                                          const float *__restrict__ rhs, float *__restrict__ e,
                                                          const double *__restrict__ run, int color) {
@@ -476,7 +482,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_mg_resid_restrict(const Geo *__re
 
 // e_f += bilinear prolongation of e_c at active fine cells; tiles of the fine
 // plane, the coarse plane is the second.
-__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_prolong(const Geo *__restrict__ geo,
+                                                          const int4 *__restrict__ bmap, const Geo one,
                                                           const uint8_t *__restrict__ af, float *__restrict__ ef,
                                                           const float *__restrict__ ec,
                                                           const double *__restrict__ run) {
@@ -508,7 +515,8 @@ __device__ __forceinline__ void zero_partial(const Geo &g, int c, double *part) 
 }
 
 // q = A_0 p at active cells; partial sums of p.q
-__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ geo,
+                                                        const int4 *__restrict__ bmap, const Geo one,
                                                         const uint8_t *__restrict__ act, const float *__restrict__ p,
                                                         float *__restrict__ q, double *__restrict__ part,
                                                         const double *__restrict__ run) {
@@ -543,7 +551,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ 
 }
 
 // partial sums of a.b
-__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ geo,
+                                                      const int4 *__restrict__ bmap, const Geo one,
                                                       const float *__restrict__ x, const float *__restrict__ y,
                                                       double *__restrict__ part, const double *__restrict__ run) {
   __shared__ double sh[kTx * kTy];
@@ -568,7 +577,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ ge
 }
 
 // p = z + beta p (beta = rho_new / rho; p = z on the first iteration)
-__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restrict__ geo,
+                                                            const int4 *__restrict__ bmap, const Geo one,
                                                             const float *__restrict__ z, float *__restrict__ p,
                                                             const double *__restrict__ sc,
                                                             const double *__restrict__ run, int first) {
@@ -594,7 +604,8 @@ __global__ void k_cg_scalars_after_dir(int U, double *__restrict__ sc) {
 }
 
 // x += alpha p, r -= alpha q (alpha = rho / p.q); partial sums of r.r
-__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ geo,
+                                                       const int4 *__restrict__ bmap, const Geo one,
                                                        const float *__restrict__ p, const float *__restrict__ q,
                                                        float *__restrict__ x, float *__restrict__ r,
                                                        const double *__restrict__ sc, double *__restrict__ part,
@@ -628,7 +639,8 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ g
 
 // out = interleave(u) at interior cells, the anchor elsewhere (bit for bit);
 // level-0 tiles, grid.z 1
-__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo, const int4 *__restrict__ bmap, const Geo one,
+__global__ void __launch_bounds__(kTx * kTy) k_mg_emit(const Geo *__restrict__ geo,
+                                                       const int4 *__restrict__ bmap, const Geo one,
                                                        const Io *__restrict__ io, const uint8_t *__restrict__ act,
                                                        const double *__restrict__ u) {
   const int4 bt = entry_of(bmap, one);
@@ -956,7 +968,8 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
       ce = cudaMemcpyAsync(m.at<float>(I.guess), p.initial_guess, nc * 4, cudaMemcpyHostToDevice, m.st);
     io[k] = Io{in, in + nc, m.at<float>(I.mask), I.warm ? m.at<float>(I.guess) : nullptr, m.at<float>(I.out)};
   }
-  if (ce == cudaSuccess) ce = cudaMemcpyAsync(m.base + m.io, io.data(), io.size() * sizeof(Io), cudaMemcpyHostToDevice, m.st);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(m.base + m.io, io.data(), io.size() * sizeof(Io), cudaMemcpyHostToDevice, m.st);
   if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, std::string("input upload: ") + cudaGetErrorString(ce));
 
   const Io *iod = m.at<Io>(m.io);
@@ -971,7 +984,8 @@ pt_status solve_group(pt_ctx *ctx, const pt_problem *ps, const std::vector<int> 
          *run = m.at<double>(m.run);
   float *x = m.at<float>(m.x), *r = m.at<float>(m.r), *z = m.at<float>(m.z), *pp = m.at<float>(m.p),
         *q = m.at<float>(m.q);
-  k_mg_assemble<<<m.grid(A, 1), kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u, bl, any_warm ? m.at<double>(m.uw) : nullptr);
+  k_mg_assemble<<<m.grid(A, 1), kBlock2, 0, m.st>>>(g0, b0, A.one, iod, act0, u, bl,
+                                                     any_warm ? m.at<double>(m.uw) : nullptr);
   m.launches = 1;
   for (int k = 0; k + 1 < Lmax; ++k) {
     const Launch &R = m.restr[k];
