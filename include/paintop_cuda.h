@@ -222,6 +222,18 @@ pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port *inputs,
                         double *residual_history, uint32_t history_cap,
                         int32_t *all_finite, pt_error *err);
 
+/* pt_op_compute with flags for the op's solve, for a backend implementation
+ * registered beside the default one (a plan picks it by implementation id):
+ * 0 is pt_op_compute exactly (red-black SOR); PT_FLAG_MULTIGRID solves the same
+ * system to the same bar by multigrid-preconditioned CG, SolverData.steps and
+ * .iterations then counting CG iterations. Any other bit is PT_INVALID_ARG
+ * (E_CUDA_SOLVE_FLAGS). The mask generators ignore the flags. */
+pt_status pt_op_compute_ex(pt_ctx *ctx, const char *op_id, const pt_port *inputs,
+                           uint32_t n_inputs, const char *params_json, float *candidate,
+                           size_t candidate_count, pt_solver_data *solver,
+                           double *residual_history, uint32_t history_cap,
+                           int32_t *all_finite, pt_error *err, uint32_t solve_flags);
+
 const char *pt_status_str(pt_status s);
 
 /* Last CUDA / watchdog detail recorded on this context ("" if none). */

@@ -27,7 +27,7 @@ STOP_REASONS = ("converged", "max-iterations", "stalled")
 # Every symbol include/paintop_cuda.h declares.
 EXPORTED = (
     "pt_ctx_create", "pt_ctx_destroy", "pt_poisson_solve", "pt_poisson_solve_batch",
-    "pt_op_compute", "pt_status_str", "pt_ctx_last_error", "pt_tile_config_count",
+    "pt_op_compute", "pt_op_compute_ex", "pt_status_str", "pt_ctx_last_error", "pt_tile_config_count",
     "pt_tile_config_info", "pt_ctx_set_config", "pt_ctx_last_config", "pt_autotune",
     "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_poisson_solve_noalloc",
     "pt_unet_create", "pt_unet_destroy", "pt_unet_param_count", "pt_unet_get_params",
@@ -118,6 +118,8 @@ def lib():
     L.pt_op_compute.argtypes = [vp, C.c_char_p, C.POINTER(PtPort), u32, C.c_char_p, vp, C.c_size_t,
                                 C.POINTER(PtSolverData), vp, u32, C.POINTER(i32), C.POINTER(PtError)]
     L.pt_op_compute.restype = C.c_int
+    L.pt_op_compute_ex.argtypes = list(L.pt_op_compute.argtypes) + [u32]
+    L.pt_op_compute_ex.restype = C.c_int
     L.pt_status_str.argtypes = [C.c_int]
     L.pt_status_str.restype = C.c_char_p
     L.pt_ctx_last_error.argtypes = [vp]
@@ -334,8 +336,10 @@ class Context:
             ret.append((out, per, reps[c].as_dict()))
         return ret
 
-    def op_compute(self, op_id: str, inputs: dict, params_json: str, history_cap: int = 100000):
-        """pt_op_compute. inputs: name -> (kind, width, height, channels, samples f32)."""
+    def op_compute(self, op_id: str, inputs: dict, params_json: str, history_cap: int = 100000,
+                   solve_flags: int = 0):
+        """pt_op_compute (pt_op_compute_ex when solve_flags is not 0). inputs:
+        name -> (kind, width, height, channels, samples f32)."""
         ports = (PtPort * len(inputs))()
         keep = []
         out_shape = None
@@ -359,8 +363,8 @@ class Context:
         hist = np.zeros(max(history_cap, 1), dtype=np.float64)
         fin = C.c_int32(0)
         err = PtError()
-        st = lib().pt_op_compute(self.h, op_id.encode(), ports, len(inputs), params_json.encode(),
-                                 cand.ctypes.data, count, C.byref(sd), hist.ctypes.data,
-                                 history_cap, C.byref(fin), C.byref(err))
+        args = (self.h, op_id.encode(), ports, len(inputs), params_json.encode(), cand.ctypes.data, count,
+                C.byref(sd), hist.ctypes.data, history_cap, C.byref(fin), C.byref(err))
+        st = lib().pt_op_compute_ex(*args, solve_flags) if solve_flags else lib().pt_op_compute(*args)
         return st, cand[:count], sd, hist[: min(sd.history_len, history_cap)].tolist(), \
             bool(fin.value), err

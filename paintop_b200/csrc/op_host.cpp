@@ -529,13 +529,18 @@ pt_status mask_op_compute(pt_ctx *ctx, bool ellipse, const pt_port *inputs, uint
 
 using namespace pt_op;
 
-extern "C" pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port *inputs,
-                                   uint32_t n_inputs, const char *params_json, float *candidate,
-                                   size_t candidate_count, pt_solver_data *solver,
-                                   double *residual_history, uint32_t history_cap,
-                                   int32_t *all_finite, pt_error *err) {
+extern "C" pt_status pt_op_compute_ex(pt_ctx *ctx, const char *op_id, const pt_port *inputs,
+                                      uint32_t n_inputs, const char *params_json, float *candidate,
+                                      size_t candidate_count, pt_solver_data *solver,
+                                      double *residual_history, uint32_t history_cap,
+                                      int32_t *all_finite, pt_error *err, uint32_t solve_flags) {
   if (err) std::memset(err, 0, sizeof(*err));
   if (!op_id || (n_inputs && !inputs)) return PT_INVALID_ARG;
+  if (solve_flags & ~PT_FLAG_MULTIGRID) {
+    set_error(err, OpError{"execution", "E_CUDA_SOLVE_FLAGS",
+                           std::string("unsupported solve flags ") + std::to_string(solve_flags), ""});
+    return PT_INVALID_ARG;
+  }
   if (std::strcmp(op_id, "mask.ellipse@1") == 0 || std::strcmp(op_id, "mask.polygon@1") == 0)
     return mask_op_compute(ctx, op_id[5] == 'e', inputs, n_inputs, params_json, candidate, candidate_count,
                            all_finite, err);
@@ -637,7 +642,7 @@ extern "C" pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port
   p.max_iterations = controls.max_iterations;
   p.tolerance = controls.tolerance;
   p.omega = OMEGA;
-  p.flags = 0;
+  p.flags = solve_flags;
   if (!ctx) {
     // validation passed but there is no device context: the backend is
     // unavailable (the E_GPU_UNAVAILABLE analogue, a Policy error)
@@ -680,4 +685,13 @@ extern "C" pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port
     *all_finite = f;
   }
   return PT_OK;
+}
+
+extern "C" pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port *inputs,
+                                   uint32_t n_inputs, const char *params_json, float *candidate,
+                                   size_t candidate_count, pt_solver_data *solver,
+                                   double *residual_history, uint32_t history_cap,
+                                   int32_t *all_finite, pt_error *err) {
+  return pt_op_compute_ex(ctx, op_id, inputs, n_inputs, params_json, candidate, candidate_count, solver,
+                          residual_history, history_cap, all_finite, err, 0);
 }

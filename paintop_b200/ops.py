@@ -24,6 +24,9 @@ import numpy as np
 from . import _lib
 
 IMPLEMENTATION_ID = "cuda.poisson@1"
+# The second implementation of the two Poisson ops: the same contract solved by
+# multigrid-preconditioned CG (pt_op_compute_ex with PT_FLAG_MULTIGRID).
+MULTIGRID_IMPLEMENTATION_ID = "cuda.multigrid@1"
 
 
 class PaintopError(Exception):
@@ -122,6 +125,14 @@ class _PoissonOp:
     OP_ID = ""
     PORTS = ("", "", "mask")
 
+    def __init__(self, multigrid: bool = False):
+        """multigrid=False: ``cuda.poisson@1`` (red-black SOR). multigrid=True:
+        ``cuda.multigrid@1``, the same inputs, params, validation, stopping bar
+        and report, solved by multigrid-preconditioned CG; ``steps`` and
+        ``iterations`` then count CG iterations."""
+        self.solve_flags = _lib.PT_FLAG_MULTIGRID if multigrid else 0
+        self.implementation_id = MULTIGRID_IMPLEMENTATION_ID if multigrid else IMPLEMENTATION_ID
+
     def compute(self, inputs: dict, params) -> dict:
         ctx = context()
         ports = {}
@@ -131,7 +142,7 @@ class _PoissonOp:
                 kind = 7  # neither an image nor a mask: a Type error in the host layer
             ports[name] = (kind, v.width, v.height, v.channels, v.samples)
         pj = json.dumps(params) if not isinstance(params, str) else params
-        st, cand, sd, hist, all_finite, err = ctx.op_compute(self.OP_ID, ports, pj)
+        st, cand, sd, hist, all_finite, err = ctx.op_compute(self.OP_ID, ports, pj, solve_flags=self.solve_flags)
         if st != _lib.PT_OK:
             if err.code:
                 raise PaintopError(err.error_class.decode(), err.code.decode(),

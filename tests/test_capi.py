@@ -87,7 +87,7 @@ def _ports(names_kinds, w=8, h=8, c=1, mask_w=None, mask_h=None):
     return ports
 
 
-def op_call(op_id, ports, params):
+def op_call(op_id, ports, params, solve_flags=None):
     from paintop_b200 import _lib
     L = _lib.lib()
     arr = (_lib.PtPort * len(ports))()
@@ -103,8 +103,9 @@ def op_call(op_id, ports, params):
     sd = _lib.PtSolverData()
     err = _lib.PtError()
     fin = C.c_int32()
-    st = L.pt_op_compute(None, op_id.encode(), arr, len(ports), params.encode(), cand.ctypes.data,
-                         out_n, C.byref(sd), None, 0, C.byref(fin), C.byref(err))
+    args = (None, op_id.encode(), arr, len(ports), params.encode(), cand.ctypes.data, out_n, C.byref(sd), None, 0,
+            C.byref(fin), C.byref(err))
+    st = L.pt_op_compute(*args) if solve_flags is None else L.pt_op_compute_ex(*args, solve_flags)
     return st, err.error_class.decode(), err.code.decode(), err.message.decode()
 
 
@@ -208,3 +209,21 @@ def test_unknown_op_and_bad_json(cuda_lib):
     assert st == 2 and cls == "reference"
     st, cls, code, _ = op_call(BLEND, blend_ports(), "{not json")
     assert st == 2 and cls == "parse"
+
+
+def test_solve_flags_entry_point(cuda_lib):
+    """pt_op_compute_ex, the entry point of the multigrid implementation: with
+    flags 0 or PT_FLAG_MULTIGRID it validates exactly as pt_op_compute (the same
+    errors, then no device); any other bit is refused before anything else."""
+    from paintop_b200 import _lib
+    for flags in (0, _lib.PT_FLAG_MULTIGRID):
+        for params in ('{"tolerance": 2.0}', '{"max_iterations": 0}', "{not json"):
+            assert op_call(BLEND, blend_ports(), params, flags) == op_call(BLEND, blend_ports(), params)
+        assert op_call(SCREENED, screened_ports(mask_w=3, mask_h=8), "{}", flags) == \
+            op_call(SCREENED, screened_ports(mask_w=3, mask_h=8), "{}")
+        st, cls, code, _ = op_call(SCREENED, screened_ports(), '{"lambda": 0.5}', flags)
+        assert (st, cls, code) == (1, "policy", "E_CUDA_UNAVAILABLE")
+    for bad in (_lib.PT_FLAG_DEVICE_POINTERS, _lib.PT_FLAG_OMEGA_AUTO, _lib.PT_FLAG_MULTIGRID | 0x100):
+        st, cls, code, msg = op_call(BLEND, blend_ports(), "{}", bad)
+        assert (st, cls, code) == (2, "execution", "E_CUDA_SOLVE_FLAGS")
+        assert msg == f"unsupported solve flags {bad}"

@@ -229,3 +229,37 @@ def test_multigrid_mixed_batch_equals_solving_alone(ctx, oracle, L):
     assert by_kind["nan"][2]["stop_reason"] == "stalled"
     assert res[4][2]["stop_reason"] == "max-iterations" and res[4][2]["iterations"] == 3
     assert all(r["converged"] for k in (0, 1, 2, 3, 8) for r in res[k][1])
+
+
+@pytest.mark.parametrize("op_name,lam", [("PoissonBlend", 0.0), ("ScreenedPoisson", 0.05)])
+def test_multigrid_implementation_through_the_op(ctx, L, op_name, lam):
+    """cuda.multigrid@1: the two Poisson ops through the op layer with
+    PT_FLAG_MULTIGRID (pt_op_compute_ex) return the flagged solve's candidate
+    bit for bit and SolverData from its worst channel, with steps counting CG
+    iterations -- far fewer than the default implementation's sweeps for the
+    same bar."""
+    from paintop_b200 import ops
+    cls = getattr(ops, op_name)
+    w, h, c = 120, 90, 3
+    src, tgt, mask = random_problem(41, w, h, c)
+    op = cls(multigrid=True)
+    assert op.implementation_id == "cuda.multigrid@1" and cls().implementation_id == "cuda.poisson@1"
+    names = cls.PORTS
+    inputs = {names[0]: ops.image_value(w, h, c, src), names[1]: ops.image_value(w, h, c, tgt),
+              names[2]: ops.mask_value(w, h, mask)}
+    params = {"tolerance": 1e-7, "max_iterations": 5000}
+    if lam:
+        params["lambda"] = lam
+    out = op.compute(inputs, params)
+    one, per, worst = ctx.solve(src, tgt, mask, w, h, c, lam=lam, max_iterations=5000, tolerance=1e-7,
+                                flags=L.PT_FLAG_MULTIGRID)
+    cand = np.asarray(out["candidate"].samples, np.float32)
+    assert np.array_equal(cand.view(np.uint32), one.view(np.uint32))
+    sd = out["report"].report.solver
+    assert sd.steps == sd.iterations == worst["iterations"] and sd.converged
+    assert sd.stop_reason == "converged" and sd.final_residual == worst["final_residual"] <= 1e-7
+    assert sd.residual_history == worst["residual_history"]
+    assert sd.kind == ("poisson" if lam == 0 else "screened-poisson")
+    sor = cls().compute(inputs, params)
+    assert sor["report"].report.solver.converged and sor["report"].report.solver.steps > 5 * sd.steps
+    assert np.abs(cand.astype(np.float64) - np.asarray(sor["candidate"].samples, np.float64)).max() <= 1e-4
