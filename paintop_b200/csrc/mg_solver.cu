@@ -536,15 +536,34 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_apply(const Geo *__restrict__ 
   const float *pc = p + g.oc + c * N;
   float *qc = q + g.oc + c * N;
   double acc = 0.0;
-  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
-    const size_t k = (size_t)j * W + i;
-    float v = 0.0f;
-    if (a[k]) {
-      // interior cells are never on the border: all four neighbours exist
-      v = d * pc[k] - (pc[k - 1] + pc[k + 1] + pc[k - W] + pc[k + W]);
-      acc += (double)pc[k] * (double)v;
+  // two of the tile's rows per pass, loads before stores (as in k_mg_smooth);
+  // the partial sum still takes the rows in order
+  const int step = gy * kTy;
+  for (int j0 = (b / gx) * kTy + threadIdx.y; j0 < H && i < W; j0 += 2 * step) {
+    const bool two = j0 + step < H;
+    const size_t k0 = (size_t)j0 * W + i, k1 = k0 + (size_t)step * W;
+    const bool a0 = a[k0] != 0, a1 = two && a[k1] != 0;
+    // interior cells are never on the border: all four neighbours exist
+    float c0 = 0.0f, s0 = 0.0f, c1 = 0.0f, s1 = 0.0f;
+    if (a0) {
+      c0 = pc[k0];
+      s0 = pc[k0 - 1] + pc[k0 + 1] + pc[k0 - W] + pc[k0 + W];
     }
-    qc[k] = v;
+    if (a1) {
+      c1 = pc[k1];
+      s1 = pc[k1 - 1] + pc[k1 + 1] + pc[k1 - W] + pc[k1 + W];
+    }
+    float v0 = 0.0f, v1 = 0.0f;
+    if (a0) {
+      v0 = d * c0 - s0;
+      acc += (double)c0 * (double)v0;
+    }
+    if (a1) {
+      v1 = d * c1 - s1;
+      acc += (double)c1 * (double)v1;
+    }
+    qc[k0] = v0;
+    if (two) qc[k1] = v1;
   }
   const double t = block_sum2(acc, sh);
   if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
@@ -568,9 +587,14 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_dot(const Geo *__restrict__ ge
   const size_t N = (size_t)W * H;
   const float *xc = x + g.oc + c * N, *yc = y + g.oc + c * N;
   double acc = 0.0;
-  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
-    const size_t o = (size_t)j * W + i;
-    acc += (double)xc[o] * (double)yc[o];
+  const int step = gy * kTy;
+  for (int j0 = (b / gx) * kTy + threadIdx.y; j0 < H && i < W; j0 += 2 * step) {
+    const bool two = j0 + step < H;
+    const size_t o0 = (size_t)j0 * W + i, o1 = o0 + (size_t)step * W;
+    const float x0 = xc[o0], y0 = yc[o0];
+    const float x1 = two ? xc[o1] : 0.0f, y1 = two ? yc[o1] : 0.0f;
+    acc += (double)x0 * (double)y0;
+    if (two) acc += (double)x1 * (double)y1;
   }
   const double t = block_sum2(acc, sh);
   if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
@@ -592,9 +616,16 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_direction(const Geo *__restric
   const size_t N = (size_t)W * H;
   const float *zc = z + g.oc + c * N;
   float *pc = p + g.oc + c * N;
-  for (int j = (b / g.gx) * kTy + threadIdx.y; j < H && i < W; j += g.gy * kTy) {
-    const size_t o = (size_t)j * W + i;
-    pc[o] = first ? zc[o] : zc[o] + beta * pc[o];  // first: p is not read (it holds what the arena held)
+  // first: p is not read (it holds what the arena held); two rows per pass,
+  // loads before stores
+  const int step = g.gy * kTy;
+  for (int j0 = (b / g.gx) * kTy + threadIdx.y; j0 < H && i < W; j0 += 2 * step) {
+    const bool two = j0 + step < H;
+    const size_t o0 = (size_t)j0 * W + i, o1 = o0 + (size_t)step * W;
+    const float z0 = zc[o0], z1 = two ? zc[o1] : 0.0f;
+    const float p0 = first ? 0.0f : pc[o0], p1 = (first || !two) ? 0.0f : pc[o1];
+    pc[o0] = first ? z0 : z0 + beta * p0;
+    if (two) pc[o1] = first ? z1 : z1 + beta * p1;
   }
 }
 
@@ -626,12 +657,25 @@ __global__ void __launch_bounds__(kTx * kTy) k_cg_step(const Geo *__restrict__ g
   const float *pc = p + g.oc + c * N, *qc = q + g.oc + c * N;
   float *xc = x + g.oc + c * N, *rc = r + g.oc + c * N;
   double acc = 0.0;
-  for (int j = (b / gx) * kTy + threadIdx.y; j < H && i < W; j += gy * kTy) {
-    const size_t o = (size_t)j * W + i;
-    xc[o] += alpha * pc[o];
-    const float rv = rc[o] - alpha * qc[o];
-    rc[o] = rv;
-    acc += (double)rv * (double)rv;
+  const int step = gy * kTy;  // two rows per pass, loads before stores
+  for (int j0 = (b / gx) * kTy + threadIdx.y; j0 < H && i < W; j0 += 2 * step) {
+    const bool two = j0 + step < H;
+    const size_t o0 = (size_t)j0 * W + i, o1 = o0 + (size_t)step * W;
+    const float p0 = pc[o0], q0 = qc[o0], x0 = xc[o0], r0 = rc[o0];
+    float p1 = 0.0f, q1 = 0.0f, x1 = 0.0f, r1 = 0.0f;
+    if (two) {
+      p1 = pc[o1]; q1 = qc[o1]; x1 = xc[o1]; r1 = rc[o1];
+    }
+    xc[o0] = x0 + alpha * p0;
+    const float rv0 = r0 - alpha * q0;
+    rc[o0] = rv0;
+    acc += (double)rv0 * (double)rv0;
+    if (two) {
+      xc[o1] = x1 + alpha * p1;
+      const float rv1 = r1 - alpha * q1;
+      rc[o1] = rv1;
+      acc += (double)rv1 * (double)rv1;
+    }
   }
   const double t = block_sum2(acc, sh);
   if (threadIdx.x == 0 && threadIdx.y == 0) part[g.part0 + (long long)c * gx * gy + b] = t;
