@@ -876,8 +876,11 @@ def batch_arm(args):
     dev = torch.device("cuda", local if ws > 1 else 0)
     allinst = synth.batch_uneven(1, args.batch)
     interior_all = [int((i.mask[1:-1, 1:-1] > 0.5).sum()) for i in allinst]
-    share = partition([estimate_cost(i.width, i.height, i.channels, n, n ** 0.5)
-                       for i, n in zip(allinst, interior_all)], ws)[rank]
+    if args.multigrid:  # about as many CG iterations for every size: pixels x channels
+        costs = [estimate_cost(i.width, i.height, i.channels) for i in allinst]
+    else:  # SOR sweeps grow with the region's extent
+        costs = [estimate_cost(i.width, i.height, i.channels, n, n ** 0.5) for i, n in zip(allinst, interior_all)]
+    share = partition(costs, ws)[rank]
     insts = [allinst[k] for k in share]
     n = len(insts)
     L = _lib.lib()

@@ -16,7 +16,10 @@ from typing import Callable, Sequence
 
 def estimate_cost(width: int, height: int, channels: int, interior: int | None = None,
                   sweeps: float = 1.0) -> float:
-    """Relative cost of one image: interior cells x channels x expected sweeps."""
+    """Relative cost of one image: interior cells x channels x expected sweeps.
+    For multigrid-preconditioned CG, whose iteration count hardly changes with
+    the region and whose kernels pass over every cell of the image, leave
+    `interior` and `sweeps` at their defaults: pixels x channels."""
     n = interior if interior is not None else width * height
     return float(n) * float(channels) * float(sweeps)
 
