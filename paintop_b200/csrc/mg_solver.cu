@@ -18,9 +18,10 @@
 // (4 e - sum of active neighbours) / 4^k + lambda e with zero outside the
 // active cells; prolongation is bilinear (weights 3/4, 1/4 per axis) into
 // active fine cells and restriction its transpose / 4; smoothing is red-black
-// Gauss-Seidel, red then black before the coarse correction and black then
-// red after it, so the V-cycle is a symmetric operator and a valid CG
-// preconditioner. Every reduction is a fixed-order tree, so a rerun is
+// SOR (kSmoothOmega; plain Gauss-Seidel on the coarsest level), red then black
+// before the coarse correction and black then red after it, so the V-cycle is
+// a symmetric operator and a valid CG preconditioner. The channels of an image
+// share its level masks. Every reduction is a fixed-order tree, so a rerun is
 // byte-identical.
 //
 // Batches: every problem of a call (pt_poisson_solve_batch) keeps its own
@@ -39,8 +40,8 @@
 // iteration k -- the CG recurrence's estimate scaled by the outer step's FP64
 // residual, replaced by the exact FP64 value at the end of every outer step;
 // refinements = outer steps after the first; omega_used = the smoother's
-// relaxation factor. Stop reasons: converged at the FP64 bar; max-iterations when the
-// CG iterations reach max_iterations; stalled when an outer step fails to
+// relaxation factor. Stop reasons: converged at the FP64 bar; max-iterations
+// when the CG iterations reach max_iterations; stalled when an outer step fails to
 // lower the FP64 residual, or at once (0 iterations, interior set to NaN)
 // when a NaN or infinity in the inputs makes the residual non-finite.
 #include <cuda_runtime.h>
