@@ -13,7 +13,7 @@ ELLIPSE = "mask.ellipse@1"
 POLYGON = "mask.polygon@1"
 
 
-def mask_call(op_id, params, w=8, h=8, ports=None, count=None):
+def mask_call(op_id, params, w=8, h=8, ports=None, count=None, solve_flags=None):
     from paintop_b200 import _lib
     L = _lib.lib()
     ports = {"extent_from": (0, w, h, 3, np.zeros(w * h * 3, np.float32))} if ports is None else ports
@@ -26,8 +26,9 @@ def mask_call(op_id, params, w=8, h=8, ports=None, count=None):
     n = w * h if count is None else count
     out = np.zeros(max(n, 1), np.float32)
     err = _lib.PtError()
-    st = L.pt_op_compute(None, op_id.encode(), arr, len(ports), params.encode(), out.ctypes.data, n, None,
-                         None, 0, None, C.byref(err))
+    args = (None, op_id.encode(), arr, len(ports), params.encode(), out.ctypes.data, n, None, None, 0, None,
+            C.byref(err))
+    st = L.pt_op_compute(*args) if solve_flags is None else L.pt_op_compute_ex(*args, solve_flags)
     return st, err.error_class.decode(), err.code.decode(), err.message.decode(), err.actual.decode()
 
 
@@ -113,3 +114,15 @@ def test_valid_requests_without_device_are_policy_unavailable(cuda_lib):
                        (POLYGON, '{"points": [[0, 0]]}')):
         st, cls, code, _, _ = mask_call(op, params)
         assert (st, cls, code) == (1, "policy", "E_CUDA_UNAVAILABLE")
+
+
+@pytest.mark.parametrize("op_id,params", [
+    (ELLIPSE, '{"center_px": [4, 4], "radii_px": [3, 3]}'),
+    (ELLIPSE, '{"center_px": [4, 4], "radii_px": [0, 3]}'),
+    (POLYGON, '{"points": [[1, 1], [6, 1], [4, 6]]}'),
+])
+def test_mask_ops_ignore_the_multigrid_flag(cuda_lib, op_id, params):
+    """pt_op_compute_ex: the mask generators ignore PT_FLAG_MULTIGRID (the
+    same validation, then no device)."""
+    from paintop_b200 import _lib
+    assert mask_call(op_id, params, solve_flags=_lib.PT_FLAG_MULTIGRID) == mask_call(op_id, params)
