@@ -777,6 +777,13 @@ struct Blob {
 Launch make_launch(Blob &blob, std::vector<Geo> &gs) {
   Launch l;
   l.n = (int)gs.size();
+  if (gs.size() == 1) {  // one instance: its geometry goes by value, no block map
+    gs[0].blk0 = 0;
+    l.one = gs[0];
+    l.blocks = (long long)gs[0].gx * gs[0].gy;
+    l.geo = blob.put(gs.data(), sizeof(Geo));
+    return l;
+  }
   std::vector<int4> bm;
   long long blk = 0;
   for (size_t k = 0; k < gs.size(); ++k) {
@@ -786,7 +793,6 @@ Launch make_launch(Blob &blob, std::vector<Geo> &gs) {
     blk += nb;
   }
   l.blocks = blk;
-  if (gs.size() == 1) l.one = gs[0];
   l.geo = blob.put(gs.data(), gs.size() * sizeof(Geo));
   l.bmap = blob.put(bm.data(), bm.size() * sizeof(int4));
   return l;
