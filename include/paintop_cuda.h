@@ -17,12 +17,14 @@
  *                           image per op call)
  *   pt_op_compute           replaces PoissonBlend::compute / ScreenedPoisson::compute
  *                           (poisson_blend.rs:534-600, screened_poisson.rs:361-430)
- *                           including resolve_controls / check_shapes validation,
+ *                           including resolve_controls / check_shapes validation
+ *                           (poisson_blend.rs:102-139,417-445; screened_poisson.rs:66-112),
  *                           and EllipseMask::compute / PolygonMask::compute
  *                           (ellipse.rs:506-540, mask_polygon.rs:427-452)
+ *   pt_op_compute_ex        the same ops with solve flags: PT_FLAG_MULTIGRID is a
+ *                           second implementation of the two Poisson ops
  *   pt_mask_ellipse         replaces ellipse.rs rasterize (:545-565)
  *   pt_mask_polygon         replaces mask_polygon.rs rasterize (:259-286)
- *                           (poisson_blend.rs:102-139,417-445; screened_poisson.rs:66-112)
  *   pt_status_str           message for a status code (the reference's typed
  *                           errors: crates/paintop-ir/src/error.rs:23-114)
  *
