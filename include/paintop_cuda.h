@@ -298,12 +298,20 @@ pt_status pt_autotune(pt_ctx *ctx, const pt_problem *ps, uint32_t n, uint32_t re
  *   stream:    the caller's cudaStream_t (NULL: the legacy default stream); the
  *              call returns after that stream has finished the solve.
  * Returns PT_OOM, before touching the GPU, when the problem needs more scratch
- * than PT_NOALLOC_SCRATCH_BYTES. The first call on each device (made with that
- * device current) looks up the array's device address once; make that first
- * call before any stream capture. All calls share the one array and leave their
- * contents in it; calls whose GPU work overlapped would race on it, so each call
- * holds a process-wide lock and waits for its stream before returning. Uses the
- * built-in tile configuration, never the tuned table. */
+ * than PT_NOALLOC_SCRATCH_BYTES, and PT_INVALID_ARG for the same image limits
+ * as pt_poisson_solve (width and height 1..2^30, at most 2^31 pixels and 2^34
+ * values). The first call on each device (made with that device current) looks
+ * up the array's device address once; make that first call before any stream
+ * capture. The CUDA runtime loads modules lazily, so that first call is also
+ * when the library's kernels and the array are placed on the device: the
+ * guarantee of no allocation begins with the second call on each device. The
+ * cached address is stale after cudaDeviceReset; calls after a reset are not
+ * supported. A stream that is capturing is refused with PT_INVALID_ARG, since
+ * the call copies from host memory and waits for its stream. All calls share
+ * the one array and leave their contents in it; calls whose GPU work overlapped
+ * would race on it, so each call holds a process-wide lock and waits for its
+ * stream before returning. Uses the built-in tile configuration, never the
+ * tuned table. */
 pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_candidate, pt_report *reports,
                                    double *history, void *stream);
 

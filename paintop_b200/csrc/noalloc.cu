@@ -21,7 +21,13 @@
 // symbol, not a device address. The first call on each device, with that
 // device current, asks the runtime for the array's device address with
 // cudaGetSymbolAddress and caches it; later calls on that device reuse it.
-// Make that first call before any stream capture.
+// Make that first call before any stream capture. Because the CUDA runtime
+// loads modules lazily, that first call is also when the library's kernels and
+// this array are placed on the device, which takes device memory once; the
+// promise of no allocation holds from the second call on each device. The
+// cached address belongs to the device's current context: after
+// cudaDeviceReset it is stale, and calls after a reset are not supported.
+// A stream that is capturing is refused with PT_INVALID_ARG.
 //
 // Sharing. Every call uses the same array and leaves its contents behind. A
 // call clears what must start at zero (barrier and error words, history) and
@@ -77,6 +83,12 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
   if (p->channels > kMaxChannels) return PT_INVALID_ARG;
   if (p->channels > 0 && (p->width == 0 || p->height == 0 || !p->source_or_guidance ||
                           !p->target_or_anchor || !p->mask || !out_candidate))
+    return PT_INVALID_ARG;
+  // the limits pt_poisson_solve applies; they also keep W, H and the tile
+  // counts below positive when cast to int
+  const unsigned long long px = (unsigned long long)p->width * p->height;
+  if (p->width > (1u << 30) || p->height > (1u << 30) || px > (1ull << 31) ||
+      px * (p->channels ? p->channels : 1) > (1ull << 34))
     return PT_INVALID_ARG;
   if (!std::isfinite(p->lambda) || p->lambda < 0.0 || !std::isfinite(p->tolerance) ||
       p->tolerance <= 0.0 || !std::isfinite(p->omega) || p->omega <= 0.0 || p->omega >= 2.0 ||
@@ -143,6 +155,11 @@ extern "C" pt_status pt_poisson_solve_noalloc(const pt_problem *p, float *out_ca
     return PT_NO_DEVICE;
   char *base = static_cast<char *>(g_scratch_dev[dev]);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The call copies from host stack arrays and waits for its stream, neither of
+  // which a capturing stream allows; refusing here leaves the caller's capture intact.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) { cudaGetLastError(); return PT_INVALID_ARG; }
+  if (cap != cudaStreamCaptureStatusNone) return PT_INVALID_ARG;
 
   SysDesc descs[kMaxChannels];
   for (uint32_t c = 0; c < C; ++c) {

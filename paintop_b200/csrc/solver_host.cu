@@ -58,7 +58,8 @@ pt_status validate(pt_ctx *ctx, const pt_problem &p) {
   if (p.channels > 0 && (p.width == 0 || p.height == 0))
     return fail(ctx, PT_INVALID_ARG, "width and height must be >= 1");
   const unsigned long long px = (unsigned long long)p.width * p.height;
-  if (px > (1ull << 31) || px * (p.channels ? p.channels : 1) > (1ull << 34))
+  if (p.width > (1u << 30) || p.height > (1u << 30) || px > (1ull << 31) ||
+      px * (p.channels ? p.channels : 1) > (1ull << 34))
     return fail(ctx, PT_INVALID_ARG, "image too large");
   if (p.channels > 0 && (!p.source_or_guidance || !p.target_or_anchor || !p.mask))
     return fail(ctx, PT_INVALID_ARG, "source, target and mask must be non-null");

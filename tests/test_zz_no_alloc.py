@@ -7,14 +7,13 @@ library instead. The test drives it through the C ABI twice in a row (the array
 keeps the first call's contents, so the second call shows that everything that
 must start at zero is cleared) and compares each result with pt_poisson_solve on
 the same device buffers. This file sorts last so that a stop-at-first-failure run
-has already run every other test.
+has already run every other test. The argument checks run on the CPU: every
+rejection returns before the call touches the CUDA runtime.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
-
-pytestmark = pytest.mark.gpu
 
 TOL_ABS = 1e-6  # the agreement the other GPU parity tests require between solvers
 
@@ -27,6 +26,7 @@ def _inputs(seed, size, channels):
     return src, tgt, inst.mask.reshape(-1).copy()
 
 
+@pytest.mark.gpu
 def test_noalloc_matches_solve_on_two_calls_in_a_row(cuda_lib):
     import torch
     from paintop_b200 import _lib
@@ -82,6 +82,7 @@ def test_noalloc_matches_solve_on_two_calls_in_a_row(cuda_lib):
         ctx.close()
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_problems_beyond_the_array(cuda_lib):
     import torch
     from paintop_b200 import _lib
@@ -94,3 +95,63 @@ def test_noalloc_rejects_problems_beyond_the_array(cuda_lib):
     reps = (_lib.PtReport * 5)()
     assert _lib.lib().pt_poisson_solve_noalloc(C.byref(p), buf.data_ptr(), reps, None,
                                                None) == _lib.PT_OOM
+
+
+def _problem(**kw):
+    from paintop_b200 import _lib
+    a = dict(width=64, height=64, channels=3, lam=0.0, max_it=100, tol=1e-6, omega=1.8,
+             flags=_lib.PT_FLAG_DEVICE_POINTERS, ptr=0x1000)
+    a.update(kw)
+    return _lib.PtProblem(a["width"], a["height"], a["channels"], a["ptr"], a["ptr"], a["ptr"],
+                          a["lam"], a["max_it"], a["tol"], a["omega"], a["flags"], a["ptr"])
+
+
+def _rejections():
+    from paintop_b200 import _lib
+    return [
+        ("host pointers", dict(flags=0)),
+        ("warm start", dict(flags=_lib.PT_FLAG_DEVICE_POINTERS | _lib.PT_FLAG_WARM_START)),
+        ("automatic omega", dict(flags=_lib.PT_FLAG_DEVICE_POINTERS | _lib.PT_FLAG_OMEGA_AUTO)),
+        ("nine channels", dict(channels=9)),
+        ("omega 0", dict(omega=0.0)),
+        ("omega 2", dict(omega=2.0)),
+        ("omega nan", dict(omega=float("nan"))),
+        ("negative lambda", dict(lam=-1.0)),
+        ("tolerance 0", dict(tol=0.0)),
+        ("zero width", dict(width=0)),
+        ("null buffers", dict(ptr=0)),
+        ("width 2^32-1", dict(width=0xFFFFFFFF, height=1)),
+        ("width 2^31", dict(width=1 << 31, height=1)),
+        ("2^31+ pixels", dict(width=1 << 16, height=(1 << 15) + 1)),
+        ("cap above 10^6", dict(max_it=1000001)),
+    ]
+
+
+@pytest.mark.parametrize("case", range(15))
+def test_noalloc_rejects_bad_arguments_before_the_gpu(cuda_lib, case):
+    from paintop_b200 import _lib
+    cases = _rejections()
+    assert len(cases) == 15
+    name, kw = cases[case]
+    p = _problem(**kw)
+    reps = (_lib.PtReport * 10)()
+    st = cuda_lib.pt_poisson_solve_noalloc(C.byref(p), 0x1000 if kw.get("ptr", 1) else None,
+                                           reps, None, None)
+    assert st == _lib.PT_INVALID_ARG, (name, st)
+
+
+def test_noalloc_rejects_null_problem_or_reports(cuda_lib):
+    from paintop_b200 import _lib
+    p = _problem()
+    assert cuda_lib.pt_poisson_solve_noalloc(None, 0x1000, (_lib.PtReport * 4)(), None,
+                                             None) == _lib.PT_INVALID_ARG
+    assert cuda_lib.pt_poisson_solve_noalloc(C.byref(p), 0x1000, None, None,
+                                             None) == _lib.PT_INVALID_ARG
+
+
+def test_noalloc_size_limit_is_checked_before_the_gpu(cuda_lib):
+    # 2048 x 2048 RGBA needs far more than the fixed array: PT_OOM with no CUDA call
+    from paintop_b200 import _lib
+    p = _problem(width=2048, height=2048, channels=4, max_it=2000)
+    assert cuda_lib.pt_poisson_solve_noalloc(C.byref(p), 0x1000, (_lib.PtReport * 5)(), None,
+                                             None) == _lib.PT_OOM
