@@ -1,39 +1,53 @@
-"""The Rust FFI crate written out in INTEGRATION.md cannot be compiled in this
-environment (no Rust toolchain), so its `#[repr(C)]` structs and `extern "C"`
-functions are checked against include/paintop_cuda.h here: the same fields in
-the same order with the same C types, and the same parameter lists."""
+"""The Rust FFI crate (rust/paintop-cuda) cannot be compiled in this environment
+(no Rust toolchain), so its binding, src/ffi.rs, is checked against
+include/paintop_cuda.h here: every struct of the header with the same fields in
+the same order and the same C types, every function with the same parameter
+names and types, and every constant with the header's value. The crate's two
+OpImplementations and the patches that register them are checked for the
+symbols they rely on."""
 import os
 import re
 
 from tests.test_capi import ROOT
 
 HEADER = os.path.join(ROOT, "include", "paintop_cuda.h")
-GUIDE = os.path.join(ROOT, "INTEGRATION.md")
+CRATE = os.path.join(ROOT, "rust", "paintop-cuda")
+FFI = os.path.join(CRATE, "src", "ffi.rs")
+PATCHES = os.path.join(ROOT, "rust", "patches")
 
 BASE = {"uint32_t": "u32", "int32_t": "i32", "uint64_t": "u64", "int64_t": "i64", "double": "f64",
         "float": "f32", "size_t": "usize", "char": "c_char", "int": "c_int", "void": "c_void"}
-SAME = {"c_int": {"c_int", "i32"}, "pt_status": {"pt_status", "i32", "c_int"}}
+SAME = {"c_int": {"c_int", "i32"}, "pt_status": {"pt_status"}}
 
 
-def c_source():
+def c_source(keep_defines=False):
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    if keep_defines:
+        return text
     return "\n".join(line for line in text.splitlines() if not line.lstrip().startswith("#"))
 
 
 def rust_type(ctype: str) -> str:
-    """A C type (as written in the header) in the Rust binding's spelling."""
+    """A C type (as written in the header) in the Rust binding's spelling.
+    qual[0] is the constness of the base type, qual[i] that of the i-th pointer
+    object; the i-th pointer (counted from the base) points to an object whose
+    constness is qual[i-1]."""
     toks = ctype.replace("*", " * ").split()
-    stars = toks.count("*")
-    const = "const" in toks
-    base = [t for t in toks if t not in ("*", "const", "struct")]
+    toks = [t for t in toks if t != "struct"]
+    base = [t for t in toks if t not in ("*", "const")]
     assert len(base) == 1, ctype
-    b = BASE.get(base[0], base[0])
-    if stars == 0:
-        return b
-    if stars == 1:
-        return ("*const " if const else "*mut ") + b
-    return "*mut " * stars + b
+    quals = [False]
+    for t in toks:
+        if t == "*":
+            quals.append(False)
+        elif t == "const":
+            quals[-1] = True
+    stars = len(quals) - 1
+    out = ""
+    for i in range(stars, 0, -1):
+        out += "*const " if quals[i - 1] else "*mut "
+    return out + BASE.get(base[0], base[0])
 
 
 def same(r: str, c: str) -> bool:
@@ -62,7 +76,7 @@ def c_structs():
 
 
 def c_functions():
-    """name -> (return type, [parameter types]) in the Rust spelling."""
+    """name -> (return type, [(parameter name, type)]) in the Rust spelling."""
     out = {}
     for chunk in c_source().split(";"):
         decl = " ".join(re.split(r"[{}]", chunk)[-1].split())
@@ -73,20 +87,34 @@ def c_functions():
         for p in m.group(3).split(","):
             p = p.strip()
             if p and p != "void":
-                ps.append(rust_type(re.match(r"(.*?)(\w+)$", p).group(1)))
+                pm = re.match(r"(.*?)(\w+)$", p)
+                ps.append((pm.group(2), rust_type(pm.group(1))))
         out[m.group(2)] = (rust_type(m.group(1)), ps)
     return out
 
 
-def rust_blocks():
-    text = open(GUIDE).read()
-    return "\n".join(re.findall(r"```rust\n(.*?)```", text, flags=re.S))
+def c_constants():
+    out = {}
+    for name, val in re.findall(r"#define (PT_[A-Z_0-9]+) (.+)", c_source(keep_defines=True)):
+        v = val.strip()
+        v = re.sub(r"(?<=[0-9a-fA-F])u\b", "", v)
+        try:
+            out[name] = int(eval(v, {}))
+        except Exception:
+            continue
+    for name, val in re.findall(r"\b(PT_[A-Z_]+) = (\d+)", c_source()):
+        out[name] = int(val)
+    return out
+
+
+def ffi_source():
+    return open(FFI).read()
 
 
 def test_rust_structs_match_the_header():
-    src = rust_blocks()
+    src = ffi_source()
     cs = c_structs()
-    seen = 0
+    seen = set()
     for name, body in re.findall(r"#\[repr\(C\)\] pub struct (pt_\w+) \{(.*?)\}", src, flags=re.S):
         if "_p:" in body:  # an opaque handle
             continue
@@ -95,22 +123,56 @@ def test_rust_structs_match_the_header():
         assert [f[0] for f in fields] == [f[0] for f in cs[name]], name
         for (n, rt), (_, ct) in zip(fields, cs[name]):
             assert same(rt, ct), (name, n, rt, ct)
-        seen += 1
-    assert seen >= 3
+        seen.add(name)
+    assert seen == set(cs)
 
 
 def test_rust_functions_match_the_header():
-    src = rust_blocks()
+    src = ffi_source()
     cf = c_functions()
-    seen = 0
+    seen = set()
     for name, params, ret in re.findall(r"pub fn (pt_\w+)\((.*?)\)\s*(?:->\s*([^;]+))?;", src, flags=re.S):
         assert name in cf, name
         cret, cps = cf[name]
-        rps = [" ".join(t.split()) for t in re.findall(r"\w+:\s*([^,]+)", " ".join(params.split()))]
-        assert len(rps) == len(cps), (name, rps, cps)
-        for k, (r, c) in enumerate(zip(rps, cps)):
+        rps = [(n, " ".join(t.split())) for n, t in
+               re.findall(r"(\w+):\s*([^,]+)", " ".join(params.split()))]
+        assert [n for n, _ in rps] == [n for n, _ in cps], (name, rps, cps)
+        for k, ((_, r), (_, c)) in enumerate(zip(rps, cps)):
             assert same(r, c), (name, k, r, c)
         if ret.strip():
             assert same(ret.strip(), cret), (name, ret, cret)
-        seen += 1
-    assert seen >= 8
+        seen.add(name)
+    assert seen == set(cf), sorted(set(cf) - seen)
+
+
+def test_rust_constants_match_the_header():
+    src = ffi_source()
+    cc = c_constants()
+    rc = {n: int(eval(v.replace("_", ""), {})) for n, v in
+          re.findall(r"pub const (PT_[A-Z_0-9]+): \w+ = ([0-9xX*+ a-fA-F_]+);", src)}
+    assert set(rc) == set(cc), sorted(set(cc) ^ set(rc))
+    for n, v in cc.items():
+        assert rc[n] == v, (n, rc[n], v)
+
+
+def test_crate_files_and_patches_are_complete():
+    for f in ("Cargo.toml", "build.rs", "src/ffi.rs", "src/lib.rs", "src/mask.rs"):
+        assert os.path.exists(os.path.join(CRATE, f)), f
+    lib = open(os.path.join(CRATE, "src", "lib.rs")).read()
+    mask = open(os.path.join(CRATE, "src", "mask.rs")).read()
+    for sym in ("pt_op_compute_ex", "impl OpImplementation for CudaPoisson", "PT_FLAG_MULTIGRID"):
+        assert sym in lib, sym
+    assert "impl OpImplementation for CudaMask" in mask and "pt_op_compute" in mask
+    # every ffi function the two implementations call is declared in ffi.rs
+    declared = set(re.findall(r"pub fn (pt_\w+)\(", ffi_source()))
+    for used in re.findall(r"ffi::(pt_\w+)\(", lib + mask):
+        assert used in declared, used
+    patches = {f: open(os.path.join(PATCHES, f)).read() for f in os.listdir(PATCHES)}
+    joined = "\n".join(patches.values())
+    assert 'ImplId::new("cuda", "poisson", 1)' in joined
+    assert 'ImplId::new("cuda", "multigrid", 1)' in joined
+    assert 'ImplId::new("cuda", "mask", 1)' in joined
+    assert "allowed_backends" in joined and "write_json" in joined or "to_canonical_bytes" in joined
+    for text in patches.values():  # unified diffs against the reference's own paths
+        assert re.search(r"^--- a/crates/", text, flags=re.M) and re.search(r"^\+\+\+ b/crates/", text, flags=re.M)
+        assert re.search(r"^@@ -\d+(,\d+)? \+\d+(,\d+)? @@", text, flags=re.M)
