@@ -160,8 +160,22 @@ def make_instance(seed: int):
     return synth.screened_2048(seed)
 
 
+def workload_config(inst, n_gpus: int) -> dict:
+    """The workload's `config`, the same dict on both arms."""
+    return {"workload": WORKLOAD["name"], "width": inst.width, "height": inst.height,
+            "channels": inst.channels, "lambda": WORKLOAD["lam"], "tolerance": WORKLOAD["tolerance"],
+            "max_iterations": WORKLOAD["max_iterations"], "omega": WORKLOAD["omega"],
+            "interior_px": int((inst.mask[1:-1, 1:-1] > 0.5).sum()),
+            "l2": "inputs larger than L2 (151 MB/solve)",
+            "parallelism": f"instances sharded over {n_gpus} GPU(s)"}
+
+
 def reference_arm(args):
-    """CPU arm: the oracle restatement of the reference op, single thread."""
+    """CPU arm: the oracle restatement of the reference op, single thread (the
+    reference solves channels one after another, poisson_blend.rs:168-236, and
+    its FullDomain op is not tiled). One step is one channel solve of the
+    workload (channels rotate); a solve costs the sum of its channel solves, so
+    solves/s = 1 / (channels x mean step time)."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
@@ -172,53 +186,99 @@ def reference_arm(args):
     src = inst.source.reshape(-1)
     tgt = inst.target.reshape(-1)
     mask = inst.mask.reshape(-1)
-    # one channel per step: the reference solves channels serially and
-    # independently, so a solve costs the sum of its channel solves
     chans = [np.ascontiguousarray(x.reshape(H, W, C)[:, :, k]).reshape(-1)
              for x in (src, tgt) for k in range(C)]
     srcs, tgts = chans[:C], chans[C:]
+    sweeps, converged = {}, {}
 
     def step(k):
         c = k % C
         t0 = time.perf_counter()
-        O.blend_channels(srcs[c], tgts[c], mask, 1, W, H, WORKLOAD["max_iterations"],
-                         WORKLOAD["tolerance"], WORKLOAD["lam"], WORKLOAD["omega"])
-        return time.perf_counter() - t0
+        _, worst, per = O.blend_channels(srcs[c], tgts[c], mask, 1, W, H, WORKLOAD["max_iterations"],
+                                         WORKLOAD["tolerance"], WORKLOAD["lam"], WORKLOAD["omega"])
+        dt = time.perf_counter() - t0
+        sweeps[c], converged[c] = int(per[0].iterations), bool(worst.converged)
+        return dt
 
     for k in range(args.warmup):
         step(k)
     times = [step(args.warmup + k) for k in range(args.steps)]
     per_channel = float(np.mean(times))
     value = 1.0 / (C * per_channel)
-    sample = (f"one channel of the {W}x{H}x{C} solve per step (channels rotate), "
-              f"solve time = {C} x mean channel time")
+    sample = (f"one channel of the {W}x{H}x{C} solve per step (channels rotate); "
+              f"solves/s = 1 / ({C} x mean step time)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_channel * C * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_channel * 1e3,
+        "step": f"one channel solve; one {UNIT[:-2]} = {C} channel solves",
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sinusoid-plus-noise images, star polygon mask)",
-        "config": {"workload": WORKLOAD["name"], **{k: v for k, v in WORKLOAD.items()
-                                                      if k != "name"}},
+        "config": workload_config(inst, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "solver": {"sweeps_per_channel": [sweeps.get(c) for c in range(C)],
+                   "channels_solved": sorted(converged), "converged": all(converged.values())},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def cpu_baseline_sample(inst):
-    """Time one full solve (all channels) of the oracle on one host core."""
+# the reference's bounded tier (crates/paintop-testkit/src/differential.rs:58-62)
+BOUNDED_MAX_ABS, BOUNDED_RMS = 1e-4, 1e-5
+
+
+def error_stats(got, want) -> dict:
+    """max |got - want| and the RMS over all samples (the reference's ErrorMap)."""
+    d = np.asarray(got, dtype=np.float64).reshape(-1) - np.asarray(want, dtype=np.float64).reshape(-1)
+    mx, rms = float(np.abs(d).max()), float(np.sqrt(np.mean(d * d)))
+    return {"max_abs": mx, "rms": rms, "within_bounded_tier": mx <= BOUNDED_MAX_ABS and rms <= BOUNDED_RMS}
+
+
+def tight_oracle(inst, lam: float):
+    """The FP64 tight oracle on the host cores: multigrid-preconditioned CG to
+    relative residual 1e-12 (oracle/mgcg_ref.c, all threads OpenMP gives it)."""
+    from oracle import oracle as O
+    O.build()
+    t0 = time.perf_counter()
+    tight, ach, its = O.mgcg_blend_channels(inst.source.reshape(-1), inst.target.reshape(-1),
+                                            inst.mask.reshape(-1), inst.channels, inst.width,
+                                            inst.height, lam=lam, rel_tol=1e-12)
+    return tight, {"method": "FP64 multigrid-preconditioned CG", "rel_res": [float(x) for x in ach],
+                   "iterations": [int(x) for x in its], "seconds": time.perf_counter() - t0,
+                   "threads": os.cpu_count()}
+
+
+def cpu_baseline_sample(inst, gpu_out=None, gpu_outs=None):
+    """CPU baseline leg: time one full solve (all channels) of the restated
+    reference op on one host core. With the GPU's output of the same inputs it
+    also states the GPU's error against that CPU output and against the FP64
+    tight oracle, and the CPU op's own error against the oracle.
+    gpu_outs: further GPU outputs of the same inputs, by name."""
     from oracle import oracle as O
     O.build()
     W, H, C = inst.width, inst.height, inst.channels
     t0 = time.perf_counter()
-    O.blend_channels(inst.source.reshape(-1), inst.target.reshape(-1), inst.mask.reshape(-1), C,
-                     W, H, WORKLOAD["max_iterations"], WORKLOAD["tolerance"], WORKLOAD["lam"],
-                     WORKLOAD["omega"])
+    ref, worst, per = O.blend_channels(inst.source.reshape(-1), inst.target.reshape(-1),
+                                       inst.mask.reshape(-1), C, W, H, WORKLOAD["max_iterations"],
+                                       WORKLOAD["tolerance"], WORKLOAD["lam"], WORKLOAD["omega"])
     dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"one full {W}x{H}x{C} solve ({dt:.1f} s) of the restated reference op"}
+    cpu = {"value": 1.0 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+           "sample": f"one full {W}x{H}x{C} solve ({dt:.1f} s) of the restated reference op",
+           "converged": bool(worst.converged), "sweeps": [int(r.iterations) for r in per]}
+    if gpu_out is None:
+        return cpu, None
+    tight, info = tight_oracle(inst, WORKLOAD["lam"])
+    parity = {"bounded_tier": {"max_abs": BOUNDED_MAX_ABS, "rms": BOUNDED_RMS,
+                               "source": "crates/paintop-testkit/src/differential.rs:58-62"},
+              "oracle": info,
+              "cpu_op_vs_oracle": error_stats(ref, tight),
+              "sor_vs_oracle": error_stats(gpu_out, tight),
+              "sor_vs_cpu_op": error_stats(gpu_out, ref)}
+    for name, out in (gpu_outs or {}).items():
+        parity[f"{name}_vs_oracle"] = error_stats(out, tight)
+        parity[f"{name}_vs_cpu_op"] = error_stats(out, ref)
+    return cpu, parity
 
 
 def mask_leg(ctx, dev, peak_gbs, reps: int = 20):
@@ -770,6 +830,7 @@ def gpu_arm(args):
     clocks = sampler.stop()
     converged = all(reps[c].converged for c in range(C))
     worst_res = max(reps[c].final_residual for c in range(C))
+    sor_out = out_d.cpu().numpy()  # the last timed solve's result, for the parity statement
 
     # ---- end-to-end arm (pinned host buffers through the C ABI) --------------
     e2e_elapsed = float("nan")
@@ -806,9 +867,10 @@ def gpu_arm(args):
     learned = None
     if ws == 1 and not args.no_learned and not args.device_only:
         learned = learned_leg(ctx, dev, with_cpu=not args.no_cpu_baseline)  # reported apart, outside the timed region
-    multigrid = None
+    multigrid, mg_out = None, None
     if ws == 1 and not args.device_only:
         multigrid = multigrid_leg(ctx, dev, inst)
+        mg_out = multigrid.pop("_out")
     mask_raster = None
     if ws == 1 and not args.device_only:
         mask_raster = mask_leg(ctx, dev, peak)
@@ -817,19 +879,16 @@ def gpu_arm(args):
 
     line = None
     if rank == 0:
-        cpu = cpu_baseline_sample(inst) if (ws == 1 and not args.no_cpu_baseline and
-                                             not args.device_only) else None
+        cpu, parity = None, None
+        if ws == 1 and not args.no_cpu_baseline and not args.device_only:
+            cpu, parity = cpu_baseline_sample(
+                inst, sor_out, {"multigrid": mg_out} if mg_out is not None else None)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded sinusoid-plus-noise images, star polygon mask)",
-            "config": {"workload": WORKLOAD["name"], "width": W, "height": H, "channels": C,
-                       "lambda": WORKLOAD["lam"], "tolerance": WORKLOAD["tolerance"],
-                       "max_iterations": WORKLOAD["max_iterations"], "omega": WORKLOAD["omega"],
-                       "interior_px": interior, "l2": "inputs larger than L2 (151 MB/solve)",
-                       "tile_config": ctx.last_config(),
-                       "parallelism": f"instances sharded over {ws} GPU(s)"},
+            "config": workload_config(inst, ws),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -838,10 +897,12 @@ def gpu_arm(args):
                          "kernel_ms_mean": float(kms.mean()),
                          "algorithmic_bytes_per_launch": float(alg_bytes.mean())},
             "cpu_baseline": cpu,
+            "parity": parity,
             "gpu_launches": launches,
             "clocks": clocks,
             "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
-                       "converged": converged, "worst_final_residual": worst_res},
+                       "converged": converged, "worst_final_residual": worst_res,
+                       "tile_config": ctx.last_config()},
             "multigrid": multigrid,
             "learned_warm_start": learned,
             "mask_raster": mask_raster,
@@ -1065,7 +1126,7 @@ def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8, with_
         return [int(reps[c].iterations) for c in range(C)], all(reps[c].converged for c in range(C)), \
             [bool(reps[c].warm_start) for c in range(C)]
 
-    res = {}
+    res, outs = {}, {}
     for mode in problems:
         for _ in range(warmup):
             run(mode)
@@ -1077,11 +1138,12 @@ def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8, with_
         e1.record(stream)
         e1.synchronize()
         sec = e0.elapsed_time(e1) / 1e3 / steps
+        outs[mode] = out.cpu().numpy()
         key = "sweeps" if mode in ("plain", "learned") else "cg_iterations"
         res[mode] = dict(solves_per_s=1.0 / sec, ms_per_solve=sec * 1e3, **{key: its}, converged=conv,
                          **({"guess_used": used} if mode.startswith("learned") else {}))
     net.close()
-    cpu = None
+    cpu, parity = None, None
     if with_cpu:
         # the restated reference op on one core: 20 sweeps of one channel give its
         # rate; a full solve (three channels, over a thousand sweeps each) is far
@@ -1096,13 +1158,20 @@ def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8, with_
                "status": "> budget" if per_sweep * 1000 * C > 60.0 else "within budget",
                "lower_bound_s_per_solve": per_sweep * 1000 * C, "cores": 1, "kind": "port",
                "sample": "20 sweeps (each with its FP64 residual) of channel 0; bound assumes 1000 sweeps per channel"}
+        # every timed path's result against the FP64 tight oracle (the CPU op's
+        # full solve is beyond the budget above, so it is not a comparison here)
+        tight, info = tight_oracle(inst, 0.0)
+        parity = {"bounded_tier": {"max_abs": BOUNDED_MAX_ABS, "rms": BOUNDED_RMS,
+                                          "source": "crates/paintop-testkit/src/differential.rs:58-62"},
+                         "oracle": info,
+                         **{f"{mode}_vs_oracle": error_stats(o, tight) for mode, o in outs.items()}}
     return {"workload": "multi_4096: 4096x4096 RGB, 8 polygons 3-10% each, rel-res 1e-6, automatic omega for SOR",
             "model": "U-Net 16-32-64-128, bf16, trained on 20,000 256x256 solves; inference pooled x%d" % scale,
             "steps": steps, **res,
             "speedup": res["learned"]["solves_per_s"] / res["plain"]["solves_per_s"],
             "speedup_multigrid": res["multigrid"]["solves_per_s"] / res["plain"]["solves_per_s"],
             "speedup_learned_multigrid": res["learned_multigrid"]["solves_per_s"] / res["multigrid"]["solves_per_s"],
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "parity": parity}
 
 
 def multigrid_leg(ctx, dev, inst, steps: int = 3, warmup: int = 1):
@@ -1142,7 +1211,7 @@ def multigrid_leg(ctx, dev, inst, steps: int = 3, warmup: int = 1):
             "refinements": [int(reps[c].refinements) for c in range(C)],
             "converged": all(reps[c].converged for c in range(C)),
             "worst_final_residual": max(reps[c].final_residual for c in range(C)),
-            "launches_per_solve": ctx.last_timing()[2]}
+            "launches_per_solve": ctx.last_timing()[2], "_out": out.cpu().numpy()}
 
 
 def main():

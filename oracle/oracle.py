@@ -104,6 +104,10 @@ def lib():
                                            C.c_size_t, C.c_size_t, C.c_double, C.c_double,
                                            C.c_uint32, C.c_void_p, C.c_void_p]
         L.pr_cg_blend_channels.restype = C.c_int
+        L.pr_mgcg_blend_channels.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                             C.c_size_t, C.c_size_t, C.c_double, C.c_double,
+                                             C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.pr_mgcg_blend_channels.restype = C.c_int
         L.pr_rb_blend_channels.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                            C.c_size_t, C.c_size_t, _Controls, C.c_double,
                                            C.c_void_p, C.POINTER(_Report), C.c_void_p]
@@ -228,6 +232,25 @@ def cg_blend_channels(source, target, mask, channels, width, height, lam=0.0, re
     if it < 0:
         raise MemoryError("oracle allocation failed")
     return out, ach[:channels]
+
+
+def mgcg_blend_channels(source, target, mask, channels, width, height, lam=0.0, rel_tol=1e-12,
+                        max_iterations=2000):
+    """FP64 multigrid-preconditioned CG tight oracle for large systems (mgcg_ref.c)
+    -> (field f64 interleaved, achieved rel-res per channel, iterations per channel)."""
+    source = np.ascontiguousarray(source, dtype=np.float32).reshape(-1)
+    target = np.ascontiguousarray(target, dtype=np.float32).reshape(-1)
+    mask = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1)
+    n = width * height
+    out = np.empty(n * channels, dtype=np.float64)
+    ach = np.zeros(max(channels, 1), dtype=np.float64)
+    its = np.zeros(max(channels, 1), dtype=np.uint32)
+    rc = lib().pr_mgcg_blend_channels(_p(source), _p(target), _p(mask), channels, width, height,
+                                      float(lam), float(rel_tol), int(max_iterations), _p(out),
+                                      _p(ach), _p(its))
+    if rc < 0:
+        raise MemoryError("oracle allocation failed")
+    return out, ach[:channels], its[:channels]
 
 
 def mask_ellipse(width, height, center, radii, angle_rad=0.0, half_width_px=0.0) -> np.ndarray:

@@ -66,6 +66,16 @@ int pr_cg_blend_channels(const float *source, const float *target, const float *
                          double rel_tol, uint32_t max_iterations, double *out_f64,
                          double *achieved);
 
+/* FP64 CG preconditioned by an aggregation multigrid V-cycle, to
+ * ||r|| <= rel_tol * ||r(anchor)||; initial (nullable) seeds the interior.
+ * Returns iterations or -1 (OOM). */
+int pr_mgcg_solve(const pr_system *s, double rel_tol, uint32_t max_iterations,
+                  const double *initial, double *field, double *achieved);
+int pr_mgcg_blend_channels(const float *source, const float *target, const float *mask,
+                           size_t channels, size_t width, size_t height, double lambda,
+                           double rel_tol, uint32_t max_iterations, double *out_f64,
+                           double *achieved, uint32_t *iterations);
+
 /* FP64 red-black SOR (the GPU method in FP64): same controls and report. */
 void pr_rb_solve(const pr_system *s, pr_controls c, double *field, double *history,
                  pr_report *rep);

@@ -24,6 +24,15 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] == 1
     assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"] == "screened_2048"
+    # the GPU arm's config dict, key for key
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.workload_config(bench.make_instance(1), 1)
+    # a step is one channel solve, and the line's time is the step's own
+    ch = d["config"]["channels"]
+    assert abs(d["ms_per_step"] * ch / 1e3 - 1.0 / d["value"]) <= 1e-9 / d["value"]
+    assert d["solver"]["converged"] is True
+    assert d["solver"]["sweeps_per_channel"][0] < d["config"]["max_iterations"]
 
 
 def test_reference_arm_other_ranks_exit_quietly():
