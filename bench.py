@@ -24,6 +24,13 @@ Arms:
                      256x256 (``train_arm``).
   --workload clone_512  the reference's CPU-runnable 512x512 RGB clone, seeds
                      1-5, beside the restated op on one core (``clone_arm``).
+  batch_uneven       (N=1) the 256-instance uneven RGB batch, red-black SOR in one
+                     persistent launch and multigrid-CG with every instance in each
+                     launch (``batch_leg``), tile configuration from the table.
+  train              (N=1) one U-Net training step, batch 64 of 256x256
+                     (``train_leg``).
+  parity             (N=1, CPU baseline leg) max |err| and RMS of the GPU results
+                     against the FP64 tight oracle and the restated reference op.
   mask_raster        (N=1) the workloads' polygon masks rasterised on the device
                      (mask.polygon@1 semantics, ``mask_leg``) beside the
                      oracle's single-core rasteriser.
@@ -876,6 +883,10 @@ def gpu_arm(args):
         mask_raster = mask_leg(ctx, dev, peak)
         if not args.no_cpu_baseline:
             mask_raster["cpu_baseline"] = mask_cpu_baseline()
+    batch_uneven, train = None, None
+    if ws == 1 and not args.device_only:
+        batch_uneven = batch_leg(ctx, dev)
+        train = train_leg(ctx, dev)
 
     line = None
     if rank == 0:
@@ -902,10 +913,14 @@ def gpu_arm(args):
             "clocks": clocks,
             "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
                        "converged": converged, "worst_final_residual": worst_res,
-                       "tile_config": ctx.last_config()},
+                       "tile_config": tile_config_label(ctx.last_config()),
+                       "tuned_entry": tuned_entry([dict(width=W, height=H, channels=C,
+                                                        lam=WORKLOAD["lam"])])},
             "multigrid": multigrid,
             "learned_warm_start": learned,
             "mask_raster": mask_raster,
+            "batch_uneven": batch_uneven,
+            "train": train,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -916,36 +931,16 @@ def gpu_arm(args):
     return 0
 
 
-def batch_arm(args):
-    """Batched uneven workload: 256 RGB instances, side log-uniform in [64, 1024],
-    aspect in [0.5, 2], ellipse masks covering 20-60%, tol 1e-6, automatic omega,
-    solved in one persistent launch per batch (graph-replayed). A step = the batch.
-    With --multigrid the same batch goes through multigrid-preconditioned CG
-    (PT_FLAG_MULTIGRID), every instance in each launch."""
+def measure_batch(ctx, dev, insts, interior, steps: int, warmup: int, multigrid: bool,
+                  sync=None, max_over_ranks=None, with_e2e: bool = True) -> dict:
+    """Solve a batch of instances in one pt_poisson_solve_batch call per step:
+    device-resident (`elapsed`) and through pinned host buffers (`e2e_elapsed`),
+    CUDA events on the context stream. Returns the timings, reports and bytes."""
     import ctypes as Ct
     import torch
-    from paintop_b200 import _lib, synth
-    from paintop_b200.shard import estimate_cost, partition
-    ws, rank, local = _dist()
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
-    dev = torch.device("cuda", local if ws > 1 else 0)
-    allinst = synth.batch_uneven(1, args.batch)
-    interior_all = [int((i.mask[1:-1, 1:-1] > 0.5).sum()) for i in allinst]
-    if args.multigrid:  # about as many CG iterations for every size: pixels x channels
-        costs = [estimate_cost(i.width, i.height, i.channels) for i in allinst]
-    else:  # SOR sweeps grow with the region's extent
-        costs = [estimate_cost(i.width, i.height, i.channels, n, n ** 0.5) for i, n in zip(allinst, interior_all)]
-    share = partition(costs, ws)[rank]
-    insts = [allinst[k] for k in share]
+    from paintop_b200 import _lib
     n = len(insts)
     L = _lib.lib()
-    ctx = _lib.Context(dev.index)
     keep = []
     probs_d = (_lib.PtProblem * n)()
     probs_h = (_lib.PtProblem * n)()
@@ -953,7 +948,7 @@ def batch_arm(args):
     outs_h = (Ct.c_void_p * n)()
     rep_arr = [(_lib.PtReport * (i.channels + 1))() for i in insts]
     rep_ptrs = (Ct.POINTER(_lib.PtReport) * n)(*[Ct.cast(r, Ct.POINTER(_lib.PtReport)) for r in rep_arr])
-    flags = _lib.PT_FLAG_MULTIGRID if args.multigrid else _lib.PT_FLAG_OMEGA_AUTO
+    flags = _lib.PT_FLAG_MULTIGRID if multigrid else _lib.PT_FLAG_OMEGA_AUTO
     h2d = d2h = 0
     for k, inst in enumerate(insts):
         sh = torch.from_numpy(inst.source.reshape(-1)).pin_memory()
@@ -983,63 +978,226 @@ def batch_arm(args):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
 
     def timed(device_ptrs):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             solve(device_ptrs)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        if sync:
+            sync()
         torch.cuda.synchronize(dev)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        kms = []
+        kms, launches = [], 0
         a.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             solve(device_ptrs)
             kms.append(ctx.last_timing()[0])
+            launches += ctx.last_timing()[2]
         b.record(stream)
         b.synchronize()
         el = a.elapsed_time(b) / 1e3
-        if ws > 1:
-            import torch.distributed as dist
-            t = torch.tensor([el], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        return el, kms
+        return (max_over_ranks(el) if max_over_ranks else el), kms, launches
 
     sampler = ClockSampler(dev.index)
     sampler.start()
-    elapsed, kms = timed(True)
+    elapsed, kms, launches = timed(True)
     clocks = sampler.stop()
-    e2e_elapsed, _ = timed(False)
+    e2e_elapsed = timed(False)[0] if with_e2e else float("nan")
     iters = [[r[c].iterations for c in range(i.channels)] for r, i in zip(rep_arr, insts)]
     conv = all(r[c].converged for r, i in zip(rep_arr, insts) for c in range(i.channels))
-    if args.multigrid:
+    if multigrid:
         # the multigrid model: 155 B per level-0 cell and channel per CG
         # iteration, a third more for the coarser levels (multigrid_arm)
         alg = sum(155.0 * 4.0 / 3.0 * i.width * i.height * sum(it) for it, i in zip(iters, insts))
     else:
         alg = sum(n_int * (BYTES_PER_SWEEP * sum(it) + BYTES_PER_RESIDUAL * (
             sum(it) + sum(r[c].refinements for c in range(i.channels))))
-            for n_int, it, r, i in zip([interior_all[k] for k in share], iters, rep_arr, insts))
+            for n_int, it, r, i in zip(interior, iters, rep_arr, insts))
+    return dict(elapsed=elapsed, e2e_elapsed=e2e_elapsed, kms=kms, launches=launches, clocks=clocks,
+                iters=iters, conv=conv, alg=alg, h2d=h2d, d2h=d2h, reps=rep_arr,
+                omegas=[float(r[0].omega_used) for r in rep_arr], config=ctx.last_config())
+
+
+def tile_config_label(cfg: int):
+    if cfg is None or cfg < 0:
+        return None
+    import ctypes as Ct
+    from paintop_b200 import _lib
+    s, w, h = Ct.c_int32(), Ct.c_int32(), Ct.c_int32()
+    _lib.lib().pt_tile_config_info(cfg, Ct.byref(s), Ct.byref(w), Ct.byref(h))
+    return {"index": cfg, "sweeps_per_step": s.value, "tile_w": w.value, "tile_h": h.value}
+
+
+def tuned_entry(problems) -> dict:
+    """The compiled-in B200 table's entry for these problems' shape key, if any
+    (paintop_b200/csrc/tune_table_b200.inc, written by paintop_b200.tune)."""
+    import re
+    from paintop_b200 import tune
+    key = tune.shape_key(problems)
+    text = open(tune.INC).read()
+    for k, v in re.findall(r"\{0x([0-9a-f]{8})u, (\d+)\}", text):
+        if int(k, 16) == key:
+            return {"key": f"0x{key:08x}", "config": int(v), "source": "compiled-in B200 table"}
+    return {"key": f"0x{key:08x}", "config": None, "source": "built-in rule (no tuned entry)"}
+
+
+def batch_cpu_sample(insts, rep_arr, multigrid: bool) -> dict:
+    """CPU baseline leg of the batch: the restated reference op on one host core
+    over 8 instances spread across the size range."""
+    from oracle import oracle as O
+    O.build()
+    n = len(insts)
+    order = sorted(range(n), key=lambda k: insts[k].width * insts[k].height)
+    sample = order[::max(1, n // 8)][:8]
+    t0 = time.perf_counter()
+    for k in sample:
+        i = insts[k]
+        om = 1.8 if multigrid else float(rep_arr[k][0].omega_used)
+        O.blend_channels(i.source.reshape(-1), i.target.reshape(-1), i.mask.reshape(-1),
+                         i.channels, i.width, i.height, 100000, 1e-6, 0.0, om)
+    dt = time.perf_counter() - t0
+    return {"value": len(sample) / dt, "unit": "instances/s", "cores": 1, "kind": "port",
+            "sample": f"{len(sample)} instances spread over the size range ({dt:.1f} s), "
+                      + ("row-major SOR at the op's omega 1.8" if multigrid else
+                         "row-major SOR at the omega the GPU chose")}
+
+
+def batch_leg(ctx, dev, steps: int = 3, warmup: int = 1) -> dict:
+    """The 256-instance uneven RGB batch in the default run (N=1): red-black
+    SOR in one persistent launch per batch, and multigrid-CG with every instance
+    in each launch, device-resident, CUDA events; tile configuration from the
+    table."""
+    from paintop_b200 import synth
+    insts = synth.batch_uneven(1, 256)
+    interior = [int((i.mask[1:-1, 1:-1] > 0.5).sum()) for i in insts]
+    peak, peak_kind = _peaks()
+    out = {"workload": "batch_uneven: 256 RGB instances, side log-uniform in [64, 1024], aspect [0.5, 2], "
+                       "ellipse masks 20-60%, rel-res 1e-6", "steps": steps}
+    probs = [dict(width=i.width, height=i.height, channels=i.channels, lam=0.0) for i in insts]
+    for mg in (False, True):
+        r = measure_batch(ctx, dev, insts, interior, steps, warmup, mg, with_e2e=False)
+        kmean = float(np.mean(r["kms"]))
+        out["multigrid" if mg else "sor"] = {
+            "instances_per_s": len(insts) * steps / r["elapsed"], "ms_per_batch": r["elapsed"] / steps * 1e3,
+            "converged": r["conv"], "max_iterations": int(max(max(x) for x in r["iters"])),
+            "roofline": {"bound": "hbm", "achieved": r["alg"] / (kmean / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": r["alg"] / (kmean / 1e3) / 1e9 / peak,
+                         "peak_kind": peak_kind,
+                         "kernel": "multigrid-CG iteration (modelled bytes)" if mg else "ptk::k_solve"},
+            "gpu_launches_per_batch": r["launches"] // max(1, steps), "clocks": r["clocks"],
+            **({} if mg else {"tile_config": tile_config_label(r["config"]),
+                              "tuned_entry": tuned_entry(probs)}),
+        }
+    out["speedup_multigrid"] = out["multigrid"]["instances_per_s"] / out["sor"]["instances_per_s"]
+    return out
+
+
+def train_leg(ctx, dev, steps: int = 10, warmup: int = 3) -> dict:
+    """One U-Net training step (batch 64 of 256x256, forward + backward + Adam)
+    in the default run (N=1), CUDA events on the context stream."""
+    import ctypes as Ct
+    import torch
+    from paintop_b200 import _lib, warmstart as wsm
+    B, S = 64, 256
+    net = wsm.UNet(ctx, seed=0)
+    try:
+        g, a, m = wsm.make_instances(B, S, seed=3)
+        f = net.features(g, a, m)
+        lm = wsm.interior_mask(m)
+        t = (a - g).contiguous()
+        loss = Ct.c_double()
+        L = _lib.lib()
+
+        def step():
+            st = L.pt_unet_train_step(net.h, f.data_ptr(), t.data_ptr(), lm.data_ptr(), B, S, S,
+                                      Ct.c_float(1e-3), Ct.byref(loss))
+            if st != _lib.PT_OK:
+                raise _lib.CudaError(st, ctx.last_error())
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+        sampler = ClockSampler(dev.index)
+        sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        clocks = sampler.stop()
+    finally:
+        net.close()
+    step_s = e0.elapsed_time(e1) / 1e3 / steps
+    flops = wsm.train_flops_per_pixel() * B * S * S
+    peak, peak_kind = _bf16_peak()
+    return {"workload": "unet_train_b64_256: batch 64 of 256x256, bf16 weights, fp32 accumulate, Adam",
+            "steps": steps, "samples_per_s": B / step_s, "ms_per_step": step_s * 1e3,
+            "roofline": {"bound": "tensor", "achieved": flops / step_s / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": flops / step_s / 1e12 / peak, "peak_kind": peak_kind,
+                         "kernel": "whole training step"},
+            "loss_last": loss.value, "clocks": clocks}
+
+
+def _bf16_peak():
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        with open(pk_path) as fh:
+            pk = json.load(fh)
+        return (float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))),
+                "measured (sustained: a step loop lasts seconds)")
+    return 1400.0, "fallback (sustained bf16 figure of earlier measurements on this hardware)"
+
+
+def batch_arm(args):
+    """Batched uneven workload: 256 RGB instances, side log-uniform in [64, 1024],
+    aspect in [0.5, 2], ellipse masks covering 20-60%, tol 1e-6, automatic omega,
+    solved in one persistent launch per batch (graph-replayed). A step = the batch.
+    With --multigrid the same batch goes through multigrid-preconditioned CG
+    (PT_FLAG_MULTIGRID), every instance in each launch."""
+    import torch
+    from paintop_b200 import _lib, synth
+    from paintop_b200.shard import estimate_cost, partition
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    allinst = synth.batch_uneven(1, args.batch)
+    interior_all = [int((i.mask[1:-1, 1:-1] > 0.5).sum()) for i in allinst]
+    if args.multigrid:  # about as many CG iterations for every size: pixels x channels
+        costs = [estimate_cost(i.width, i.height, i.channels) for i in allinst]
+    else:  # SOR sweeps grow with the region's extent
+        costs = [estimate_cost(i.width, i.height, i.channels, n, n ** 0.5) for i, n in zip(allinst, interior_all)]
+    share = partition(costs, ws)[rank]
+    insts = [allinst[k] for k in share]
+    ctx = _lib.Context(dev.index)
+
+    def sync():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(el):
+        if ws == 1:
+            return el
+        import torch.distributed as dist
+        t = torch.tensor([el], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    r = measure_batch(ctx, dev, insts, [interior_all[k] for k in share], args.steps, args.warmup,
+                      args.multigrid, sync=sync, max_over_ranks=max_over_ranks)
+    elapsed, e2e_elapsed, kms, iters, conv, alg = (r["elapsed"], r["e2e_elapsed"], r["kms"], r["iters"],
+                                                   r["conv"], r["alg"])
     total = len(allinst)
     line = None
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            from oracle import oracle as O
-            O.build()
-            order = sorted(range(n), key=lambda k: insts[k].width * insts[k].height)
-            sample = order[::max(1, n // 8)][:8]
-            t0 = time.perf_counter()
-            for k in sample:
-                i = insts[k]
-                om = 1.8 if args.multigrid else float(rep_arr[k][0].omega_used)
-                O.blend_channels(i.source.reshape(-1), i.target.reshape(-1), i.mask.reshape(-1),
-                                 i.channels, i.width, i.height, 100000, 1e-6, 0.0, om)
-            dt = time.perf_counter() - t0
-            cpu = {"value": len(sample) / dt, "unit": "instances/s", "cores": 1, "kind": "port",
-                   "sample": f"{len(sample)} instances spread over the size range ({dt:.1f} s), "
-                             + ("row-major SOR at the op's omega 1.8" if args.multigrid else
-                                "row-major SOR at the omega the GPU chose")}
+            cpu = batch_cpu_sample(insts, r["reps"], args.multigrid)
         peak, peak_kind = _peaks()
         kmean = float(np.mean(kms))
         line = {
@@ -1053,18 +1211,18 @@ def batch_arm(args):
             "config": {"workload": "batch_uneven", "instances": total, "tolerance": 1e-6,
                        "omega": "smoother 1.25" if args.multigrid else "automatic (device, per channel)",
                        "solver": "multigrid-CG" if args.multigrid else "red-black SOR",
-                       "tile_config": None if args.multigrid else ctx.last_config(),
                        "l2": "inputs larger than L2"},
             "e2e": {"value": total * args.steps / e2e_elapsed, "unit": "instances/s",
-                    "h2d_bytes_per_step": h2d * ws, "d2h_bytes_per_step": d2h * ws},
+                    "h2d_bytes_per_step": r["h2d"] * ws, "d2h_bytes_per_step": r["d2h"] * ws},
             "roofline": {"bound": "hbm", "achieved": alg / (kmean / 1e3) / 1e9, "peak": peak,
                          "unit": "GB/s", "frac": alg / (kmean / 1e3) / 1e9 / peak, "traffic": None,
                          "kernel": "multigrid-CG iteration (all kernels, modelled bytes)" if args.multigrid
                          else "ptk::k_solve", "peak_kind": peak_kind, "kernel_ms_mean": kmean},
-            "cpu_baseline": cpu, "gpu_launches": int(args.steps * ctx.last_timing()[2]),
-            "clocks": clocks,
+            "cpu_baseline": cpu, "gpu_launches": int(r["launches"]),
+            "clocks": r["clocks"],
             "solver": {"converged": conv, "max_iterations": int(max(max(x) for x in iters)),
-                       "sum_iterations": int(sum(sum(x) for x in iters))},
+                       "sum_iterations": int(sum(sum(x) for x in iters)),
+                       "tile_config": None if args.multigrid else tile_config_label(r["config"])},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -198,6 +198,7 @@ class Context:
         if st != PT_OK:
             raise CudaError(st, "pt_ctx_create")
         self.h = h
+        self.device = int(device)
         self._children = weakref.WeakSet()  # objects whose C handles point into this context
 
     def adopt(self, child) -> None:

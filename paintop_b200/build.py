@@ -42,7 +42,7 @@ def _stale(obj: str, deps: list[str]) -> bool:
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     headers = [os.path.join(d, f) for d in (CSRC, os.path.join(CSRC, "unet")) for f in os.listdir(d)
-               if f.endswith((".h", ".cuh"))]
+               if f.endswith((".h", ".cuh", ".inc"))]
     headers.append(os.path.join(ROOT, "include", "paintop_cuda.h"))
     objs = []
     changed = force

@@ -68,12 +68,13 @@ __device__ __forceinline__ unsigned long long now_ns() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait on an mbarrier phase (wall-clock limit).
-__device__ __forceinline__ bool wait_phase(uint64_t *mbar, uint32_t parity) {
+// Bounded wait on an mbarrier phase (wall-clock limit, kWaitNs by default).
+__device__ __forceinline__ bool wait_phase(uint64_t *mbar, uint32_t parity,
+                                           unsigned long long limit_ns = kWaitNs) {
   const unsigned long long t0 = now_ns();
   while (true) {
     if (mbar_wait(mbar, parity, 64)) return true;
-    if (now_ns() - t0 > kWaitNs) return false;
+    if (now_ns() - t0 > limit_ns) return false;
   }
 }
 __host__ __device__ inline uint32_t pow2_cols(int n) {
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int gstride = (R + 2) * HP;      // entries between channel groups of a stage
   const int stage_bytes = GB * gstride * 16;
   const int n0 = blockIdx.y * N;      // the CTA's output channels
+  const unsigned long long wait_ns = a.wait_ns ? a.wait_ns : kWaitNs;
   unsigned char *sW = sm;
   unsigned char *sA = sm + g.w_bytes;
   const uint32_t acc_cols = pow2_cols(N);
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
         const int b = tile / HW, r = tile - b * HW, rg = r / g.s.segs_x, x0 = (r - rg * g.s.segs_x) * SW;
         for (int c = 0; c < nkc; ++c, ++it) {
           const int s = it % nst;
-          if (!wait_phase(&empty[s], ((it / nst) & 1) ^ 1) || *(volatile int *)&s_abort) {
+          if (!wait_phase(&empty[s], ((it / nst) & 1) ^ 1, wait_ns) || *(volatile int *)&s_abort) {
             atomicExch(&s_abort, 1);
             stop = true;
             break;
@@ -190,15 +192,21 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       const uint32_t astep = (uint32_t)(2 * gstride);          // two channel groups of the halo (entries)
       int it = 0, ti = 0;
       bool stop = false;
+      // test knob (a.stall): wait first on a phase that nothing completes before
+      // the drain below, so the wait runs out and the CTA takes the abort path
+      if (a.stall && !wait_phase(&drain, 0, wait_ns)) {
+        atomicExch(&s_abort, 1);
+        stop = true;
+      }
       for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x, ++ti) {
         const int acc = ti % kEpiGroups;
-        if (!wait_phase(&tempty[acc], ((ti / kEpiGroups) & 1) ^ 1)) {
+        if (!wait_phase(&tempty[acc], ((ti / kEpiGroups) & 1) ^ 1, wait_ns)) {
           atomicExch(&s_abort, 1);
           break;
         }
         for (int c = 0; c < nkc; ++c, ++it) {
           const int s = it % nst;
-          if (!wait_phase(&full[s], (it / nst) & 1) || *(volatile int *)&s_abort) {
+          if (!wait_phase(&full[s], (it / nst) & 1, wait_ns) || *(volatile int *)&s_abort) {
             atomicExch(&s_abort, 1);
             stop = true;
             break;
@@ -239,7 +247,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       // lane 0 decides for the warp: tmem loads below are warp-collective
       int go = 0;
       if (lane == 0) {
-        go = wait_phase(&tfull[wg], k & 1) && !*(volatile int *)&s_abort;
+        go = wait_phase(&tfull[wg], k & 1, wait_ns) && !*(volatile int *)&s_abort;
         if (!go) atomicExch(&s_abort, 1);
       }
       if (!__shfl_sync(0xffffffffu, go, 0)) break;

@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -104,7 +105,9 @@ long long npix(const pt_unet *n, int level) {
 
 // (Re)size the activation buffers for a batch shape.
 pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
-  if (n->act_mem && n->B == B && n->H == H && n->W == W) return PT_OK;
+  if (n->act_mem && n->B == B && n->H == H && n->W == W)
+    // a wait that gave up in an earlier call must not fail this one
+    return cudaMemsetAsync(n->err, 0, sizeof(int), n->ctx->stream) == cudaSuccess ? PT_OK : PT_LAUNCH_FAILED;
   struct Item { Act *a; int c; int level; };
   Item items[] = {{&n->X0, 16, 0},  {&n->E0a, 16, 0}, {&n->CAT0, 48, 0}, {&n->P1, 16, 1},   {&n->E1a, 32, 1},
                   {&n->CAT1, 96, 1}, {&n->P2, 32, 2},  {&n->E2a, 64, 2},  {&n->CAT2, 192, 2}, {&n->P3, 64, 3},
@@ -154,8 +157,23 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
 // A channel slice [off, ...) of a buffer (off a multiple of 8).
 ActView view(const Act &t, int off = 0) { return ActView{t.p, t.c / 8, off / 8}; }
 
-pt_status conv(pt_unet *n, int l, const Act &x, int x_off, const Act &y, int y_off, bool relu) {
+// Host fault injection for tests of the bounded waits (no GPU fault involved):
+// PAINTOP_CUDA_FAULT=unet-stall makes the first convolution of a forward pass
+// wait on a barrier phase that nothing completes, under a 0.1 s limit. The
+// wait runs out, the kernel takes its abort path, and the call returns
+// PT_TIMEOUT; the next call runs normally.
+bool stall_injected() {
+  const char *f = std::getenv("PAINTOP_CUDA_FAULT");
+  return f && !std::strcmp(f, "unet-stall");
+}
+
+pt_status conv(pt_unet *n, int l, const Act &x, int x_off, const Act &y, int y_off, bool relu,
+               bool stall = false) {
   ConvArgs a{};
+  if (stall) {
+    a.stall = 1;
+    a.wait_ns = 100000000ull;
+  }
   a.x = view(x, x_off); a.cin = kLayers[l].cin;
   a.w = n->wbf + n->wb_off[l];
   a.bias = n->params + n->b_off[l];
@@ -202,7 +220,7 @@ pt_status forward(pt_unet *n, const float *features) {
   const long long P0 = npix(n, 0);
   (void)P0;
   CK(launch_features_to_input(features, view(n->X0), n->B, n->H, n->W, st), "input");
-  RET(conv(n, 0, n->X0, 0, n->E0a, 0, true));
+  RET(conv(n, 0, n->X0, 0, n->E0a, 0, true, stall_injected()));
   RET(conv(n, 1, n->E0a, 0, n->CAT0, 32, true));  // e0 -> skip slice
   CK(launch_avgpool2(view(n->CAT0, 32), view(n->P1), n->B, n->H, n->W, 2, st), "pool");
   RET(conv(n, 2, n->P1, 0, n->E1a, 0, true));
@@ -430,7 +448,11 @@ pt_status pt_unet_forward(pt_unet *n, const float *features, uint32_t batch, uin
   int kerr = 0;
   CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, n->ctx->stream), "err copy");
   CK(cudaStreamSynchronize(n->ctx->stream), "sync");
-  return kerr ? PT_TIMEOUT : PT_OK;
+  if (kerr) {
+    n->ctx->last_error = "a tensor-core pipeline wait gave up";
+    return PT_TIMEOUT;
+  }
+  return PT_OK;
 }
 
 pt_status pt_unet_loss_grad(pt_unet *n, const float *features, const float *target, const float *loss_mask,
@@ -524,7 +546,11 @@ pt_status pt_unet_guess(pt_unet *n, const float *guidance, const float *anchor, 
   int kerr = 0;
   CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, st), "err copy");
   CK(cudaStreamSynchronize(st), "sync");
-  return kerr ? PT_TIMEOUT : PT_OK;
+  if (kerr) {
+    n->ctx->last_error = "a tensor-core pipeline wait gave up";
+    return PT_TIMEOUT;
+  }
+  return PT_OK;
 }
 
 pt_status pt_unet_save(pt_unet *n, const char *path) {

@@ -37,6 +37,8 @@ struct ConvArgs {
   ActView mask;            // mask.p != nullptr: zero outputs where mask <= 0 (ReLU backward)
   int B, H, W;
   int *err;                // set to 1 if a bounded wait gave up
+  unsigned long long wait_ns;  // limit of each pipeline wait (0: the 2 s default)
+  int stall;               // test knob: the MMA warp first waits on a phase nothing completes
 };
 
 // 3x3 convolution backward-weights.
