@@ -1301,6 +1301,17 @@ def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8, with_
         res[mode] = dict(solves_per_s=1.0 / sec, ms_per_solve=sec * 1e3, **{key: its}, converged=conv,
                          **({"guess_used": used} if mode.startswith("learned") else {}))
     net.close()
+    # the cost gate's choice per method (warmstart.GuessGate: a fixed table of
+    # measured times), and the best gated path against the best plain one
+    gate = warmstart.GuessGate()
+    gated = {}
+    for method, plain_mode in (("sor", "plain"), ("multigrid", "multigrid")):
+        use, entry = gate.decide(W, H, C, 1, method)
+        mode = ("learned" if method == "sor" else "learned_multigrid") if use else plain_mode
+        gated[method] = {"use_guess": use, "table_entry": entry, "ms_per_solve": res[mode]["ms_per_solve"]}
+    best_plain = min(res["plain"]["ms_per_solve"], res["multigrid"]["ms_per_solve"])
+    best_gated = min(v["ms_per_solve"] for v in gated.values())
+    gated["speedup_best_gated_vs_best_plain"] = best_plain / best_gated
     cpu, parity = None, None
     if with_cpu:
         # the restated reference op on one core: 20 sweeps of one channel give its
@@ -1329,7 +1340,7 @@ def learned_leg(ctx, dev, steps: int = 2, warmup: int = 1, scale: int = 8, with_
             "speedup": res["learned"]["solves_per_s"] / res["plain"]["solves_per_s"],
             "speedup_multigrid": res["multigrid"]["solves_per_s"] / res["plain"]["solves_per_s"],
             "speedup_learned_multigrid": res["learned_multigrid"]["solves_per_s"] / res["multigrid"]["solves_per_s"],
-            "cpu_baseline": cpu, "parity": parity}
+            "gate": gated, "cpu_baseline": cpu, "parity": parity}
 
 
 def multigrid_leg(ctx, dev, inst, steps: int = 3, warmup: int = 1):

@@ -561,3 +561,46 @@ def load_params(net: UNet, path: str) -> None:
         if n != net.param_count:
             raise ValueError(f"{path}: {n} parameters, the network has {net.param_count}")
         net.set_params(np.frombuffer(f.read(4 * n), dtype="<f4"))
+
+
+# ---------------------------------------------------------------------------
+# cost gate: run the network only where its guess pays for its inference
+# ---------------------------------------------------------------------------
+GATE_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warmstart_gate_b200.json")
+METHODS = ("sor", "multigrid")
+
+
+def gate_key(width: int, height: int, channels: int, batch: int, method: str) -> str:
+    """Entries are keyed like the tile-configuration table: floor(log2) of the
+    pixels over all channels and images, floor(log2) of one image's pixels,
+    whether the call holds a batch, and the iteration (SOR or multigrid)."""
+    if method not in METHODS:
+        raise ValueError(f"method must be one of {METHODS}")
+    px = float(width) * height
+    lt = max(0, math.floor(math.log2(max(px * channels * batch, 1.0))))
+    ll = max(0, math.floor(math.log2(max(px, 1.0))))
+    return f"{lt}:{ll}:{int(batch > 1)}:{method}"
+
+
+class GuessGate:
+    """A fixed table of measured end-to-end times per shape key and method:
+    the time of a plain solve and of network inference plus the warm-started
+    solve, both to the same bar. The network runs only where the second was
+    measured faster; a shape the table does not hold gets the plain solve (the
+    guess is never used blind). The decision depends on nothing but the
+    problem's shape and the method, so it is the same on every call."""
+
+    def __init__(self, path: str = GATE_TABLE):
+        self.path = path
+        self.entries = {}
+        if os.path.exists(path):
+            with open(path) as f:
+                for e in json.load(f)["entries"]:
+                    self.entries[e["key"]] = e
+
+    def decide(self, width: int, height: int, channels: int, batch: int = 1, method: str = "sor"):
+        """-> (use the guess?, the entry that decided, or None)."""
+        e = self.entries.get(gate_key(width, height, channels, batch, method))
+        if e is None:
+            return False, None
+        return bool(e["learned_ms"] < e["plain_ms"]), e
