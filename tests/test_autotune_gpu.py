@@ -14,6 +14,7 @@ import pytest
 
 TOL_ABS = 1e-6  # agreement between two solves of the same system to rel-res 1e-9
 MARGIN = 0.05   # autotune.cpp, kReplaceMargin
+NCFG = 8        # tile configurations (pt_tile_config_count)
 
 
 def _problems():
@@ -47,7 +48,7 @@ def test_autotune_writes_reads_back_and_is_stable(ctx, tmp_path):
         probs = _problems()
         key = tune.shape_key(probs)
         cfg1, ms1, conv, _ = tune.autotune(ctx, probs, repeats=2)
-        assert conv and len(ms1) == 5 and all(t > 0 for t in ms1)
+        assert conv and len(ms1) == NCFG and all(t > 0 for t in ms1)
         assert _table(path)[key] == cfg1
         # re-tuning keeps the entry unless another configuration now beats it
         # by more than the margin
@@ -65,7 +66,7 @@ def test_autotune_writes_reads_back_and_is_stable(ctx, tmp_path):
             outs.append(out)
         assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
         # the tuned configuration agrees with every other one on the same system
-        for cfg in range(5):
+        for cfg in range(NCFG):
             ctx.set_config(cfg)
             try:
                 other, per, _ = ctx.solve(p["source"], p["target"], p["mask"], 1000, 900, 3, lam=0.01,
