@@ -100,8 +100,12 @@ def _profile_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks + throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region. NVML is
+    polled from a thread every 2 ms (reads only; nothing is set), so even a
+    timed region of tens of milliseconds gets a few dozen samples; without
+    NVML, nvidia-smi is sampled every 50 ms."""
 
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -109,9 +113,27 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.nvml = None
+        self.samples = []   # (sm MHz, max MHz, set of reasons)
         self.lines = []
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.nvml = (pynvml, h, bits, mx)
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
@@ -128,38 +150,54 @@ class ClockSampler:
             time.sleep(0.01)
         self.mark = len(self.lines)
 
+    def _poll(self):
+        pynvml, h, bits, mx = self.nvml
+        while not self._stop.is_set():
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), {n for n, b in bits.items() if rs & b}))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.thread.join(timeout=2)
-        lines = self.lines[getattr(self, "mark", 0):] or self.lines[-1:]
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
+        if self.nvml is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
+            samples, source = self.samples, "nvml, 2 ms"
+        elif self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+            samples, source = [], "nvidia-smi, 50 ms"
+            for ln in self.lines[getattr(self, "mark", 0):] or self.lines[-1:]:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    samples.append((float(parts[1]), float(parts[2]),
+                                    {n for n, v in zip(self.NAMES, parts[5:9]) if v.lower() == "active"}))
+                except ValueError:
+                    continue
+        else:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not samples:
+            return None
+        reasons = set().union(*(r for _, _, r in samples))
+        return {"sm_mhz": statistics.median(x for x, _, _ in samples), "sm_max_mhz": samples[-1][1],
+                "reasons": sorted(reasons), "samples": len(samples), "source": source}
 
 
 def make_instance(seed: int):
@@ -904,6 +942,10 @@ def gpu_arm(args):
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "dram_frac": (traffic / (float(kms.mean()) / 1e3) / 1e9 / peak) if traffic else None,
+                         "frac_note": "frac: algorithmic bytes (temporal blocking reuses tiles in shared "
+                                      "memory, so it can exceed 1); dram_frac: ncu DRAM bytes of the "
+                                      "committed capture over this run's kernel time",
                          "kernel": "ptk::k_solve", "peak_kind": peak_kind,
                          "kernel_ms_mean": float(kms.mean()),
                          "algorithmic_bytes_per_launch": float(alg_bytes.mean())},
