@@ -796,6 +796,8 @@ def gpu_arm(args):
     dev = torch.device("cuda", local if ws > 1 else 0)
     from paintop_b200 import _lib
     ctx = _lib.Context(dev.index)
+    if args.tile_config >= 0:
+        ctx.set_config(args.tile_config)
 
     inst = make_instance(1 + rank)
     W, H, C = inst.width, inst.height, inst.channels
@@ -1441,6 +1443,8 @@ def main():
                     help="batch_uneven: solve by multigrid-preconditioned CG instead of red-black SOR")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-warm-start leg (4096x4096 RGB, learned vs plain)")
+    ap.add_argument("--tile-config", type=int, default=-1,
+                    help="force this tile configuration of the SOR solve (default: the tuned table)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "cuda":
         args.warmup = 3
