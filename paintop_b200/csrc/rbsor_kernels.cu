@@ -701,7 +701,7 @@ __device__ __forceinline__ void band_wait(const int *prog, int warp, int need, i
   __threadfence_block();
 }
 
-template <int S, int TH>
+template <int S, int TH, bool WIN>
 __device__ void sweep_tile_banded(const KParams &P, const SysDesc &d, int t, const Tile &tl, int s,
                                   int cur, float *sE, float *sG, uint8_t *sC, double *sacc, int *prog) {
   using G = Geo<S, TH>;
@@ -775,6 +775,14 @@ __device__ void sweep_tile_banded(const KParams &P, const SysDesc &d, int t, con
       double part = 0.0;
       float4 up = Eo[(r_first - 1) * RQ + l16];
       float4 ct = Eo[r_first * RQ + l16];
+      // WIN: the other colour's rows also slide down as FP64, each entry
+      // converted once per half-sweep (the residual then converts only the
+      // cell's own e and g, and one same-row neighbour from the next lane)
+      double ud[4], cd[4];
+      if (WIN && duty) {
+        ud[0] = up.x; ud[1] = up.y; ud[2] = up.z; ud[3] = up.w;
+        cd[0] = ct.x; cd[1] = ct.y; cd[2] = ct.z; cd[3] = ct.w;
+      }
 #pragma unroll
       for (int i = 0; i < NH; ++i) {
         const int ly = r_first + i;
@@ -793,7 +801,31 @@ __device__ void sweep_tile_banded(const KParams &P, const SysDesc &d, int t, con
         if (cc & 0xff00u) ne.y = fmaf(w, ((((L[1] + R[1]) + up.y) + dn.y) - gc.y) * inv - ec.y, ec.y);
         if (cc & 0xff0000u) ne.z = fmaf(w, ((((L[2] + R[2]) + up.z) + dn.z) - gc.z) * inv - ec.z, ec.z);
         if (cc & 0xff000000u) ne.w = fmaf(w, ((((L[3] + R[3]) + up.w) + dn.w) - gc.w) * inv - ec.w, ec.w);
-        if (duty && ly >= OY0 && ly < OY1) {
+        if constexpr (WIN) {
+          double dd4[4];
+          if (duty) { dd4[0] = dn.x; dd4[1] = dn.y; dd4[2] = dn.z; dd4[3] = dn.w; }
+          if (duty && ly >= OY0 && ly < OY1) {
+            const int xq = x0 + q;
+            const float4 ee = h ? ne : ec;
+            const double nb = (double)(q ? next : prev);
+            // same-row neighbours as FP64: entries k+q-1, k+q of (nb, cd...)
+            const double a0 = q ? cd[0] : nb, a1 = q ? cd[1] : cd[0], a2 = q ? cd[2] : cd[1],
+                         a3 = q ? cd[3] : cd[2], a4 = q ? nb : cd[3];
+            auto rd = [&](double l, double r, double u, double dw, float e, float g) -> double {
+              const double ns = ((l + r) + u) + dw;
+              const double rr = fma(-dd, (double)e, ns) - (double)g;
+              return rr * rr;
+            };
+            if ((cc & 0xffu) && xq >= OX0 && xq < OX1) part += rd(a0, a1, ud[0], dd4[0], ee.x, gc.x);
+            if ((cc & 0xff00u) && xq + 2 >= OX0 && xq + 2 < OX1) part += rd(a1, a2, ud[1], dd4[1], ee.y, gc.y);
+            if ((cc & 0xff0000u) && xq + 4 >= OX0 && xq + 4 < OX1) part += rd(a2, a3, ud[2], dd4[2], ee.z, gc.z);
+            if ((cc & 0xff000000u) && xq + 6 >= OX0 && xq + 6 < OX1) part += rd(a3, a4, ud[3], dd4[3], ee.w, gc.w);
+          }
+          if (duty) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) { ud[k] = cd[k]; cd[k] = dd4[k]; }
+          }
+        } else if (duty && ly >= OY0 && ly < OY1) {
           const int xq = x0 + q;
           const float4 ee = h ? ne : ec;
           if ((cc & 0xffu) && xq >= OX0 && xq < OX1) part += resid(L[0], R[0], up.x, dn.x, ee.x, gc.x);
@@ -1086,12 +1118,15 @@ __device__ int claim_tile(const KParams &P, int rot, int *idx, unsigned *gen,
 
 // Dynamic shared memory of k_solve: the tile planes and the reduction scratch,
 // plus, for the banded sweep, its per-warp partials and progress words.
-template <int S, int TH, bool BAND>
+// Sweep variants: 0 a block barrier after every half-sweep (sweep_tile); 1
+// banded, neighbour-synchronised warps (sweep_tile_banded); 2 banded with the
+// FP64 row window.
+template <int S, int TH, int VAR>
 constexpr size_t solve_smem() {
-  return Geo<S, TH>::kSmem + (BAND ? (size_t)S * kWarps * sizeof(double) + kWarps * sizeof(int) : 0);
+  return Geo<S, TH>::kSmem + (VAR ? (size_t)S * kWarps * sizeof(double) + kWarps * sizeof(int) : 0);
 }
 
-template <int S, int TH, bool BAND>
+template <int S, int TH, int VAR>
 __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
   using G = Geo<S, TH>;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1129,7 +1164,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
     const int s = __ldcg(&stp->s);
     const int cur = __ldcg(&stp->cur);
     if (mode == M_SWEEP || mode == M_REDO) {
-      if constexpr (BAND) sweep_tile_banded<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sacc, sprog);
+      if constexpr (VAR > 0) sweep_tile_banded<S, TH, VAR == 2>(P, d, t, tl, s, cur, sE, sG, sC, sacc, sprog);
       else sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
     } else if (mode == M_FOLD) {
       fold_tile<S, TH>(P, d, tl, cur);
@@ -1178,14 +1213,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
 // ----------------------------------------------------------------------------
 // launch entry points (host)
 // ----------------------------------------------------------------------------
-template <int S, int TH, bool BAND>
+template <int S, int TH, int VAR>
 static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
-  constexpr size_t smem = solve_smem<S, TH, BAND>();
-  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH, BAND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  constexpr size_t smem = solve_smem<S, TH, VAR>();
+  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH, BAND>, kThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH, VAR>, kThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int grid = per_sm * sms;
@@ -1194,20 +1229,21 @@ static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
   return cudaSuccess;
 }
 
-template <int S, int TH, bool BAND>
+template <int S, int TH, int VAR>
 static cudaError_t launch_prepared_t(const KParams &P, int grid, cudaStream_t stream) {
   KParams Pc = P;
   Pc.S = S;
   // No block waits for a particular other block (work is claimed, never
   // assigned), so an ordinary launch suffices; the grid fills the GPU once.
-  k_solve<S, TH, BAND><<<grid, kThreads, solve_smem<S, TH, BAND>(), stream>>>(Pc);
+  k_solve<S, TH, VAR><<<grid, kThreads, solve_smem<S, TH, VAR>(), stream>>>(Pc);
   return cudaGetLastError();
 }
 
 // Configurations 0-4 sweep with a block barrier after every half-sweep; 5-7
 // are the banded sweep (neighbour-synchronised warps) on the tiles of 1, 2
-// and 4. Every loaded height TH + 2(2S+1) leaves rows 1..LH-2 a multiple of 32.
-int tile_config_count() { return 8; }
+// and 4; 8-10 the banded sweep with the FP64 row window on the same tiles.
+// Every loaded height TH + 2(2S+1) leaves rows 1..LH-2 a multiple of 32.
+int tile_config_count() { return 11; }
 
 TileConfig tile_config(int idx) {
   switch (idx) {
@@ -1218,20 +1254,26 @@ TileConfig tile_config(int idx) {
     case 4: return {4, 80, tile_w(4)};
     case 5: return {2, 88, tile_w(2)};
     case 6: return {3, 84, tile_w(3)};
+    case 7: return {4, 80, tile_w(4)};
+    case 8: return {2, 88, tile_w(2)};
+    case 9: return {3, 84, tile_w(3)};
     default: return {4, 80, tile_w(4)};
   }
 }
 
 size_t tile_config_smem(int idx) {
   switch (idx) {
-    case 0: return solve_smem<1, 60, false>();
-    case 1: return solve_smem<2, 88, false>();
-    case 2: return solve_smem<3, 84, false>();
-    case 3: return solve_smem<3, 52, false>();
-    case 4: return solve_smem<4, 80, false>();
-    case 5: return solve_smem<2, 88, true>();
-    case 6: return solve_smem<3, 84, true>();
-    default: return solve_smem<4, 80, true>();
+    case 0: return solve_smem<1, 60, 0>();
+    case 1: return solve_smem<2, 88, 0>();
+    case 2: return solve_smem<3, 84, 0>();
+    case 3: return solve_smem<3, 52, 0>();
+    case 4: return solve_smem<4, 80, 0>();
+    case 5: return solve_smem<2, 88, 1>();
+    case 6: return solve_smem<3, 84, 1>();
+    case 7: return solve_smem<4, 80, 1>();
+    case 8: return solve_smem<2, 88, 2>();
+    case 9: return solve_smem<3, 84, 2>();
+    default: return solve_smem<4, 80, 2>();
   }
 }
 
@@ -1258,27 +1300,33 @@ cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t
 
 cudaError_t prepare_solve(const KParams &P, int cfg, int sms, int *grid) {
   switch (cfg) {
-    case 0: return prepare_solve_t<1, 60, false>(P, sms, grid);
-    case 1: return prepare_solve_t<2, 88, false>(P, sms, grid);
-    case 2: return prepare_solve_t<3, 84, false>(P, sms, grid);
-    case 3: return prepare_solve_t<3, 52, false>(P, sms, grid);
-    case 4: return prepare_solve_t<4, 80, false>(P, sms, grid);
-    case 5: return prepare_solve_t<2, 88, true>(P, sms, grid);
-    case 6: return prepare_solve_t<3, 84, true>(P, sms, grid);
-    default: return prepare_solve_t<4, 80, true>(P, sms, grid);
+    case 0: return prepare_solve_t<1, 60, 0>(P, sms, grid);
+    case 1: return prepare_solve_t<2, 88, 0>(P, sms, grid);
+    case 2: return prepare_solve_t<3, 84, 0>(P, sms, grid);
+    case 3: return prepare_solve_t<3, 52, 0>(P, sms, grid);
+    case 4: return prepare_solve_t<4, 80, 0>(P, sms, grid);
+    case 5: return prepare_solve_t<2, 88, 1>(P, sms, grid);
+    case 6: return prepare_solve_t<3, 84, 1>(P, sms, grid);
+    case 7: return prepare_solve_t<4, 80, 1>(P, sms, grid);
+    case 8: return prepare_solve_t<2, 88, 2>(P, sms, grid);
+    case 9: return prepare_solve_t<3, 84, 2>(P, sms, grid);
+    default: return prepare_solve_t<4, 80, 2>(P, sms, grid);
   }
 }
 
 cudaError_t launch_prepared(const KParams &P, int cfg, int grid, cudaStream_t stream) {
   switch (cfg) {
-    case 0: return launch_prepared_t<1, 60, false>(P, grid, stream);
-    case 1: return launch_prepared_t<2, 88, false>(P, grid, stream);
-    case 2: return launch_prepared_t<3, 84, false>(P, grid, stream);
-    case 3: return launch_prepared_t<3, 52, false>(P, grid, stream);
-    case 4: return launch_prepared_t<4, 80, false>(P, grid, stream);
-    case 5: return launch_prepared_t<2, 88, true>(P, grid, stream);
-    case 6: return launch_prepared_t<3, 84, true>(P, grid, stream);
-    default: return launch_prepared_t<4, 80, true>(P, grid, stream);
+    case 0: return launch_prepared_t<1, 60, 0>(P, grid, stream);
+    case 1: return launch_prepared_t<2, 88, 0>(P, grid, stream);
+    case 2: return launch_prepared_t<3, 84, 0>(P, grid, stream);
+    case 3: return launch_prepared_t<3, 52, 0>(P, grid, stream);
+    case 4: return launch_prepared_t<4, 80, 0>(P, grid, stream);
+    case 5: return launch_prepared_t<2, 88, 1>(P, grid, stream);
+    case 6: return launch_prepared_t<3, 84, 1>(P, grid, stream);
+    case 7: return launch_prepared_t<4, 80, 1>(P, grid, stream);
+    case 8: return launch_prepared_t<2, 88, 2>(P, grid, stream);
+    case 9: return launch_prepared_t<3, 84, 2>(P, grid, stream);
+    default: return launch_prepared_t<4, 80, 2>(P, grid, stream);
   }
 }
 
