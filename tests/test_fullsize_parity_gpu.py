@@ -122,3 +122,29 @@ def test_multi_4096_within_bounded_tier(ctx, multi, mode):
     if mode.startswith("learned"):
         assert all(reps[c].warm_start for c in range(Ch))
     within_tier(out.cpu().numpy(), multi["tight"], f"{mode} vs FP64 oracle")
+
+
+@pytest.mark.parametrize("multigrid", [False, True])
+def test_batch_uneven_within_bounded_tier(ctx, oracle, multigrid):
+    """The 256-instance uneven RGB batch (side log-uniform in [64, 1024], ellipse
+    masks 20-60%, rel-res 1e-6) in one pt_poisson_solve_batch call: SOR with
+    automatic omega, or multigrid-CG with every instance in each launch. Sixteen
+    instances spread over the size range are held to the bounded tier against
+    the FP64 oracle."""
+    from paintop_b200 import _lib, synth
+    insts = synth.batch_uneven(1, 256)
+    flags = _lib.PT_FLAG_MULTIGRID if multigrid else _lib.PT_FLAG_OMEGA_AUTO
+    probs = [dict(source=i.source.reshape(-1), target=i.target.reshape(-1), mask=i.mask.reshape(-1),
+                  width=i.width, height=i.height, channels=i.channels, lam=0.0, max_iterations=100000,
+                  tolerance=1e-6, omega=1.8, flags=flags) for i in insts]
+    results = ctx.solve_batch(probs)
+    order = sorted(range(len(insts)), key=lambda k: insts[k].width * insts[k].height)
+    for k in order[::16]:
+        out, per = results[k][0], results[k][1]
+        assert all(r["converged"] for r in per), k
+        i = insts[k]
+        tight, ach, _ = oracle.mgcg_blend_channels(i.source.reshape(-1), i.target.reshape(-1),
+                                                   i.mask.reshape(-1), i.channels, i.width, i.height,
+                                                   lam=0.0, rel_tol=1e-12)
+        assert (ach <= 1e-12).all()
+        within_tier(out, tight, f"instance {k} ({i.width}x{i.height})")
