@@ -634,282 +634,6 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
   }
 }
 
-// ---- banded variant: neighbour-synchronised half-sweeps -----------------------
-//
-// The same tile step as sweep_tile (same loads, same cell arithmetic in the
-// same operation order, the same FP64 residuals, the same write-back), with
-// the work of a half-sweep split differently. Warp w owns a fixed band of NB
-// consecutive loaded rows (1 + NB*w ...), half-warp hw the NH = NB/2 rows
-// 1 + NB*w + NH*hw ... of it, for all 2S half-sweeps. A half-sweep of colour
-// h reads the other colour's rows ly-1, ly, ly+1 and writes colour h's row ly,
-// so a band depends only on the neighbouring bands: a warp starts half-sweep p
-// once warps w-1 and w+1 have finished half-sweep p-1 (their writes of the
-// rows it reads are complete, and their reads of the rows it is about to
-// overwrite are done). That replaces the block barrier after every half-sweep
-// by two progress words in shared memory (release / acquire at CTA scope);
-// warps skew instead of waiting for the slowest. Inside a half-warp the other
-// colour's rows slide down a three-row window in registers, so each is loaded
-// and converted to FP64 once per half-sweep instead of three times.
-//
-// Every wait is bounded: a wait that gives up sets the kernel's error word
-// (KERR_STALLED) and the warp goes on; the next claim of every block sees the
-// error and the kernel ends. No wait can depend on a later half-sweep, so in a
-// correct kernel none gives up.
-constexpr unsigned long long kBandWaitNs = 1000000000ull;  // 1 s
-
-__device__ __forceinline__ int ld_acquire_cta_s32(const int *p) {
-  int v;
-  asm volatile("ld.acquire.cta.shared::cta.s32 %0, [%1];"
-               : "=r"(v)
-               : "r"((unsigned)__cvta_generic_to_shared(p))
-               : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_cta_s32(int *p, int v) {
-  asm volatile("st.release.cta.shared::cta.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
-               "r"(v)
-               : "memory");
-}
-
-// Publish that this warp has finished `done` half-sweeps (all lanes call).
-__device__ __forceinline__ void band_publish(int *prog, int warp, int done) {
-  __threadfence_block();
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) st_release_cta_s32(prog + warp, done);
-}
-
-// Wait until both neighbouring warps have finished `need` half-sweeps (all
-// lanes call; lane 0 polls).
-__device__ __forceinline__ void band_wait(const int *prog, int warp, int need, int *err) {
-  if ((threadIdx.x & 31) == 0) {
-    const int a = warp > 0 ? warp - 1 : warp;
-    const int b = warp < kWarps - 1 ? warp + 1 : warp;
-    unsigned long long t0 = 0;
-    for (unsigned k = 0;; ++k) {
-      if (ld_acquire_cta_s32(prog + a) >= need && ld_acquire_cta_s32(prog + b) >= need) break;
-      if ((k & 255u) == 255u) {
-        const unsigned long long now = gtimer();
-        if (!t0) t0 = now;
-        else if (now - t0 > kBandWaitNs) {
-          atomicCAS(err, 0, KERR_STALLED);
-          break;
-        }
-      }
-    }
-  }
-  __syncwarp();
-  __threadfence_block();
-}
-
-template <int S, int TH, bool WIN>
-__device__ void sweep_tile_banded(const KParams &P, const SysDesc &d, int t, const Tile &tl, int s,
-                                  int cur, float *sE, float *sG, uint8_t *sC, double *sacc, int *prog) {
-  using G = Geo<S, TH>;
-  constexpr int NB = (G::LH - 2) / kWarps;  // rows per warp
-  constexpr int NH = NB / 2;                // rows per half-warp
-  static_assert((G::LH - 2) % kWarps == 0 && NB % 2 == 0, "bands must tile rows 1..LH-2");
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int X0 = tl.tx * G::TW - G::HX;
-  const int Y0 = tl.ty * TH - G::H;
-  const int gi0 = X0 >> 1;
-  const float *__restrict__ ein = cur ? P.e1 : P.e0;
-  float *__restrict__ eout = cur ? P.e0 : P.e1;
-
-  constexpr int V = kPWL / 4;
-  for (int k = tid; k < 2 * G::LH * V; k += kThreads) {
-    const int c = k / (G::LH * V);
-    const int r = k - c * (G::LH * V);
-    const int ly = r / V, v = r - ly * V;
-    const int gy = Y0 + ly, gi = gi0 + 4 * v;
-    const bool in = gy >= 0 && gy < d.H && gi >= 0 && gi < d.pw;
-    const long long o = in ? plane_index(d, c, gy, gi) : d.off;
-    const int so = c * G::PLANE + ly * kPWL + 4 * v;
-    cp_async16(sE + so, ein + o, in);
-    cp_async16(sG + so, P.g + o, in);
-    cp_async4(sC + so, P.cell + o, in);
-  }
-  if (tid < kWarps) prog[tid] = 0;
-  cp_async_wait_all();
-  __syncthreads();
-
-  const int pl = Y0 & 1;
-  const float w = d.omega, inv = d.inv_denom;
-  const double dd = 4.0 + d.lambda;
-  constexpr int OX0 = G::HX, OX1 = G::HX + G::TW;
-  constexpr int OY0 = G::H, OY1 = G::H + TH;
-  constexpr int RQ = kPWL / 4;
-  const int hw = lane >> 4, l16 = lane & 15;
-  const int r_first = 1 + NB * warp + NH * hw;  // this half-warp's first row
-  const int x0 = 8 * l16;                      // loaded column of the lane's first plane entry (q = 0)
-  double acc[S];
-#pragma unroll
-  for (int j = 0; j < S; ++j) acc[j] = 0.0;
-
-  auto resid = [&](float l, float r, float u, float dn, float e, float g) -> double {
-    const double ns = (((double)l + (double)r) + (double)u) + (double)dn;
-    const double rr = fma(-dd, (double)e, ns) - (double)g;
-    return rr * rr;
-  };
-  // the same-row neighbours of the lane's four cells: cell k's left/right are
-  // entries k+q-1 / k+q of the other colour's row (prev / next from the
-  // neighbouring lanes)
-  auto lr = [&](int q, const float4 &ct, float prev, float next, float (&L)[4], float (&R)[4]) {
-    const float a = q ? ct.x : prev, b = q ? ct.y : ct.x, c = q ? ct.z : ct.y, e4 = q ? ct.w : ct.z,
-                f = q ? next : ct.w;
-    L[0] = a; R[0] = b; L[1] = b; R[1] = c; L[2] = c; R[2] = e4; L[3] = e4; R[3] = f;
-  };
-
-  int err_seen = 0;
-  int phase = 0;
-#pragma unroll
-  for (int j = 0; j < S; ++j) {
-    if (j >= s) break;
-#pragma unroll
-    for (int h = 0; h < 2; ++h, ++phase) {
-      if (phase > 0) band_wait(prog, warp, phase, P.err);
-      float4 *Ec = reinterpret_cast<float4 *>(sE + h * G::PLANE);
-      const float4 *Eo = reinterpret_cast<const float4 *>(sE + (1 - h) * G::PLANE);
-      const float4 *Gc = reinterpret_cast<const float4 *>(sG + h * G::PLANE);
-      const uint32_t *Cc = reinterpret_cast<const uint32_t *>(sC + h * G::PLANE);
-      const bool duty = (h == 1) || (j > 0);
-      double part = 0.0;
-      float4 up = Eo[(r_first - 1) * RQ + l16];
-      float4 ct = Eo[r_first * RQ + l16];
-      // WIN: the other colour's rows also slide down as FP64, each entry
-      // converted once per half-sweep (the residual then converts only the
-      // cell's own e and g, and one same-row neighbour from the next lane)
-      double ud[4], cd[4];
-      if (WIN && duty) {
-        ud[0] = up.x; ud[1] = up.y; ud[2] = up.z; ud[3] = up.w;
-        cd[0] = ct.x; cd[1] = ct.y; cd[2] = ct.z; cd[3] = ct.w;
-      }
-#pragma unroll
-      for (int i = 0; i < NH; ++i) {
-        const int ly = r_first + i;
-        const int r4 = ly * RQ + l16;
-        const float4 dn = Eo[r4 + RQ];
-        const float4 gc = Gc[r4];
-        const float4 ec = Ec[r4];
-        const uint32_t cc = Cc[r4];
-        const int q = (h + ly + pl) & 1;
-        const float prev = __shfl_up_sync(0xffffffffu, ct.w, 1, 16);
-        const float next = __shfl_down_sync(0xffffffffu, ct.x, 1, 16);
-        float L[4], R[4];
-        lr(q, ct, prev, next, L, R);
-        float4 ne = ec;
-        if (cc & 0xffu) ne.x = fmaf(w, ((((L[0] + R[0]) + up.x) + dn.x) - gc.x) * inv - ec.x, ec.x);
-        if (cc & 0xff00u) ne.y = fmaf(w, ((((L[1] + R[1]) + up.y) + dn.y) - gc.y) * inv - ec.y, ec.y);
-        if (cc & 0xff0000u) ne.z = fmaf(w, ((((L[2] + R[2]) + up.z) + dn.z) - gc.z) * inv - ec.z, ec.z);
-        if (cc & 0xff000000u) ne.w = fmaf(w, ((((L[3] + R[3]) + up.w) + dn.w) - gc.w) * inv - ec.w, ec.w);
-        if constexpr (WIN) {
-          double dd4[4];
-          if (duty) { dd4[0] = dn.x; dd4[1] = dn.y; dd4[2] = dn.z; dd4[3] = dn.w; }
-          if (duty && ly >= OY0 && ly < OY1) {
-            const int xq = x0 + q;
-            const float4 ee = h ? ne : ec;
-            const double nb = (double)(q ? next : prev);
-            // same-row neighbours as FP64: entries k+q-1, k+q of (nb, cd...)
-            const double a0 = q ? cd[0] : nb, a1 = q ? cd[1] : cd[0], a2 = q ? cd[2] : cd[1],
-                         a3 = q ? cd[3] : cd[2], a4 = q ? nb : cd[3];
-            auto rd = [&](double l, double r, double u, double dw, float e, float g) -> double {
-              const double ns = ((l + r) + u) + dw;
-              const double rr = fma(-dd, (double)e, ns) - (double)g;
-              return rr * rr;
-            };
-            if ((cc & 0xffu) && xq >= OX0 && xq < OX1) part += rd(a0, a1, ud[0], dd4[0], ee.x, gc.x);
-            if ((cc & 0xff00u) && xq + 2 >= OX0 && xq + 2 < OX1) part += rd(a1, a2, ud[1], dd4[1], ee.y, gc.y);
-            if ((cc & 0xff0000u) && xq + 4 >= OX0 && xq + 4 < OX1) part += rd(a2, a3, ud[2], dd4[2], ee.z, gc.z);
-            if ((cc & 0xff000000u) && xq + 6 >= OX0 && xq + 6 < OX1) part += rd(a3, a4, ud[3], dd4[3], ee.w, gc.w);
-          }
-          if (duty) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) { ud[k] = cd[k]; cd[k] = dd4[k]; }
-          }
-        } else if (duty && ly >= OY0 && ly < OY1) {
-          const int xq = x0 + q;
-          const float4 ee = h ? ne : ec;
-          if ((cc & 0xffu) && xq >= OX0 && xq < OX1) part += resid(L[0], R[0], up.x, dn.x, ee.x, gc.x);
-          if ((cc & 0xff00u) && xq + 2 >= OX0 && xq + 2 < OX1) part += resid(L[1], R[1], up.y, dn.y, ee.y, gc.y);
-          if ((cc & 0xff0000u) && xq + 4 >= OX0 && xq + 4 < OX1) part += resid(L[2], R[2], up.z, dn.z, ee.z, gc.z);
-          if ((cc & 0xff000000u) && xq + 6 >= OX0 && xq + 6 < OX1) part += resid(L[3], R[3], up.w, dn.w, ee.w, gc.w);
-        }
-        Ec[r4] = ne;
-        up = ct;
-        ct = dn;
-      }
-      if (h == 1) acc[j] += part;
-      else if (j > 0) acc[j - 1] += part;
-      band_publish(prog, warp, phase + 1);
-    }
-  }
-  // red cells' residual of the final state, over the owned rows of the band
-  band_wait(prog, warp, phase, P.err);
-  {
-    const float4 *Er = reinterpret_cast<const float4 *>(sE);
-    const float4 *Eb = reinterpret_cast<const float4 *>(sE + G::PLANE);
-    const float4 *Gr = reinterpret_cast<const float4 *>(sG);
-    const uint32_t *Cr = reinterpret_cast<const uint32_t *>(sC);
-    double part = 0.0;
-    float4 up = Eb[(r_first - 1) * RQ + l16];
-    float4 ct = Eb[r_first * RQ + l16];
-#pragma unroll
-    for (int i = 0; i < NH; ++i) {
-      const int ly = r_first + i;
-      const int r4 = ly * RQ + l16;
-      const float4 dn = Eb[r4 + RQ];
-      const int q = (ly + pl) & 1;
-      const float prev = __shfl_up_sync(0xffffffffu, ct.w, 1, 16);
-      const float next = __shfl_down_sync(0xffffffffu, ct.x, 1, 16);
-      if (ly >= OY0 && ly < OY1) {
-        const float4 gc = Gr[r4], ec = Er[r4];
-        const uint32_t cc = Cr[r4];
-        float L[4], R[4];
-        lr(q, ct, prev, next, L, R);
-        const int xq = x0 + q;
-        if ((cc & 0xffu) && xq >= OX0 && xq < OX1) part += resid(L[0], R[0], up.x, dn.x, ec.x, gc.x);
-        if ((cc & 0xff00u) && xq + 2 >= OX0 && xq + 2 < OX1) part += resid(L[1], R[1], up.y, dn.y, ec.y, gc.y);
-        if ((cc & 0xff0000u) && xq + 4 >= OX0 && xq + 4 < OX1) part += resid(L[2], R[2], up.z, dn.z, ec.z, gc.z);
-        if ((cc & 0xff000000u) && xq + 6 >= OX0 && xq + 6 < OX1) part += resid(L[3], R[3], up.w, dn.w, ec.w, gc.w);
-      }
-      up = ct;
-      ct = dn;
-    }
-#pragma unroll
-    for (int j = 0; j < S; ++j)
-      if (j == s - 1) acc[j] += part;
-  }
-  (void)err_seen;
-  // the S tile partials: a warp's xor butterfly, then the warps in index order
-  // (its own scratch: other warps may still be reading g)
-#pragma unroll
-  for (int j = 0; j < S; ++j) {
-    if (j >= s) break;
-    double v = acc[j];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) sacc[j * kWarps + warp] = v;
-  }
-  __syncthreads();
-  if (tid < s) {
-    double tot = 0.0;
-    for (int ww = 0; ww < kWarps; ++ww) tot += sacc[tid * kWarps + ww];
-    P.partial[(long long)tid * P.ntiles + t] = tot;
-  }
-
-  constexpr int OV = G::TW / 8;
-  for (int k = tid; k < 2 * TH * OV; k += kThreads) {
-    const int c = k / (TH * OV);
-    const int r = k - c * (TH * OV);
-    const int ly = G::H + r / OV, v = G::HX / 8 + r % OV;
-    const int gy = Y0 + ly, gi = gi0 + 4 * v;
-    if (gy < d.H && gi < d.pw) {
-      const int so = c * G::PLANE + ly * kPWL + 4 * v;
-      *reinterpret_cast<float4 *>(eout + plane_index(d, c, gy, gi)) =
-          *reinterpret_cast<const float4 *>(sE + so);
-    }
-  }
-}
-
 // u += e on interior cells; e = 0 (owned cells of the tile).
 template <int S, int TH>
 __device__ void fold_tile(const KParams &P, const SysDesc &d, const Tile &tl, int cur) {
@@ -1116,17 +840,7 @@ __device__ int claim_tile(const KParams &P, int rot, int *idx, unsigned *gen,
   }
 }
 
-// Dynamic shared memory of k_solve: the tile planes and the reduction scratch,
-// plus, for the banded sweep, its per-warp partials and progress words.
-// Sweep variants: 0 a block barrier after every half-sweep (sweep_tile); 1
-// banded, neighbour-synchronised warps (sweep_tile_banded); 2 banded with the
-// FP64 row window.
-template <int S, int TH, int VAR>
-constexpr size_t solve_smem() {
-  return Geo<S, TH>::kSmem + (VAR ? (size_t)S * kWarps * sizeof(double) + kWarps * sizeof(int) : 0);
-}
-
-template <int S, int TH, int VAR>
+template <int S, int TH>
 __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
   using G = Geo<S, TH>;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1134,8 +848,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
   float *sG = sE + 2 * G::PLANE;
   uint8_t *sC = reinterpret_cast<uint8_t *>(sG + 2 * G::PLANE);
   double *sred = reinterpret_cast<double *>(sC + 2 * G::PLANE);
-  double *sacc = sred + kWarps;                    // banded sweep: S x kWarps partials
-  int *sprog = reinterpret_cast<int *>(sacc + S * kWarps);  // banded sweep: progress words
   __shared__ int s_last, s_sys, s_idx;
   __shared__ unsigned s_gen;
   const unsigned long long t_start = gtimer();
@@ -1164,8 +876,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
     const int s = __ldcg(&stp->s);
     const int cur = __ldcg(&stp->cur);
     if (mode == M_SWEEP || mode == M_REDO) {
-      if constexpr (VAR > 0) sweep_tile_banded<S, TH, VAR == 2>(P, d, t, tl, s, cur, sE, sG, sC, sacc, sprog);
-      else sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
+      sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
     } else if (mode == M_FOLD) {
       fold_tile<S, TH>(P, d, tl, cur);
     } else {
@@ -1213,14 +924,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
 // ----------------------------------------------------------------------------
 // launch entry points (host)
 // ----------------------------------------------------------------------------
-template <int S, int TH, int VAR>
+template <int S, int TH>
 static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
-  constexpr size_t smem = solve_smem<S, TH, VAR>();
-  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  using G = Geo<S, TH>;
+  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)G::kSmem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH, VAR>, kThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH>, kThreads, G::kSmem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int grid = per_sm * sms;
@@ -1229,51 +940,38 @@ static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
   return cudaSuccess;
 }
 
-template <int S, int TH, int VAR>
+template <int S, int TH>
 static cudaError_t launch_prepared_t(const KParams &P, int grid, cudaStream_t stream) {
+  using G = Geo<S, TH>;
   KParams Pc = P;
   Pc.S = S;
   // No block waits for a particular other block (work is claimed, never
   // assigned), so an ordinary launch suffices; the grid fills the GPU once.
-  k_solve<S, TH, VAR><<<grid, kThreads, solve_smem<S, TH, VAR>(), stream>>>(Pc);
+  k_solve<S, TH><<<grid, kThreads, G::kSmem, stream>>>(Pc);
   return cudaGetLastError();
 }
 
-// Configurations 0-4 sweep with a block barrier after every half-sweep; 5-7
-// are the banded sweep (neighbour-synchronised warps) on the tiles of 1, 2
-// and 4; 8-10 the banded sweep with the FP64 row window on the same tiles.
-// Every loaded height TH + 2(2S+1) leaves rows 1..LH-2 a multiple of 32.
-int tile_config_count() { return 11; }
+int tile_config_count() { return 5; }
 
+// (sweeps per step S, owned tile height TH); every loaded height TH + 2(2S+1)
+// leaves rows 1..LH-2 a multiple of 32.
 TileConfig tile_config(int idx) {
   switch (idx) {
     case 0: return {1, 60, tile_w(1)};
     case 1: return {2, 88, tile_w(2)};
     case 2: return {3, 84, tile_w(3)};
     case 3: return {3, 52, tile_w(3)};
-    case 4: return {4, 80, tile_w(4)};
-    case 5: return {2, 88, tile_w(2)};
-    case 6: return {3, 84, tile_w(3)};
-    case 7: return {4, 80, tile_w(4)};
-    case 8: return {2, 88, tile_w(2)};
-    case 9: return {3, 84, tile_w(3)};
     default: return {4, 80, tile_w(4)};
   }
 }
 
 size_t tile_config_smem(int idx) {
   switch (idx) {
-    case 0: return solve_smem<1, 60, 0>();
-    case 1: return solve_smem<2, 88, 0>();
-    case 2: return solve_smem<3, 84, 0>();
-    case 3: return solve_smem<3, 52, 0>();
-    case 4: return solve_smem<4, 80, 0>();
-    case 5: return solve_smem<2, 88, 1>();
-    case 6: return solve_smem<3, 84, 1>();
-    case 7: return solve_smem<4, 80, 1>();
-    case 8: return solve_smem<2, 88, 2>();
-    case 9: return solve_smem<3, 84, 2>();
-    default: return solve_smem<4, 80, 2>();
+    case 0: return Geo<1, 60>::kSmem;
+    case 1: return Geo<2, 88>::kSmem;
+    case 2: return Geo<3, 84>::kSmem;
+    case 3: return Geo<3, 52>::kSmem;
+    default: return Geo<4, 80>::kSmem;
   }
 }
 
@@ -1300,33 +998,21 @@ cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t
 
 cudaError_t prepare_solve(const KParams &P, int cfg, int sms, int *grid) {
   switch (cfg) {
-    case 0: return prepare_solve_t<1, 60, 0>(P, sms, grid);
-    case 1: return prepare_solve_t<2, 88, 0>(P, sms, grid);
-    case 2: return prepare_solve_t<3, 84, 0>(P, sms, grid);
-    case 3: return prepare_solve_t<3, 52, 0>(P, sms, grid);
-    case 4: return prepare_solve_t<4, 80, 0>(P, sms, grid);
-    case 5: return prepare_solve_t<2, 88, 1>(P, sms, grid);
-    case 6: return prepare_solve_t<3, 84, 1>(P, sms, grid);
-    case 7: return prepare_solve_t<4, 80, 1>(P, sms, grid);
-    case 8: return prepare_solve_t<2, 88, 2>(P, sms, grid);
-    case 9: return prepare_solve_t<3, 84, 2>(P, sms, grid);
-    default: return prepare_solve_t<4, 80, 2>(P, sms, grid);
+    case 0: return prepare_solve_t<1, 60>(P, sms, grid);
+    case 1: return prepare_solve_t<2, 88>(P, sms, grid);
+    case 2: return prepare_solve_t<3, 84>(P, sms, grid);
+    case 3: return prepare_solve_t<3, 52>(P, sms, grid);
+    default: return prepare_solve_t<4, 80>(P, sms, grid);
   }
 }
 
 cudaError_t launch_prepared(const KParams &P, int cfg, int grid, cudaStream_t stream) {
   switch (cfg) {
-    case 0: return launch_prepared_t<1, 60, 0>(P, grid, stream);
-    case 1: return launch_prepared_t<2, 88, 0>(P, grid, stream);
-    case 2: return launch_prepared_t<3, 84, 0>(P, grid, stream);
-    case 3: return launch_prepared_t<3, 52, 0>(P, grid, stream);
-    case 4: return launch_prepared_t<4, 80, 0>(P, grid, stream);
-    case 5: return launch_prepared_t<2, 88, 1>(P, grid, stream);
-    case 6: return launch_prepared_t<3, 84, 1>(P, grid, stream);
-    case 7: return launch_prepared_t<4, 80, 1>(P, grid, stream);
-    case 8: return launch_prepared_t<2, 88, 2>(P, grid, stream);
-    case 9: return launch_prepared_t<3, 84, 2>(P, grid, stream);
-    default: return launch_prepared_t<4, 80, 2>(P, grid, stream);
+    case 0: return launch_prepared_t<1, 60>(P, grid, stream);
+    case 1: return launch_prepared_t<2, 88>(P, grid, stream);
+    case 2: return launch_prepared_t<3, 84>(P, grid, stream);
+    case 3: return launch_prepared_t<3, 52>(P, grid, stream);
+    default: return launch_prepared_t<4, 80>(P, grid, stream);
   }
 }
 

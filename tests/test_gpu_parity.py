@@ -177,7 +177,7 @@ def random_problem(seed, w, h, c, density=0.6):
 
 
 @pytest.mark.parametrize("cap", [1, 2, 3, 4, 5, 7, 11, 64])
-@pytest.mark.parametrize("cfg", list(range(11)))
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4])
 def test_stops_exactly_at_the_cap(ctx, cap, cfg):
     w, h, c = 150, 90, 2
     src, tgt, mask = random_problem(cap, w, h, c)
@@ -194,7 +194,7 @@ def test_stops_exactly_at_the_cap(ctx, cap, cfg):
         assert r["final_residual"] == r["residual_history"][-1]
 
 
-@pytest.mark.parametrize("cfg", list(range(11)))
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4])
 def test_history_matches_oracle_at_small_sizes(ctx, oracle, cfg):
     # red-black and lexicographic iterates differ, but both must converge to the
     # same fixed point; the GPU history is one FP64 residual per sweep.
@@ -216,39 +216,6 @@ def test_history_matches_oracle_at_small_sizes(ctx, oracle, cfg):
         assert r["final_residual"] == r["residual_history"][-1]
     ref_out, ref_worst, _ = oracle.blend_channels(src, tgt, mask, c, w, h, 4000, 1e-9, 0.05, 1.8)
     assert np.abs(out - ref_out).max() <= 1e-6
-
-
-@pytest.mark.parametrize("banded,twin", [(5, 1), (6, 2), (7, 4), (8, 1), (9, 2), (10, 4)])
-def test_banded_sweep_matches_its_barrier_twin(ctx, banded, twin):
-    """The banded sweep (warps synchronised with their neighbours only) does
-    the same cell arithmetic as the configuration with a block barrier after
-    every half-sweep on the same tiles: the same sweeps, the same stop, and the
-    same result up to the summation order of the FP64 residual partials."""
-    src, tgt, mask = random_problem(71, 333, 257, 3, density=0.7)
-    res = {}
-    for cfg in (banded, twin):
-        ctx.set_config(cfg)
-        try:
-            res[cfg] = ctx.solve(src, tgt, mask, 333, 257, 3, lam=0.01, max_iterations=2000,
-                                 tolerance=1e-8)
-        finally:
-            ctx.set_config(-1)
-    (ob, pb, _), (ot, pt, _) = res[banded], res[twin]
-    assert all(r["converged"] for r in pb) and all(r["converged"] for r in pt)
-    for a, b in zip(pb, pt):
-        assert abs(a["iterations"] - b["iterations"]) <= 1
-        k = min(a["iterations"], b["iterations"])
-        ha, hb = np.array(a["residual_history"][:k]), np.array(b["residual_history"][:k])
-        assert np.allclose(ha, hb, rtol=1e-9, atol=0)
-    assert np.abs(ob.astype(np.float64) - ot).max() <= 1e-6
-    # and reruns of the banded sweep are byte-identical
-    ctx.set_config(banded)
-    try:
-        again, _, _ = ctx.solve(src, tgt, mask, 333, 257, 3, lam=0.01, max_iterations=2000,
-                                tolerance=1e-8)
-    finally:
-        ctx.set_config(-1)
-    assert np.array_equal(again.view(np.uint32), ob.view(np.uint32))
 
 
 def test_non_interior_pixels_equal_target_bitwise(ctx):
