@@ -527,17 +527,25 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
     const double rr = fma(-dd, (double)e, ns) - (double)g;
     return rr * rr;
   };
-  // the four cells of a lane together: each square added in cell order, a
-  // cell that is not interior adds +0.0 (part is a sum of squares, so adding
-  // +0.0 leaves it bit for bit as skipping the cell would)
+  // the four cells of a lane together: each square added in cell order as
+  // fma(r, r, part); a cell that is not interior adds fma(0, 0, part) = part,
+  // bit for bit what skipping it gives
+  auto rval = [&](float l, float r, float u, float dn, float e, float g) -> double {
+    const double ns = (((double)l + (double)r) + (double)u) + (double)dn;
+    return fma(-dd, (double)e, ns) - (double)g;
+  };
   auto resid4 = [&](double &part, uint32_t cc, float L0, float R0, float L1, float R1, float L2, float R2,
                     float L3, float R3, const float4 &up, const float4 &dn, const float4 &e, const float4 &g) {
-    const double r0 = resid(L0, R0, up.x, dn.x, e.x, g.x), r1 = resid(L1, R1, up.y, dn.y, e.y, g.y),
-                 r2 = resid(L2, R2, up.z, dn.z, e.z, g.z), r3 = resid(L3, R3, up.w, dn.w, e.w, g.w);
-    part += (cc & 0xffu) ? r0 : 0.0;
-    part += (cc & 0xff00u) ? r1 : 0.0;
-    part += (cc & 0xff0000u) ? r2 : 0.0;
-    part += (cc & 0xff000000u) ? r3 : 0.0;
+    double r0 = rval(L0, R0, up.x, dn.x, e.x, g.x), r1 = rval(L1, R1, up.y, dn.y, e.y, g.y),
+           r2 = rval(L2, R2, up.z, dn.z, e.z, g.z), r3 = rval(L3, R3, up.w, dn.w, e.w, g.w);
+    r0 = (cc & 0xffu) ? r0 : 0.0;
+    r1 = (cc & 0xff00u) ? r1 : 0.0;
+    r2 = (cc & 0xff0000u) ? r2 : 0.0;
+    r3 = (cc & 0xff000000u) ? r3 : 0.0;
+    part = fma(r0, r0, part);
+    part = fma(r1, r1, part);
+    part = fma(r2, r2, part);
+    part = fma(r3, r3, part);
   };
 
 #pragma unroll
