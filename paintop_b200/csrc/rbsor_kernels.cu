@@ -460,16 +460,12 @@ __global__ void k_emit(KParams P, int sys0, int TW, int TH) {
 // ----------------------------------------------------------------------------
 // the persistent solve kernel
 // ----------------------------------------------------------------------------
-// Sweep variants (bits of VAR): kVarIlp computes a lane's four FP64 residuals
-// together behind one lane-level test, so their conversion and FP64 chains
-// interleave (the owned columns come in whole lanes: HX and TW are multiples
-// of 8); kVarPerm stores the cell-flag rows in slot ly ^ ((ly >> 1) & 1), so
-// the two rows a warp reads (two apart) fall in different shared-memory banks.
-// Both give results bit-identical to VAR = 0.
-constexpr int kVarIlp = 1, kVarPerm = 2;
-__host__ __device__ constexpr int cell_slot(int ly, int var) { return (var & kVarPerm) ? (ly ^ ((ly >> 1) & 1)) : ly; }
+// Cell-flag rows are stored in slot ly ^ ((ly >> 1) & 1): the two rows a warp
+// reads (two apart, one per half-warp) then sit an odd number of 64-byte rows
+// apart, in different shared-memory banks (rows two apart would share all 16).
+__host__ __device__ constexpr int cell_slot(int ly) { return ly ^ ((ly >> 1) & 1); }
 
-template <int S, int TH, int VAR>
+template <int S, int TH>
 __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile &tl, int s,
                            int cur, float *sE, float *sG, uint8_t *sC, double *sred) {
   using G = Geo<S, TH>;
@@ -494,7 +490,7 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
     const int so = c * G::PLANE + ly * kPWL + 4 * v;
     cp_async16(sE + so, ein + o, in);
     cp_async16(sG + so, P.g + o, in);
-    cp_async4(sC + c * G::PLANE + cell_slot(ly, VAR) * kPWL + 4 * v, P.cell + o, in);
+    cp_async4(sC + c * G::PLANE + cell_slot(ly) * kPWL + 4 * v, P.cell + o, in);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -508,7 +504,7 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
   static_assert((G::LH - 2) % 32 == 0, "rows 1..LH-2 must split evenly over the warps");
   static_assert(TH % 4 == 0, "owned rows come in groups of four");
   static_assert(OX0 % 8 == 0 && OX1 % 8 == 0, "owned columns come in whole lanes");
-  static_assert(!(VAR & kVarPerm) || G::LH % 4 == 0 || G::LH % 4 == 2, "cell slots stay inside the plane");
+  static_assert(G::LH % 4 == 0 || G::LH % 4 == 2, "cell slots stay inside the plane");
   constexpr int LO = OX0 / 8, LE = OX1 / 8;         // lanes (l16) whose cells are owned
   constexpr int kRowPairs = (G::LH - 2) / 2;
   // Each lane owns four consecutive plane entries (four cells of one colour) of
@@ -522,11 +518,6 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
 #pragma unroll
   for (int j = 0; j < S; ++j) acc[j] = 0.0;
 
-  auto resid = [&](float l, float r, float u, float dn, float e, float g) -> double {
-    const double ns = (((double)l + (double)r) + (double)u) + (double)dn;
-    const double rr = fma(-dd, (double)e, ns) - (double)g;
-    return rr * rr;
-  };
   // the four cells of a lane together: each square added in cell order as
   // fma(r, r, part); a cell that is not interior adds fma(0, 0, part) = part,
   // bit for bit what skipping it gives
@@ -567,7 +558,7 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
         const float4 up = Eo[r4 - RQ], dn = Eo[r4 + RQ], ct = Eo[r4];
         const float4 gc = Gc[r4];
         const float4 ec = Ec[r4];
-        const uint32_t cc = Cc[cell_slot(ly, VAR) * RQ + l16];
+        const uint32_t cc = Cc[cell_slot(ly) * RQ + l16];
         const float prev = __shfl_up_sync(0xffffffffu, ct.w, 1, 16);
         const float next = __shfl_down_sync(0xffffffffu, ct.x, 1, 16);
         float L0, R0, L1, R1, L2, R2, L3, R3;
@@ -581,17 +572,11 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
         if (cc & 0xff00u) ne.y = fmaf(w, ((((L1 + R1) + up.y) + dn.y) - gc.y) * inv - ec.y, ec.y);
         if (cc & 0xff0000u) ne.z = fmaf(w, ((((L2 + R2) + up.z) + dn.z) - gc.z) * inv - ec.z, ec.z);
         if (cc & 0xff000000u) ne.w = fmaf(w, ((((L3 + R3) + up.w) + dn.w) - gc.w) * inv - ec.w, ec.w);
-        if constexpr ((VAR & kVarIlp) != 0) {
-          if (duty && ly >= OY0 && ly < OY1 && l16 >= LO && l16 < LE && cc != 0u)
-            resid4(part, cc, L0, R0, L1, R1, L2, R2, L3, R3, up, dn, h ? ne : ec, gc);
-        } else if (duty && ly >= OY0 && ly < OY1) {
-          const int x0 = 8 * l16 + q;  // loaded column of the lane's first cell
-          const float4 ee = h ? ne : ec;  // black: state j after its update; red: state j-1
-          if ((cc & 0xffu) && x0 >= OX0 && x0 < OX1) part += resid(L0, R0, up.x, dn.x, ee.x, gc.x);
-          if ((cc & 0xff00u) && x0 + 2 >= OX0 && x0 + 2 < OX1) part += resid(L1, R1, up.y, dn.y, ee.y, gc.y);
-          if ((cc & 0xff0000u) && x0 + 4 >= OX0 && x0 + 4 < OX1) part += resid(L2, R2, up.z, dn.z, ee.z, gc.z);
-          if ((cc & 0xff000000u) && x0 + 6 >= OX0 && x0 + 6 < OX1) part += resid(L3, R3, up.w, dn.w, ee.w, gc.w);
-        }
+        // a lane's four residuals together behind one lane-level test, so their
+        // conversion and FP64 chains interleave (the owned columns come in whole
+        // lanes: HX and TW are multiples of 8)
+        if (duty && ly >= OY0 && ly < OY1 && l16 >= LO && l16 < LE && cc != 0u)
+          resid4(part, cc, L0, R0, L1, R1, L2, R2, L3, R3, up, dn, h ? ne : ec, gc);
         Ec[r4] = ne;
       }
       if (h == 1) acc[j] += part;
@@ -613,7 +598,7 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
       const int r4 = ly * RQ + l16;
       const float4 up = Eb[r4 - RQ], dn = Eb[r4 + RQ], ct = Eb[r4];
       const float4 gc = Gr[r4], ec = Er[r4];
-      const uint32_t cc = Cr[cell_slot(ly, VAR) * RQ + l16];
+      const uint32_t cc = Cr[cell_slot(ly) * RQ + l16];
       const float prev = __shfl_up_sync(0xffffffffu, ct.w, 1, 16);
       const float next = __shfl_down_sync(0xffffffffu, ct.x, 1, 16);
       float L0, R0, L1, R1, L2, R2, L3, R3;
@@ -622,15 +607,7 @@ __device__ void sweep_tile(const KParams &P, const SysDesc &d, int t, const Tile
       } else {
         L0 = ct.x; R0 = ct.y; L1 = ct.y; R1 = ct.z; L2 = ct.z; R2 = ct.w; L3 = ct.w; R3 = next;
       }
-      if constexpr ((VAR & kVarIlp) != 0) {
-        if (l16 >= LO && l16 < LE && cc != 0u) resid4(part, cc, L0, R0, L1, R1, L2, R2, L3, R3, up, dn, ec, gc);
-      } else {
-        const int x0 = 8 * l16 + q;
-        if ((cc & 0xffu) && x0 >= OX0 && x0 < OX1) part += resid(L0, R0, up.x, dn.x, ec.x, gc.x);
-        if ((cc & 0xff00u) && x0 + 2 >= OX0 && x0 + 2 < OX1) part += resid(L1, R1, up.y, dn.y, ec.y, gc.y);
-        if ((cc & 0xff0000u) && x0 + 4 >= OX0 && x0 + 4 < OX1) part += resid(L2, R2, up.z, dn.z, ec.z, gc.z);
-        if ((cc & 0xff000000u) && x0 + 6 >= OX0 && x0 + 6 < OX1) part += resid(L3, R3, up.w, dn.w, ec.w, gc.w);
-      }
+      if (l16 >= LO && l16 < LE && cc != 0u) resid4(part, cc, L0, R0, L1, R1, L2, R2, L3, R3, up, dn, ec, gc);
     }
 #pragma unroll
     for (int j = 0; j < S; ++j)
@@ -879,7 +856,7 @@ __device__ int claim_tile(const KParams &P, int rot, int *idx, unsigned *gen,
   }
 }
 
-template <int S, int TH, int VAR>
+template <int S, int TH>
 __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
   using G = Geo<S, TH>;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -915,7 +892,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
     const int s = __ldcg(&stp->s);
     const int cur = __ldcg(&stp->cur);
     if (mode == M_SWEEP || mode == M_REDO) {
-      sweep_tile<S, TH, VAR>(P, d, t, tl, s, cur, sE, sG, sC, sred);
+      sweep_tile<S, TH>(P, d, t, tl, s, cur, sE, sG, sC, sred);
     } else if (mode == M_FOLD) {
       fold_tile<S, TH>(P, d, tl, cur);
     } else {
@@ -963,14 +940,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(KParams P) {
 // ----------------------------------------------------------------------------
 // launch entry points (host)
 // ----------------------------------------------------------------------------
-template <int S, int TH, int VAR>
+template <int S, int TH>
 static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
   using G = Geo<S, TH>;
-  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_solve<S, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)G::kSmem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH, VAR>, kThreads, G::kSmem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<S, TH>, kThreads, G::kSmem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int grid = per_sm * sms;
@@ -979,41 +956,36 @@ static cudaError_t prepare_solve_t(const KParams &P, int sms, int *grid_out) {
   return cudaSuccess;
 }
 
-template <int S, int TH, int VAR>
+template <int S, int TH>
 static cudaError_t launch_prepared_t(const KParams &P, int grid, cudaStream_t stream) {
   using G = Geo<S, TH>;
   KParams Pc = P;
   Pc.S = S;
   // No block waits for a particular other block (work is claimed, never
   // assigned), so an ordinary launch suffices; the grid fills the GPU once.
-  k_solve<S, TH, VAR><<<grid, kThreads, G::kSmem, stream>>>(Pc);
+  k_solve<S, TH><<<grid, kThreads, G::kSmem, stream>>>(Pc);
   return cudaGetLastError();
 }
 
-// (sweeps per step S, owned tile height TH); every loaded height TH + 2(2S+1)
-// leaves rows 1..LH-2 a multiple of 32. Configurations 5-8 are the sweep
-// variants (kVarIlp, kVarIlp | kVarPerm) on the tiles of 2, 4 and 1.
-int tile_config_count() { return 9; }
+int tile_config_count() { return 5; }
 
+// (sweeps per step S, owned tile height TH); every loaded height TH + 2(2S+1)
+// leaves rows 1..LH-2 a multiple of 32.
 TileConfig tile_config(int idx) {
   switch (idx) {
     case 0: return {1, 60, tile_w(1)};
     case 1: return {2, 88, tile_w(2)};
     case 2: return {3, 84, tile_w(3)};
     case 3: return {3, 52, tile_w(3)};
-    case 4: return {4, 80, tile_w(4)};
-    case 5: return {3, 84, tile_w(3)};
-    case 6: return {3, 84, tile_w(3)};
-    case 7: return {4, 80, tile_w(4)};
-    default: return {2, 88, tile_w(2)};
+    default: return {4, 80, tile_w(4)};
   }
 }
 
 size_t tile_config_smem(int idx) {
   switch (idx) {
     case 0: return Geo<1, 60>::kSmem;
-    case 1: case 8: return Geo<2, 88>::kSmem;
-    case 2: case 5: case 6: return Geo<3, 84>::kSmem;
+    case 1: return Geo<2, 88>::kSmem;
+    case 2: return Geo<3, 84>::kSmem;
     case 3: return Geo<3, 52>::kSmem;
     default: return Geo<4, 80>::kSmem;
   }
@@ -1042,29 +1014,21 @@ cudaError_t launch_assembly(const KParams &P, const TileConfig &tc, cudaStream_t
 
 cudaError_t prepare_solve(const KParams &P, int cfg, int sms, int *grid) {
   switch (cfg) {
-    case 0: return prepare_solve_t<1, 60, 0>(P, sms, grid);
-    case 1: return prepare_solve_t<2, 88, 0>(P, sms, grid);
-    case 2: return prepare_solve_t<3, 84, 0>(P, sms, grid);
-    case 3: return prepare_solve_t<3, 52, 0>(P, sms, grid);
-    case 4: return prepare_solve_t<4, 80, 0>(P, sms, grid);
-    case 5: return prepare_solve_t<3, 84, kVarIlp>(P, sms, grid);
-    case 6: return prepare_solve_t<3, 84, kVarIlp | kVarPerm>(P, sms, grid);
-    case 7: return prepare_solve_t<4, 80, kVarIlp | kVarPerm>(P, sms, grid);
-    default: return prepare_solve_t<2, 88, kVarIlp | kVarPerm>(P, sms, grid);
+    case 0: return prepare_solve_t<1, 60>(P, sms, grid);
+    case 1: return prepare_solve_t<2, 88>(P, sms, grid);
+    case 2: return prepare_solve_t<3, 84>(P, sms, grid);
+    case 3: return prepare_solve_t<3, 52>(P, sms, grid);
+    default: return prepare_solve_t<4, 80>(P, sms, grid);
   }
 }
 
 cudaError_t launch_prepared(const KParams &P, int cfg, int grid, cudaStream_t stream) {
   switch (cfg) {
-    case 0: return launch_prepared_t<1, 60, 0>(P, grid, stream);
-    case 1: return launch_prepared_t<2, 88, 0>(P, grid, stream);
-    case 2: return launch_prepared_t<3, 84, 0>(P, grid, stream);
-    case 3: return launch_prepared_t<3, 52, 0>(P, grid, stream);
-    case 4: return launch_prepared_t<4, 80, 0>(P, grid, stream);
-    case 5: return launch_prepared_t<3, 84, kVarIlp>(P, grid, stream);
-    case 6: return launch_prepared_t<3, 84, kVarIlp | kVarPerm>(P, grid, stream);
-    case 7: return launch_prepared_t<4, 80, kVarIlp | kVarPerm>(P, grid, stream);
-    default: return launch_prepared_t<2, 88, kVarIlp | kVarPerm>(P, grid, stream);
+    case 0: return launch_prepared_t<1, 60>(P, grid, stream);
+    case 1: return launch_prepared_t<2, 88>(P, grid, stream);
+    case 2: return launch_prepared_t<3, 84>(P, grid, stream);
+    case 3: return launch_prepared_t<3, 52>(P, grid, stream);
+    default: return launch_prepared_t<4, 80>(P, grid, stream);
   }
 }
 

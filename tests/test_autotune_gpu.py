@@ -14,7 +14,7 @@ import pytest
 
 TOL_ABS = 1e-6  # agreement between two solves of the same system to rel-res 1e-9
 MARGIN = 0.05   # autotune.cpp, kReplaceMargin
-NCFG = 9        # tile configurations (pt_tile_config_count)
+NCFG = 5        # tile configurations (pt_tile_config_count)
 
 
 def _problems():

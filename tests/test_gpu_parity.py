@@ -177,7 +177,7 @@ def random_problem(seed, w, h, c, density=0.6):
 
 
 @pytest.mark.parametrize("cap", [1, 2, 3, 4, 5, 7, 11, 64])
-@pytest.mark.parametrize("cfg", list(range(9)))
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4])
 def test_stops_exactly_at_the_cap(ctx, cap, cfg):
     w, h, c = 150, 90, 2
     src, tgt, mask = random_problem(cap, w, h, c)
@@ -194,7 +194,7 @@ def test_stops_exactly_at_the_cap(ctx, cap, cfg):
         assert r["final_residual"] == r["residual_history"][-1]
 
 
-@pytest.mark.parametrize("cfg", list(range(9)))
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4])
 def test_history_matches_oracle_at_small_sizes(ctx, oracle, cfg):
     # red-black and lexicographic iterates differ, but both must converge to the
     # same fixed point; the GPU history is one FP64 residual per sweep.
@@ -216,29 +216,6 @@ def test_history_matches_oracle_at_small_sizes(ctx, oracle, cfg):
         assert r["final_residual"] == r["residual_history"][-1]
     ref_out, ref_worst, _ = oracle.blend_channels(src, tgt, mask, c, w, h, 4000, 1e-9, 0.05, 1.8)
     assert np.abs(out - ref_out).max() <= 1e-6
-
-
-@pytest.mark.parametrize("variant,base", [(5, 2), (6, 2), (7, 4), (8, 1)])
-def test_sweep_variants_are_bit_identical_to_their_base(ctx, variant, base):
-    """The sweep variants change only control flow (a lane's four FP64
-    residuals behind one test) and the shared-memory rows of the cell flags:
-    output, reports and residual history equal the base configuration's bit
-    for bit, on a ragged mask with several channels and on the screened star."""
-    from paintop_b200 import synth
-    star = synth.screened_2048(3, size=384)
-    cases = [random_problem(71, 333, 257, 3, density=0.7) + (333, 257, 3, 0.01),
-             (star.source.reshape(-1), star.target.reshape(-1), star.mask.reshape(-1), 384, 384, 4, 0.01)]
-    for src, tgt, mask, w, h, c, lam in cases:
-        res = {}
-        for cfg in (variant, base):
-            ctx.set_config(cfg)
-            try:
-                res[cfg] = ctx.solve(src, tgt, mask, w, h, c, lam=lam, max_iterations=2000, tolerance=1e-8)
-            finally:
-                ctx.set_config(-1)
-        (ov, pv, wv), (ob, pb, wb) = res[variant], res[base]
-        assert np.array_equal(ov.view(np.uint32), ob.view(np.uint32))
-        assert pv == pb and wv == wb
 
 
 def test_non_interior_pixels_equal_target_bitwise(ctx):
