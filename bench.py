@@ -879,6 +879,7 @@ def gpu_arm(args):
     clocks = sampler.stop()
     converged = all(reps[c].converged for c in range(C))
     worst_res = max(reps[c].final_residual for c in range(C))
+    head_cfg = ctx.last_config()  # the timed solves' tile configuration (later legs change it)
     sor_out = out_d.cpu().numpy()  # the last timed solve's result, for the parity statement
 
     # ---- end-to-end arm (pinned host buffers through the C ABI) --------------
@@ -960,7 +961,7 @@ def gpu_arm(args):
             "clocks": clocks,
             "solver": {"iterations_per_channel": iters[-1], "refinements": refines[-1],
                        "converged": converged, "worst_final_residual": worst_res,
-                       "tile_config": tile_config_label(ctx.last_config()),
+                       "tile_config": tile_config_label(head_cfg),
                        "tuned_entry": tuned_entry([dict(width=W, height=H, channels=C,
                                                         lam=WORKLOAD["lam"])])},
             "multigrid": multigrid,
