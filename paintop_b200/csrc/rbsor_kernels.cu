@@ -92,9 +92,12 @@ __device__ __forceinline__ bool interior_at(const SysDesc &d, int x, int y) {
 
 // Interior cells per tile (owned region only) and their bounding box. min/max
 // are order-independent, so the box is deterministic.
+// The channels of an image share its mask, so only channel 0's blocks count;
+// they store the count and box for every channel's copy of the tile.
 __global__ void k_tile_count(KParams P, int TW, int TH) {
   const Tile tl = P.tiles[blockIdx.x];
   const SysDesc d = P.sys[tl.sys];
+  if (d.chan != 0) return;
   __shared__ int s[32];
   __shared__ int sb[4];
   if (threadIdx.x < 4) sb[threadIdx.x] = (threadIdx.x < 2) ? 0x7fffffff : -1;
@@ -117,8 +120,13 @@ __global__ void k_tile_count(KParams P, int TW, int TH) {
   if (threadIdx.x == 0) {
     int t = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
-    P.tcount[blockIdx.x] = t;
-    P.tbox[blockIdx.x] = make_int4(sb[0], sb[1], sb[2], sb[3]);
+    const int4 box = make_int4(sb[0], sb[1], sb[2], sb[3]);
+    const int local = (int)blockIdx.x - d.tile0;  // the tile's index within its system
+    for (int c = 0; c < d.C; ++c) {
+      const int tt = P.sys[tl.sys + c].tile0 + local;
+      P.tcount[tt] = t;
+      P.tbox[tt] = box;
+    }
   }
 }
 
@@ -147,7 +155,18 @@ __device__ __forceinline__ double anchor_residual(const SysDesc &d, long long px
 // poisson.rs:315-321 (residual), operand for operand.
 __global__ void __launch_bounds__(kThreads) k_assemble(KParams P, int TW, int TH) {
   __shared__ double sred[kWarps];
-  const int t = blockIdx.x;
+  // Block order: within each image, its channels' copies of a tile come one
+  // after another, so the interleaved source and target pixels a tile reads
+  // are still in L2 for the other channels' blocks. The tiles of an image are
+  // channel 0's, then channel 1's, ...; block b of the image takes channel
+  // b % C's tile b / C.
+  int t = blockIdx.x;
+  {
+    const SysDesc &d0 = P.sys[P.tiles[t].sys];
+    const int base = d0.tile0 - d0.chan * d0.ntiles;  // the image's first tile
+    const int local = t - base;
+    t = base + (local % d0.C) * d0.ntiles + local / d0.C;
+  }
   const Tile tl = P.tiles[t];
   const SysDesc d = P.sys[tl.sys];
   if (!tile_support(P, d, tl.tx, tl.ty)) return;
@@ -440,19 +459,38 @@ __global__ void k_compact(KParams P) {
 __global__ void k_emit(KParams P, int sys0, int TW, int TH) {
   const SysDesc d0 = P.sys[sys0];
   const long long npx = (long long)d0.W * d0.H;
+  const int C = d0.C;
+  // four channels with 16-byte aligned images: one vector load and store per pixel
+  const bool vec4 = C == 4 && ((reinterpret_cast<uintptr_t>(d0.tgt) | reinterpret_cast<uintptr_t>(d0.out)) & 15) == 0;
   for (long long px = blockIdx.x * (long long)blockDim.x + threadIdx.x; px < npx;
        px += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(px / d0.W), x = (int)(px - (long long)y * d0.W);
     const int tx = x / TW, ty = y / TH;
     const int c = (x + y) & 1, i = x >> 1;
-    for (int ch = 0; ch < d0.C; ++ch) {
+    // the channels share the tile counts (k_tile_count stores one per channel)
+    const bool active = P.tcount[d0.tile0 + ty * d0.ntx + tx] > 0;
+    if (vec4) {
+      float4 v = *reinterpret_cast<const float4 *>(d0.tgt + px * 4);
+      if (active) {
+        float *vv = reinterpret_cast<float *>(&v);
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          if (P.st[sys0 + ch].out_anchor) continue;
+          const long long o = plane_index(P.sys[sys0 + ch], c, y, i);
+          if (P.cell[o]) vv[ch] = (float)P.u[o];
+        }
+      }
+      *reinterpret_cast<float4 *>(d0.out + px * 4) = v;
+      continue;
+    }
+    for (int ch = 0; ch < C; ++ch) {
       const SysDesc &d = P.sys[sys0 + ch];
-      float v = d.tgt[px * d.C + ch];
-      if (P.tcount[d.tile0 + ty * d.ntx + tx] > 0 && !P.st[sys0 + ch].out_anchor) {
+      float v = d.tgt[px * C + ch];
+      if (active && !P.st[sys0 + ch].out_anchor) {
         const long long o = plane_index(d, c, y, i);
         if (P.cell[o]) v = (float)P.u[o];
       }
-      d.out[px * d.C + ch] = v;
+      d.out[px * C + ch] = v;
     }
   }
 }
