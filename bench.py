@@ -1193,11 +1193,17 @@ def clone_leg(ctx, dev, with_cpu: bool = True) -> dict:
         out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": 1, "kind": "port",
                                "sample": f"seed 1, omega 1.9 ({dt:.2f} s, worst-channel sweeps {worst.iterations})"}
         tight, info = tight_oracle(i0, 0.0)
-        out["parity"] = {"oracle": info, "note": "seed 1; rel-res 1e-5 leaves an error set by the slowest mode "
-                                                 "for every method, the CPU op's included",
-                         "cpu_op_vs_oracle": error_stats(ref, tight),
-                         **{f"{n}_vs_oracle": error_stats(v, tight) for n, v in first.items()},
-                         **{f"{n}_vs_cpu_op": error_stats(v, ref) for n, v in first.items()}}
+        cpu_err = error_stats(ref, tight)
+        gpu_err = {n: error_stats(v, tight) for n, v in first.items()}
+        out["parity"] = {
+            "oracle": info,
+            "bar": "max error against the FP64 oracle at most twice the CPU op's own (tests/test_gpu_parity.py, "
+                   "test_clone_512_against_oracles): at rel-res 1e-5 on pure Poisson the error is set by the "
+                   "slowest mode for every method, the reference op's included, so the bounded tier is not the bar",
+            "cpu_op_vs_oracle": cpu_err,
+            **{f"{n}_vs_oracle": e for n, e in gpu_err.items()},
+            **{f"{n}_vs_cpu_op": error_stats(v, ref) for n, v in first.items()},
+            "within_bar": {n: e["max_abs"] <= 2.0 * cpu_err["max_abs"] for n, e in gpu_err.items()}}
     return out
 
 
