@@ -29,29 +29,6 @@ struct pt_ctx {
   cudaGraphExec_t mgexec[2] = {nullptr, nullptr};  // multigrid-CG iteration: first / later
   std::string mgkey;           // the problem shape and arena the multigrid graphs were captured for
   long long mgnodes = 0;       // kernels in one of those iterations
-  // host-buffer solves: row bands of an output that hold no interior tile are
-  // copied back from the staged target on `stream2` while the solve runs
-  cudaStream_t stream2 = nullptr;
-  cudaEvent_t band_ev = nullptr;   // the band flags are on the host
-  cudaEvent_t side_ev = nullptr;   // stream2's copies are done
-  int *band_host = nullptr;        // pinned: one flag per band of every image
-  size_t band_cap = 0;
-
-  bool reserve_bands(size_t n) {
-    if (!stream2 && cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking) != cudaSuccess) return false;
-    if (!band_ev && cudaEventCreateWithFlags(&band_ev, cudaEventDisableTiming) != cudaSuccess) return false;
-    if (!side_ev && cudaEventCreateWithFlags(&side_ev, cudaEventDisableTiming) != cudaSuccess) return false;
-    if (n <= band_cap) return true;
-    if (band_host) cudaFreeHost(band_host);
-    band_host = nullptr;
-    band_cap = 0;
-    if (cudaHostAlloc(reinterpret_cast<void **>(&band_host), n * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
-      band_host = nullptr;
-      return false;
-    }
-    band_cap = n;
-    return true;
-  }
 
   void drop_graphs() {
     if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }  // they point into the arena
@@ -89,10 +66,6 @@ struct pt_ctx {
     drop_graphs();
     for (auto &e : ev)
       if (e) { cudaEventDestroy(e); e = nullptr; }
-    if (stream2) { cudaStreamSynchronize(stream2); cudaStreamDestroy(stream2); stream2 = nullptr; }
-    if (band_ev) { cudaEventDestroy(band_ev); band_ev = nullptr; }
-    if (side_ev) { cudaEventDestroy(side_ev); side_ev = nullptr; }
-    if (band_host) { cudaFreeHost(band_host); band_host = nullptr; band_cap = 0; }
     if (arena) cudaFree(arena);
     arena = nullptr;
     arena_cap = 0;

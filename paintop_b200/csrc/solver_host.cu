@@ -93,16 +93,8 @@ struct Plan {
 // Arena layout (byte offsets) for one call.
 struct Layout {
   size_t sys, st, claim, arrive, tiles, tcount, tbox, act, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in,
-      mask, out, regions, label, rsize, rmax, bands, total;
+      mask, out, regions, label, rsize, rmax, total;
 };
-
-// Row bands of every image (one flag each for the early copy of host outputs).
-size_t band_count(const Plan &pl) {
-  size_t n = 0;
-  for (const SysDesc &d : pl.sys)
-    if (d.chan == 0) n += (size_t)d.nty;
-  return n;
-}
 
 Layout layout(const Plan &pl, bool stage) {
   Layout L{};
@@ -135,7 +127,6 @@ Layout layout(const Plan &pl, bool stage) {
   L.label = take((size_t)pl.rpix * sizeof(int));
   L.rsize = take((size_t)pl.rpix * sizeof(int));
   L.rmax = take(pl.regions.size() * sizeof(int));
-  L.bands = stage ? take(band_count(pl) * sizeof(int)) : 0;
   L.total = o;
   return L;
 }
@@ -241,8 +232,6 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (!ctx->reserve(L.total)) return fail(ctx, PT_OOM, "device arena allocation failed");
   char *base = static_cast<char *>(ctx->arena);
   cudaStream_t st = ctx->stream;
-  if (!devptr && !ctx->reserve_bands(band_count(pl)))
-    return fail(ctx, PT_OOM, "pinned band-flag allocation failed");
   for (auto &e : ctx->ev)
     if (!e && cudaEventCreate(&e) != cudaSuccess) return fail(ctx, PT_LAUNCH_FAILED, "event create");
   cudaEventRecord(ctx->ev[0], st);
@@ -329,7 +318,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   ctx->last_grid = grid;
   ctx->last_cfg = pl.cfg;
   long long launches = 5;  // tile count, compaction, assembly, init, solve
-  for (uint32_t i = 0; i < n; ++i) launches += ps[i].channels > 0 ? (devptr ? 1 : 2) : 0;  // emits, band flags
+  for (uint32_t i = 0; i < n; ++i) launches += ps[i].channels > 0 ? 1 : 0;  // emits
 
   // Everything from here to the results is stream work on the device: with
   // device pointers it is captured once into a CUDA graph and replayed while
@@ -345,19 +334,6 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     cudaError_t e = cudaMemsetAsync(base + L.bar, 0, kBarWords * sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.err, 0, sizeof(int), st);
     if (e == cudaSuccess) e = launch_assembly(P, pl.tc, st, any_warm);
-    if (!devptr && e == cudaSuccess) {
-      // which row bands hold interior tiles: on the host long before the solve ends
-      int *bands = reinterpret_cast<int *>(base + L.bands);
-      size_t boff = 0;
-      for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) {
-        if (ps[i].channels == 0) continue;
-        e = launch_band_flags(P, sys0[i], bands + boff, st);
-        boff += (size_t)pl.sys[sys0[i]].nty;
-      }
-      if (e == cudaSuccess && boff)
-        e = cudaMemcpyAsync(ctx->band_host, bands, boff * sizeof(int), cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaEventRecord(ctx->band_ev, st);
-    }
     if (e == cudaSuccess) e = record(ctx->ev[1], capturing);
     if (e == cudaSuccess) e = launch_prepared(P, pl.cfg, grid, st);
     if (e == cudaSuccess) e = record(ctx->ev[2], capturing);
@@ -408,32 +384,11 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   ce = cudaMemcpyAsync(states.data(), base + L.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&kerr, base + L.err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (!devptr && ce == cudaSuccess) {
-    // Row bands without an interior tile output the target: copy them from the
-    // staged target on the side stream while the solve still runs; the other
-    // bands follow the emit on the main stream. Each run of equal bands is one
-    // copy. The host waits here only for the uploads and the assembly.
-    ce = cudaEventSynchronize(ctx->band_ev);
-    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(ctx->stream2, ctx->band_ev, 0);
-    size_t boff = 0;
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
       if (ps[i].channels == 0) continue;
-      const SysDesc &d0 = pl.sys[sys0[i]];
-      const size_t row = (size_t)ps[i].width * ps[i].channels, TH = (size_t)pl.tc.th;
-      const int *flags = ctx->band_host + boff;
-      for (int ty = 0; ty < d0.nty && ce == cudaSuccess;) {
-        int ty1 = ty + 1;
-        while (ty1 < d0.nty && flags[ty1] == flags[ty]) ++ty1;
-        const size_t r0 = ty * TH, r1 = std::min((size_t)ps[i].height, ty1 * TH);
-        const float *from = flags[ty] ? d0.out : d0.tgt;
-        ce = cudaMemcpyAsync(outs[i] + r0 * row, from + r0 * row, (r1 - r0) * row * sizeof(float),
-                             cudaMemcpyDeviceToHost, flags[ty] ? st : ctx->stream2);
-        ty = ty1;
-      }
-      boff += (size_t)d0.nty;
+      const size_t nf = (size_t)ps[i].width * ps[i].height * ps[i].channels;
+      ce = cudaMemcpyAsync(outs[i], pl.sys[sys0[i]].out, nf * sizeof(float), cudaMemcpyDeviceToHost, st);
     }
-    if (ce == cudaSuccess) ce = cudaEventRecord(ctx->side_ev, ctx->stream2);
-    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, ctx->side_ev, 0);
-    if (ce != cudaSuccess) cudaStreamSynchronize(ctx->stream2);
   }
   if (histories && !devptr && ce == cudaSuccess) {
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
