@@ -29,7 +29,7 @@ EXPORTED = (
     "pt_ctx_create", "pt_ctx_destroy", "pt_poisson_solve", "pt_poisson_solve_batch",
     "pt_op_compute", "pt_op_compute_ex", "pt_status_str", "pt_ctx_last_error", "pt_tile_config_count",
     "pt_tile_config_info", "pt_ctx_set_config", "pt_ctx_last_config", "pt_autotune",
-    "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_poisson_solve_noalloc",
+    "pt_ctx_set_budget", "pt_ctx_stream", "pt_ctx_last_timing", "pt_ctx_last_transfer", "pt_poisson_solve_noalloc",
     "pt_unet_create", "pt_unet_destroy", "pt_unet_param_count", "pt_unet_get_params",
     "pt_unet_set_params", "pt_unet_features", "pt_unet_forward", "pt_unet_loss_grad",
     "pt_unet_train_step", "pt_unet_save", "pt_unet_load", "pt_unet_guess", "pt_unet_grad_record",
@@ -142,6 +142,8 @@ def lib():
     L.pt_ctx_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                      C.POINTER(C.c_int64)]
     L.pt_ctx_last_timing.restype = C.c_int
+    L.pt_ctx_last_transfer.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.pt_ctx_last_transfer.restype = C.c_int
     L.pt_poisson_solve_noalloc.argtypes = [C.POINTER(PtProblem), vp, C.POINTER(PtReport), vp, vp]
     L.pt_poisson_solve_noalloc.restype = C.c_int
     u64, f32 = C.c_uint64, C.c_float
@@ -245,6 +247,12 @@ class Context:
         a, b, n = C.c_double(), C.c_double(), C.c_int64()
         lib().pt_ctx_last_timing(self.h, C.byref(a), C.byref(b), C.byref(n))
         return a.value, b.value, int(n.value)
+
+    def last_transfer(self):
+        """(host->device bytes, device->host bytes) of the last red-black solve call."""
+        a, b = C.c_uint64(), C.c_uint64()
+        lib().pt_ctx_last_transfer(self.h, C.byref(a), C.byref(b))
+        return int(a.value), int(b.value)
 
     def last_config(self) -> int:
         return int(lib().pt_ctx_last_config(self.h))

@@ -23,6 +23,7 @@ struct pt_ctx {
   double last_solve_ms = 0.0;  // persistent kernel, CUDA events on `stream`
   double last_call_ms = 0.0;   // whole call from first upload to last download
   long long last_launches = 0; // kernels launched by the last call
+  unsigned long long last_h2d = 0, last_d2h = 0;  // bytes the last solve moved each way
   bool graphs = true;          // capture device-pointer solves into a CUDA graph
   cudaGraphExec_t gexec = nullptr;
   std::string gkey;            // the plan the cached graph was captured for

@@ -312,6 +312,7 @@ pt_status mask_finish(pt_ctx *ctx, size_t npx, bool device_out, float *mask, con
   ctx->last_solve_ms = a;
   ctx->last_call_ms = b;
   ctx->last_launches = launches;
+  ctx->last_h2d = ctx->last_d2h = 0;  // not counted on this path
   return PT_OK;
 }
 

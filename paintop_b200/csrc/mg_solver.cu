@@ -1355,6 +1355,7 @@ pt_status ptk_solve_mg_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, floa
     ctx->last_solve_ms = solve_ms;
     ctx->last_call_ms = call_ms;
     ctx->last_launches = launches;
+    ctx->last_h2d = ctx->last_d2h = 0;  // not counted on this path
   }
   return PT_OK;
 }

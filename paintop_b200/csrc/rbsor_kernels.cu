@@ -495,6 +495,19 @@ __global__ void k_emit(KParams P, int sys0, int TW, int TH) {
   }
 }
 
+// flags[ty] = 1 if row band ty (tile rows ty * TH ...) of image sys0 holds a
+// tile with interior cells, else 0. The solve reads an image's source and
+// target only in those bands and one row either side; the output of every
+// other band is the target, bit for bit (k_emit).
+__global__ void k_band_flags(KParams P, int sys0, int *flags) {
+  const SysDesc d = P.sys[sys0];
+  for (int ty = threadIdx.x; ty < d.nty; ty += blockDim.x) {
+    int any = 0;
+    for (int tx = 0; tx < d.ntx && !any; ++tx) any = P.tcount[d.tile0 + ty * d.ntx + tx] > 0;
+    flags[ty] = any;
+  }
+}
+
 // ----------------------------------------------------------------------------
 // the persistent solve kernel
 // ----------------------------------------------------------------------------
@@ -1074,6 +1087,17 @@ cudaError_t launch_solve(const KParams &P, int cfg, int sms, cudaStream_t stream
   cudaError_t e = prepare_solve(P, cfg, sms, grid);
   if (e != cudaSuccess) return e;
   return launch_prepared(P, cfg, *grid, stream);
+}
+
+cudaError_t launch_tile_count(const KParams &P, const TileConfig &tc, cudaStream_t stream) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_tile_count<<<P.ntiles, 256, 0, stream>>>(P, tc.tw, tc.th);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_flags(const KParams &P, int sys0, int *flags, cudaStream_t stream) {
+  k_band_flags<<<1, 256, 0, stream>>>(P, sys0, flags);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,

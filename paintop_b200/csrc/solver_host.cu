@@ -93,8 +93,16 @@ struct Plan {
 // Arena layout (byte offsets) for one call.
 struct Layout {
   size_t sys, st, claim, arrive, tiles, tcount, tbox, act, e0, e1, g, cell, u, bp, partial, fpart, hist, bar, err, in,
-      mask, out, regions, label, rsize, rmax, total;
+      mask, out, regions, label, rsize, rmax, bands, total;
 };
+
+// Row bands of every image (one flag each, host-buffer solves).
+size_t band_count(const Plan &pl) {
+  size_t n = 0;
+  for (const SysDesc &d : pl.sys)
+    if (d.chan == 0) n += (size_t)d.nty;
+  return n;
+}
 
 Layout layout(const Plan &pl, bool stage) {
   Layout L{};
@@ -127,6 +135,7 @@ Layout layout(const Plan &pl, bool stage) {
   L.label = take((size_t)pl.rpix * sizeof(int));
   L.rsize = take((size_t)pl.rpix * sizeof(int));
   L.rmax = take(pl.regions.size() * sizeof(int));
+  L.bands = stage ? take(band_count(pl) * sizeof(int)) : 0;
   L.total = o;
   return L;
 }
@@ -237,6 +246,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   cudaEventRecord(ctx->ev[0], st);
 
   // ---- stage inputs and bind the per-system image pointers
+  unsigned long long h2d = 0, d2h = 0;  // bytes moved by this call
   {
     size_t in_off = 0, mask_off = 0, out_off = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -247,16 +257,13 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
                   *guess = p.initial_guess;
       float *out = outs[i];
       if (!devptr) {
+        // only the mask goes up now: which rows of the images the solve reads
+        // is known once the tiles are counted (upload_active_rows below)
         float *in = reinterpret_cast<float *>(base + L.in) + in_off;
         float *dm = reinterpret_cast<float *>(base + L.mask) + mask_off;
-        ce = cudaMemcpyAsync(in, src, nf * sizeof(float), cudaMemcpyHostToDevice, st);
-        if (ce == cudaSuccess)
-          ce = cudaMemcpyAsync(in + nf, tgt, nf * sizeof(float), cudaMemcpyHostToDevice, st);
-        if (ce == cudaSuccess)
-          ce = cudaMemcpyAsync(dm, mask, img * sizeof(float), cudaMemcpyHostToDevice, st);
-        if (ce == cudaSuccess && (p.flags & PT_FLAG_WARM_START))
-          ce = cudaMemcpyAsync(in + 2 * nf, guess, nf * sizeof(float), cudaMemcpyHostToDevice, st);
-        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "input upload");
+        ce = cudaMemcpyAsync(dm, mask, img * sizeof(float), cudaMemcpyHostToDevice, st);
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "mask upload");
+        h2d += img * sizeof(float);
         src = in; tgt = in + nf; mask = dm;
         guess = (p.flags & PT_FLAG_WARM_START) ? in + 2 * nf : nullptr;
         out = reinterpret_cast<float *>(base + L.out) + out_off;
@@ -271,6 +278,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       }
     }
   }
+  h2d += pl.sys.size() * sizeof(SysDesc) + pl.tiles.size() * sizeof(Tile) + pl.regions.size() * sizeof(RegionDesc);
   ce = cudaMemcpyAsync(base + L.sys, pl.sys.data(), pl.sys.size() * sizeof(SysDesc),
                        cudaMemcpyHostToDevice, st);
   if (ce == cudaSuccess)
@@ -312,13 +320,67 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   P.rsize = reinterpret_cast<int *>(base + L.rsize);
   P.rmax = reinterpret_cast<int *>(base + L.rmax);
 
+  // ---- host buffers: upload only the rows the solve reads. The tiles are
+  // counted from the masks, and for each image the row bands that hold an
+  // interior tile come back to the host (one int per band). The solve reads
+  // source, target and guess only at interior cells and their four
+  // neighbours, so those bands and one row either side go up; the output rows
+  // of the other bands are the target bit for bit and are filled on the host
+  // while the GPU works.
+  std::vector<int> bandf;
+  if (!devptr) {
+    int *bands = reinterpret_cast<int *>(base + L.bands);
+    ce = launch_tile_count(P, pl.tc, st);
+    size_t nb = 0;
+    for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
+      if (ps[i].channels == 0) continue;
+      ce = launch_band_flags(P, sys0[i], bands + nb, st);
+      nb += (size_t)pl.sys[sys0[i]].nty;
+    }
+    bandf.assign(nb, 0);
+    if (ce == cudaSuccess && nb)
+      ce = cudaMemcpyAsync(bandf.data(), bands, nb * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "band flags");
+    d2h += nb * sizeof(int);
+    size_t boff = 0;
+    for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
+      const pt_problem &p = ps[i];
+      if (p.channels == 0) continue;
+      const SysDesc &d0 = pl.sys[sys0[i]];
+      const size_t row = (size_t)p.width * p.channels, TH = (size_t)pl.tc.th, H = p.height;
+      const int *f = bandf.data() + boff;
+      for (int ty = 0; ty < d0.nty && ce == cudaSuccess;) {
+        int ty1 = ty + 1;
+        while (ty1 < d0.nty && f[ty1] == f[ty]) ++ty1;
+        if (f[ty]) {
+          const size_t r0 = ty * TH > 0 ? ty * TH - 1 : 0, r1 = std::min(H, ty1 * TH + 1);
+          const size_t off = r0 * row, bytes = (r1 - r0) * row * sizeof(float);
+          ce = cudaMemcpyAsync(const_cast<float *>(d0.src) + off, p.source_or_guidance + off, bytes,
+                               cudaMemcpyHostToDevice, st);
+          if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(const_cast<float *>(d0.tgt) + off, p.target_or_anchor + off, bytes,
+                                 cudaMemcpyHostToDevice, st);
+          if (ce == cudaSuccess && (p.flags & PT_FLAG_WARM_START))
+            ce = cudaMemcpyAsync(const_cast<float *>(d0.guess) + off, p.initial_guess + off, bytes,
+                                 cudaMemcpyHostToDevice, st);
+          h2d += bytes * ((p.flags & PT_FLAG_WARM_START) ? 3 : 2);
+        }
+        ty = ty1;
+      }
+      boff += (size_t)d0.nty;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "input upload");
+  }
+
   int grid = 0;
   ce = prepare_solve(P, pl.cfg, ctx->sms, &grid);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "solve prepare");
   ctx->last_grid = grid;
   ctx->last_cfg = pl.cfg;
   long long launches = 5;  // tile count, compaction, assembly, init, solve
-  for (uint32_t i = 0; i < n; ++i) launches += ps[i].channels > 0 ? 1 : 0;  // emits
+  for (uint32_t i = 0; i < n; ++i) launches += ps[i].channels > 0 ? (devptr ? 1 : 2) : 0;  // emits, band flags
+  if (!devptr) launches += 1;  // the first tile count
 
   // Everything from here to the results is stream work on the device: with
   // device pointers it is captured once into a CUDA graph and replayed while
@@ -381,13 +443,33 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   // ---- download
   std::vector<SysState> states(nsys);
   int kerr = 0;
+  d2h += nsys * sizeof(SysState) + sizeof(int);
   ce = cudaMemcpyAsync(states.data(), base + L.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&kerr, base + L.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  // host buffers: the bands with interior tiles come down after the emit;
+  // the other rows are the target (filled on the host below)
+  struct HostRows { float *out; const float *tgt; size_t off, n; };
+  std::vector<HostRows> host_rows;
   if (!devptr && ce == cudaSuccess) {
+    size_t boff = 0;
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
       if (ps[i].channels == 0) continue;
-      const size_t nf = (size_t)ps[i].width * ps[i].height * ps[i].channels;
-      ce = cudaMemcpyAsync(outs[i], pl.sys[sys0[i]].out, nf * sizeof(float), cudaMemcpyDeviceToHost, st);
+      const SysDesc &d0 = pl.sys[sys0[i]];
+      const size_t row = (size_t)ps[i].width * ps[i].channels, TH = (size_t)pl.tc.th, H = ps[i].height;
+      const int *f = bandf.data() + boff;
+      for (int ty = 0; ty < d0.nty && ce == cudaSuccess;) {
+        int ty1 = ty + 1;
+        while (ty1 < d0.nty && f[ty1] == f[ty]) ++ty1;
+        const size_t r0 = ty * TH, r1 = std::min(H, ty1 * TH), off = r0 * row, cnt = (r1 - r0) * row;
+        if (f[ty]) {
+          ce = cudaMemcpyAsync(outs[i] + off, d0.out + off, cnt * sizeof(float), cudaMemcpyDeviceToHost, st);
+          d2h += cnt * sizeof(float);
+        } else {
+          host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, off, cnt});
+        }
+        ty = ty1;
+      }
+      boff += (size_t)d0.nty;
     }
   }
   if (histories && !devptr && ce == cudaSuccess) {
@@ -397,6 +479,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
         const SysDesc &d = pl.sys[sys0[i] + c];
         const size_t cnt = ps[i].max_iterations;
         if (!cnt) continue;
+        d2h += cnt * sizeof(double);
         ce = cudaMemcpyAsync(histories[i] + (size_t)c * cnt,
                              reinterpret_cast<double *>(base + L.hist) + d.hist_off, cnt * sizeof(double),
                              cudaMemcpyDeviceToHost, st);
@@ -405,6 +488,8 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   }
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "result download");
   cudaEventRecord(ctx->ev[3], st);
+  // while the device works: the output rows that are the target
+  for (const HostRows &r : host_rows) std::memcpy(r.out + r.off, r.tgt + r.off, r.n * sizeof(float));
   ce = cudaStreamSynchronize(st);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "stream synchronize");
   {
@@ -415,6 +500,8 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     ctx->last_solve_ms = a;
     ctx->last_call_ms = b;
     ctx->last_launches = launches;
+    ctx->last_h2d = h2d;
+    ctx->last_d2h = d2h;
   }
   if (kerr != KERR_NONE)
     return fail(ctx, PT_TIMEOUT, kerr == KERR_DEADLINE ? "solve exceeded its wall budget"
@@ -542,6 +629,13 @@ pt_status pt_ctx_last_timing(const pt_ctx *ctx, double *solve_kernel_ms, double 
   if (solve_kernel_ms) *solve_kernel_ms = ctx->last_solve_ms;
   if (call_ms) *call_ms = ctx->last_call_ms;
   if (kernel_launches) *kernel_launches = ctx->last_launches;
+  return PT_OK;
+}
+
+pt_status pt_ctx_last_transfer(const pt_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes) {
+  if (!ctx) return PT_INVALID_ARG;
+  if (h2d_bytes) *h2d_bytes = ctx->last_h2d;
+  if (d2h_bytes) *d2h_bytes = ctx->last_d2h;
   return PT_OK;
 }
 

@@ -86,6 +86,7 @@ unsafe extern "C" {
     pub fn pt_ctx_stream(ctx: *const pt_ctx) -> *mut c_void;
     pub fn pt_ctx_last_timing(ctx: *const pt_ctx, solve_kernel_ms: *mut f64, call_ms: *mut f64,
         kernel_launches: *mut i64) -> pt_status;
+    pub fn pt_ctx_last_transfer(ctx: *const pt_ctx, h2d_bytes: *mut u64, d2h_bytes: *mut u64) -> pt_status;
     pub fn pt_tile_config_count() -> u32;
     pub fn pt_tile_config_info(idx: u32, sweeps_per_step: *mut i32, tile_w: *mut i32,
         tile_h: *mut i32) -> pt_status;

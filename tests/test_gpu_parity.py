@@ -8,6 +8,8 @@ Tolerances (stated here, measured against the FP64 CG oracle driven to 1e-12):
   * every non-interior pixel equals the target bit for bit;
   * reruns are byte-identical.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -452,3 +454,57 @@ def test_non_finite_inputs_follow_the_reference(ctx, oracle, case):
     assert worst["stop_reason"] == rworst.stop_reason and worst["converged"] == rworst.converged
     assert np.isnan(worst["final_residual"]) == np.isnan(rworst.final_residual)
     assert np.array_equal(~np.isfinite(out), ~np.isfinite(ref))
+
+
+def test_host_buffers_move_only_the_rows_the_solve_reads(ctx):
+    """A host-buffer solve uploads source and target only in the tile row bands
+    that hold interior cells (and one row either side), downloads only those
+    bands, and fills the other output rows with the target on the host. Its
+    output and reports equal the device-pointer solve's (which reads whole
+    images) bit for bit, even after an earlier call left other images in the
+    staging buffers; a NaN in the target far from the region comes out
+    unchanged; and the bytes moved are the rows that were needed."""
+    import torch
+    from paintop_b200 import _lib
+    w, h, c = 640, 600, 3
+    rng = np.random.default_rng(5)
+    src = rng.random(w * h * c).astype(np.float32)
+    tgt = rng.random(w * h * c).astype(np.float32)
+    mask = np.zeros((h, w), np.float32)
+    mask[250:330, 200:420] = 1.0
+    tgt3 = tgt.reshape(h, w, c)
+    tgt3[20, 30, 1] = np.nan  # far from the region: a target-only band
+    # fill the staging buffers with another image first
+    other = random_problem(9, w, h, c, density=0.8)
+    ctx.solve(*other, w, h, c, lam=0.01)
+    out_h, per_h, worst_h = ctx.solve(src, tgt, mask.reshape(-1), w, h, c, lam=0.01, tolerance=1e-8)
+    up, down = ctx.last_transfer()
+    dev = torch.device("cuda", 0)
+    ds = [torch.as_tensor(x, device=dev) for x in (src, tgt, mask.reshape(-1))]
+    out_d = torch.empty(w * h * c, device=dev)
+    hist_d = torch.zeros(c * 2000, dtype=torch.float64, device=dev)
+    reps = (_lib.PtReport * (c + 1))()
+    p = _lib.PtProblem(w, h, c, ds[0].data_ptr(), ds[1].data_ptr(), ds[2].data_ptr(), 0.01, 2000, 1e-8, 1.8,
+                       _lib.PT_FLAG_DEVICE_POINTERS, None)
+    torch.cuda.synchronize()
+    assert _lib.lib().pt_poisson_solve(ctx.h, C.byref(p), out_d.data_ptr(), reps, hist_d.data_ptr()) == 0
+    got = out_d.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), out_h.view(np.uint32))
+    hist = hist_d.cpu().numpy()
+    for k in range(c):
+        assert reps[k].iterations == per_h[k]["iterations"]
+        assert reps[k].final_residual == per_h[k]["final_residual"]
+        assert hist[k * 2000: k * 2000 + reps[k].iterations].tolist() == per_h[k]["residual_history"]
+    assert np.isnan(out_h.reshape(h, w, c)[20, 30, 1])
+    # bytes: the bands holding rows 250..329 (and one row either side) went up
+    # as source and target, plus the mask; only those bands came down
+    s_, tw_, th_ = C.c_int32(), C.c_int32(), C.c_int32()
+    _lib.lib().pt_tile_config_info(ctx.last_config(), C.byref(s_), C.byref(tw_), C.byref(th_))
+    th = th_.value
+    b0, b1 = 250 // th, 329 // th + 1
+    r0, r1 = max(0, b0 * th - 1), min(h, b1 * th + 1)
+    row = w * c * 4
+    assert up >= 2 * (r1 - r0) * row + w * h * 4 and up < 2 * (r1 - r0) * row + w * h * 4 + (1 << 20)
+    down_rows = (min(h, b1 * th) - b0 * th) * row
+    assert down >= down_rows and down < down_rows + (1 << 20)
+    assert up < 2 * w * h * c * 4
