@@ -26,9 +26,11 @@
 // channel) taken in chunks of up to 64 channels per pipeline stage: K groups
 // (g, g+1) of one tap are (R + 2) * HP entries apart. The CTA's weights stay resident in shared
 // memory. Roles: one warp's lane 0 issues TMA loads into a ring of stages
-// (full/empty mbarriers); one warp allocates TMEM and its lane 0 issues the
-// MMAs into one accumulator per epilogue warpgroup; two warpgroups take
-// alternate tiles through the epilogue (bias, ReLU, ReLU mask -> bf16).
+// (full/empty mbarriers); two issuer warps (lane 0 of each) issue the MMAs
+// into one buffer per epilogue warpgroup, issuer i taking the accumulators
+// of output rows i, i + 2, ... (the first also allocates TMEM); two
+// warpgroups take alternate tiles through the epilogue (bias, ReLU, ReLU
+// mask -> bf16).
 //
 // k_wgrad_tma<CP> (backward-weights, R = 1): D[co][tap][ci] += sum over the
 // segment's pixels of dY[p][co] X[p + off(tap)][ci]. GEMM rows = output
@@ -40,7 +42,9 @@
 // start entry. A CTA owns a fixed
 // range of segments, one part of the channels and one or all three dx values,
 // accumulates in TMEM and writes one fp32 partial per (tap, co, ci); the
-// partials are summed in chunk order by k_wgrad_reduce.
+// partials are summed in chunk order by k_wgrad_reduce. The CTAs of the
+// first channel part also sum dY over their segments for the bias gradient
+// (one partial per chunk and output channel, summed by the same reduce).
 //
 // Every wait is bounded in time; a CTA whose wait expires sets the error word,
 // stops issuing, drains its copies and MMAs (bounded), frees its TMEM and
@@ -100,9 +104,14 @@ struct ConvTmaGeom {
   int w_bytes;          // resident weight bytes of the CTA's part (rounded to 1024)
 };
 
-constexpr int kEpiGroups = 2;                            // epilogue warpgroups (one accumulator each)
-constexpr int kConvThreads = 32 * (4 * kEpiGroups + 2);  // + producer warp + MMA warp
-constexpr int kProdWarp = 4 * kEpiGroups, kMmaWarp = 4 * kEpiGroups + 1;
+constexpr int kEpiGroups = 2;  // epilogue warpgroups (one accumulator each)
+// MMA issuers: one thread issues a tcgen05.mma about every 156 cycles
+// whatever its shape, while the tensor core takes an M = 128, K = 16 MMA of
+// N <= 32 every ~37 cycles (its 4 KB A operand read from shared memory); with
+// two CTAs per SM, two issuing warps per CTA come within a few percent of that.
+constexpr int kIssuers = 2;
+constexpr int kConvThreads = 32 * (4 * kEpiGroups + 1 + kIssuers);  // + producer warp + issuers
+constexpr int kProdWarp = 4 * kEpiGroups, kMmaWarp = 4 * kEpiGroups + 1;  // first issuer
 
 constexpr int kChunkGroups = 8;  // channel groups (64 channels) per pipeline stage
 
@@ -112,7 +121,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint64_t full[kMaxStages], empty[kMaxStages], tfull[kEpiGroups], tempty[kEpiGroups], drain;
   __shared__ uint32_t tbase;
-  __shared__ int s_abort, s_issued, s_consumed;
+  __shared__ int s_abort, s_issued, s_consumed[kIssuers];
   __shared__ float sbias[N];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g8 = a.cin / 8;           // channel groups of the input
@@ -123,6 +132,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int gstride = (R + 2) * HP;      // entries between channel groups of a stage
   const int stage_bytes = GB * gstride * 16;
   const int n0 = blockIdx.y * N;      // the CTA's output channels
+  const int nis = min(kIssuers, R);   // issuers with rows: issuer i takes rows i, i + nis, ...
   const unsigned long long wait_ns = a.wait_ns ? a.wait_ns : kWaitNs;
   unsigned char *sW = sm;
   unsigned char *sA = sm + g.w_bytes;
@@ -134,16 +144,16 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   if (tid == 0) {
     for (int s = 0; s < nst; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&empty[s], nis);  // one commit per issuer
     }
     for (int k = 0; k < kEpiGroups; ++k) {
-      mbar_init(&tfull[k], 1);
+      mbar_init(&tfull[k], nis);
       mbar_init(&tempty[k], 4);
     }
-    mbar_init(&drain, 1);
+    mbar_init(&drain, nis);
     s_abort = 0;
     s_issued = 0;
-    s_consumed = 0;
+    for (int i = 0; i < kIssuers; ++i) s_consumed[i] = 0;
   }
   // resident weights of rows n0 .. n0+N-1, K-major core matrices: row n, K group kk = tap * g8 + j
   for (int idx = tid; idx < N * KK; idx += blockDim.x) {
@@ -182,9 +192,10 @@ __global__ void __launch_bounds__(kConvThreads, 2)
         }
       }
     }
-  } else if (warp == kMmaWarp) {
-    // ---------------- MMA issuer ----------------
-    if (lane == 0) {
+  } else if (warp >= kMmaWarp) {
+    // ---------------- MMA issuers: each owns the accumulators of its rows ----------------
+    const int issuer = warp - kMmaWarp;
+    if (lane == 0 && issuer < nis) {
       const uint32_t idesc = instr_desc_bf16(128, N, false, false);
       // descriptors advance by adding (bytes >> 4) to their address field
       const uint64_t bdesc0 = smem_desc(smem_u32(sW), (N / 8) * 128, 128);
@@ -194,7 +205,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       bool stop = false;
       // test knob (a.stall): wait first on a phase that nothing completes before
       // the drain below, so the wait runs out and the CTA takes the abort path
-      if (a.stall && !wait_phase(&drain, 0, wait_ns)) {
+      if (a.stall && issuer == 0 && !wait_phase(&drain, 0, wait_ns)) {
         atomicExch(&s_abort, 1);
         stop = true;
       }
@@ -215,7 +226,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
           const int gcn = min(kChunkGroups, g8 - c * kChunkGroups);
           const uint64_t adesc0 = smem_desc(smem_u32(sA + s * stage_bytes), gstride * 16, 128);
 #pragma unroll 1
-          for (int rr = 0; rr < R; ++rr) {
+          for (int rr = issuer; rr < R; rr += nis) {
             const uint32_t d = tm + acc * buf_cols + rr * acc_cols;
             uint32_t accumulate = c > 0 ? 1u : 0u;
             for (int tap = 0; tap < 9; ++tap) {
@@ -231,7 +242,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
             }
           }
           mma_commit(&empty[s]);
-          s_consumed = it + 1;
+          s_consumed[issuer] = it + 1;
         }
         if (stop) break;
         mma_commit(&tfull[acc]);
@@ -298,12 +309,17 @@ __global__ void __launch_bounds__(kConvThreads, 2)
 
   __syncthreads();
   if (s_abort && tid == 0) atomicExch(a.err, 1);
-  if (warp == kMmaWarp && lane == 0) {
-    // drain: loads issued but never consumed (only after an abort), then
-    // every MMA issued and the barrier arrivals they signal
-    for (int it = s_consumed; it < s_issued; ++it) wait_phase(&full[it % nst], (it / nst) & 1);
+  if (warp >= kMmaWarp && warp - kMmaWarp < nis && lane == 0) {
+    // drain: loads issued but not consumed by every issuer (only after an
+    // abort), then every MMA each issuer issued and the barrier arrivals
+    // they signal
+    if (warp == kMmaWarp) {
+      int lo = s_issued;
+      for (int i = 0; i < nis; ++i) lo = min(lo, s_consumed[i]);
+      for (int it = lo; it < s_issued; ++it) wait_phase(&full[it % nst], (it / nst) & 1);
+    }
     mma_commit(&drain);
-    wait_phase(&drain, 0);
+    if (warp == kMmaWarp) wait_phase(&drain, 0);
   }
   tc_fence_before_sync();
   __syncthreads();
@@ -328,14 +344,21 @@ struct WgradTmaGeom {
 // rows = the halo's 3 * CP / 8 (group, dy) groups (padded to 128 the same
 // way), columns = the output channels: the same MMA count with N = cout
 // instead of 3 * CP, a third of the tensor work when cout = 16 = CP.
+// Warps: 0-3 epilogue, 4 producer, 5.. MMA issuers. With T the three dx
+// accumulators are independent and each gets its own issuer (N = cout is
+// small, so one issuer would bound the tensor core); without T, N = 3 CP is
+// wide enough for one.
+constexpr int kWgIssuers = 3;
+constexpr int kWgThreads = 32 * (5 + kWgIssuers);
+
 template <int CP, bool T>
-__global__ void __launch_bounds__(192, 2)
+__global__ void __launch_bounds__(kWgThreads, 2)
     k_wgrad_tma(const __grid_constant__ CUtensorMap dymap, const __grid_constant__ CUtensorMap xmap, WgradArgs a,
                 WgradTmaGeom g) {
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint64_t full[kMaxStages], empty[kMaxStages], done, drain;
   __shared__ uint32_t tbase;
-  __shared__ int s_abort, s_issued, s_consumed;
+  __shared__ int s_abort, s_issued, s_consumed[kWgIssuers];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int G8 = CP / 8;          // channel groups of the part
   constexpr int NC = 3 * CP;          // GEMM columns per dx: (group, dy, channel)
@@ -351,18 +374,22 @@ __global__ void __launch_bounds__(192, 2)
   const int seg0 = blockIdx.x * g.seg_per_chunk;
   const int nitems = max(0, min(g.seg_per_chunk, g.s.nseg - seg0));
   const int HW = a.H * g.s.segs_x;  // R = 1: one tile per row and segment
+  const int nis = T ? min(kWgIssuers, g.ndx) : 1;  // issuer i takes dx t = i, i + nis, ...
+  // the first CTA of each segment chunk also sums dY for the bias gradient
+  // (warps 0-3, from the stages the MMAs read, while the MMAs run)
+  const bool colsum = a.db != nullptr && blockIdx.y == 0;
 
   if (warp == 5) tmem_alloc(&tbase, ncols);
   if (tid == 0) {
     for (int s = 0; s < nst; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&empty[s], nis + (colsum ? 4 : 0));  // one commit per issuer (+ the summing warps)
     }
-    mbar_init(&done, 1);
-    mbar_init(&drain, 1);
+    mbar_init(&done, nis);
+    mbar_init(&drain, nis);
     s_abort = 0;
     s_issued = 0;
-    s_consumed = 0;
+    for (int i = 0; i < kWgIssuers; ++i) s_consumed[i] = 0;
   }
   tc_fence_before_sync();
   __syncthreads();
@@ -386,8 +413,9 @@ __global__ void __launch_bounds__(192, 2)
         s_issued = it + 1;
       }
     }
-  } else if (warp == 5) {
-    if (lane == 0) {
+  } else if (warp >= 5) {
+    const int issuer = warp - 5;
+    if (lane == 0 && issuer < nis) {
       const uint32_t idesc = instr_desc_bf16(128, T ? a.cout : NC, true, true);
       for (int it = 0; it < nitems; ++it) {
         const int s = it % nst;
@@ -401,7 +429,7 @@ __global__ void __launch_bounds__(192, 2)
         // column groups at HP rows, pixel groups at 128 bytes. 16 pixels =
         // 256 bytes = 16 in the descriptors' address field.
         const uint64_t ydesc = smem_desc(a0, 128, SW * 16);
-        for (int t = 0; t < g.ndx; ++t) {
+        for (int t = issuer; t < g.ndx; t += nis) {
           const uint64_t xdesc = smem_desc(b0 + (uint32_t)((CW - 1 + dx0 + t) * 16), 128, rowb);
           const uint64_t adesc0 = T ? xdesc : ydesc, bdesc0 = T ? ydesc : xdesc;
           const uint32_t d = tm + t * dcols;
@@ -409,9 +437,66 @@ __global__ void __launch_bounds__(192, 2)
           for (int k = 1; k < SW / 16; ++k) mma_bf16(d, adesc0 + 16 * k, bdesc0 + 16 * k, idesc, 1u);
         }
         mma_commit(&empty[s]);
-        s_consumed = it + 1;
+        s_consumed[issuer] = it + 1;
       }
       if (!s_abort) mma_commit(&done);
+    }
+  } else if (colsum) {
+    // db partial of this chunk: warp w sums channel groups w, w + 4, ...;
+    // lane l pixels l, l + 32, ... of each segment, segments in order, then
+    // a fixed shuffle tree over the lanes. Stage layout: group g's SW pixels
+    // of 8 channels at (g * SW + p) * 16 bytes; pixels past W load as zero.
+    const int G = a.cout / 8;
+    float acc[4][8];
+#pragma unroll
+    for (int gi = 0; gi < 4; ++gi)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[gi][j] = 0.0f;
+    bool sum_ok = true;
+    for (int it = 0; it < nitems; ++it) {
+      const int s = it % nst;
+      int go = 0;
+      if (lane == 0) {
+        go = wait_phase(&full[s], (it / nst) & 1) && !*(volatile int *)&s_abort;
+        if (!go) atomicExch(&s_abort, 1);
+      }
+      if (!__shfl_sync(0xffffffffu, go, 0)) {
+        sum_ok = false;
+        break;
+      }
+      const unsigned char *st = sm + s * stage_bytes;
+#pragma unroll
+      for (int gi = 0; gi < 4; ++gi) {
+        const int grp = warp + 4 * gi;
+        if (grp < G)
+          for (int p = lane; p < SW; p += 32) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(st + ((size_t)grp * SW + p) * 16);
+            const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const float2 f = __bfloat1622float2(h[k]);
+              acc[gi][2 * k] += f.x;
+              acc[gi][2 * k + 1] += f.y;
+            }
+          }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (sum_ok) {
+#pragma unroll
+      for (int gi = 0; gi < 4; ++gi) {
+        const int grp = warp + 4 * gi;
+        if (grp < G) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            float v = acc[gi][j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) a.db_part[(long long)blockIdx.x * a.cout + grp * 8 + j] = v;
+          }
+        }
+      }
     }
   }
   __syncthreads();
@@ -467,10 +552,14 @@ __global__ void __launch_bounds__(192, 2)
     }
   }
   if (!ok && tid == 0) atomicExch(a.err, 1);
-  if (warp == 5 && lane == 0) {
-    for (int it = s_consumed; it < s_issued; ++it) wait_phase(&full[it % nst], (it / nst) & 1);
+  if (warp >= 5 && warp - 5 < nis && lane == 0) {
+    if (warp == 5) {
+      int lo = s_issued;
+      for (int i = 0; i < nis; ++i) lo = min(lo, s_consumed[i]);
+      for (int it = lo; it < s_issued; ++it) wait_phase(&full[it % nst], (it / nst) & 1);
+    }
     mma_commit(&drain);
-    wait_phase(&drain, 0);
+    if (warp == 5) wait_phase(&drain, 0);
   }
   tc_fence_before_sync();
   __syncthreads();
@@ -655,7 +744,7 @@ static cudaError_t launch_wgrad_tma_t(const WgradArgs &a, cudaStream_t st, int *
   if (pow2_cols(g.ndx * (T ? a.cout : 3 * CP)) >= 256 && smem < 80 * 1024) smem = 80 * 1024;
   cudaError_t e = cudaFuncSetAttribute(k_wgrad_tma<CP, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_wgrad_tma<CP, T><<<dim3(nchunks, gy), 192, smem, st>>>(dym, xm, a, g);
+  k_wgrad_tma<CP, T><<<dim3(nchunks, gy), kWgThreads, smem, st>>>(dym, xm, a, g);
   *chunks = nchunks;
   return cudaGetLastError();
 }
@@ -678,7 +767,7 @@ cudaError_t launch_wgrad(const WgradArgs &a, cudaStream_t st) {
     }
   }
   if (e != cudaSuccess) return e;
-  return launch_wgrad_reduce(a.part, chunks, a.cout, a.cin, a.dw, st);
+  return launch_wgrad_reduce(a.part, chunks, a.cout, a.cin, a.dw, a.db ? a.db_part : nullptr, a.db, st);
 }
 
 }  // namespace unet

@@ -122,15 +122,16 @@ pt_status ensure_acts(pt_unet *n, int B, int H, int W) {
   auto al = [](size_t v) { return (v + 255) / 256 * 256; };
   for (auto &it : items) total += al((size_t)P0 / (1ull << (2 * it.level)) * it.c * 2);
   // fp32/double scratch
-  size_t maxch = 0;
+  size_t maxch = 0, maxdb = 0;
   for (int l = 0; l < 14; ++l) {
     const int lev = (l <= 1 || l >= 12) ? 0 : (l <= 3 || l >= 10) ? 1 : (l <= 5 || l >= 8) ? 2 : 3;
     const int ch = wgrad_chunks(B, H >> lev, W >> lev);
     const size_t need = (size_t)ch * 9 * kLayers[l].cout * kLayers[l].cin;
     if (need > maxch) maxch = need;
+    if ((size_t)ch * kLayers[l].cout > maxdb) maxdb = (size_t)ch * kLayers[l].cout;
   }
   const size_t f_pred = al(P0 * 4), f_dpred = al(P0 * 4), f_w = al((size_t)maxch * 4),
-               f_c = al((size_t)std::max(colsum_parts(P0), head_bwd_blocks(P0)) * 129 * 4), f_cnt = al(1025 * 4),
+               f_c = al(std::max(maxdb, (size_t)head_bwd_blocks(P0) * (kHeadIn + 1)) * 4), f_cnt = al(1025 * 4),
                f_l = al(1024 * 8), f_err = 256;
   total += f_pred + f_dpred + f_w + f_c + f_cnt + f_l + f_err;
   if (n->act_mem) { cudaFree(n->act_mem); n->act_mem = nullptr; }
@@ -196,16 +197,16 @@ pt_status dgrad(pt_unet *n, int l, const Act &dy, const Act &dx, int dx_off, con
   return PT_OK;
 }
 
-// dW (into grad) from dY (pre-activation) and the forward input x; db = colsum(dY)
+// dW and db (into grad) from dY (pre-activation) and the forward input x;
+// db[co] = sum over pixels of dY[p][co], summed by the same kernel
 pt_status wgrad(pt_unet *n, int l, const Act &dy, const Act &x, int x_off) {
   WgradArgs a{};
   a.dy = view(dy); a.cout = kLayers[l].cout;
   a.x = view(x, x_off); a.cin = kLayers[l].cin;
   a.B = n->B; a.H = n->H >> dy.level; a.W = n->W >> dy.level;
   a.part = n->wpart; a.dw = n->grad + n->w_off[l]; a.err = n->err;
+  a.db_part = n->cpart; a.db = n->grad + n->b_off[l];
   CK(launch_wgrad(a, n->ctx->stream), "conv backward-weights");
-  CK(launch_colsum(view(dy), kLayers[l].cout / 8, a.B, a.H, a.W, n->cpart, n->grad + n->b_off[l], n->ctx->stream),
-     "bias gradient");
   return PT_OK;
 }
 

@@ -162,36 +162,6 @@ __global__ void k_upsample2_bwd(ActView dout, ActView act, ActView din, int B, i
   }
 }
 
-// db[c] = sum_p dY[p][c]: block k sums pixels [k * chunk, (k + 1) * chunk)
-// (p = b * H * W + y * W + x) with blockDim / groups pixel lanes per 8-channel
-// group, lanes combined in lane order; k_colsum_reduce then sums the block
-// partials in block order.
-__global__ void k_colsum(ActView dy, int groups, int B, int H, int W, int chunk, float *part) {
-  __shared__ float sh[256][8];
-  const long long HW = (long long)H * W, P = (long long)B * HW;
-  const int lanes = blockDim.x / groups;
-  const int g = threadIdx.x % groups, ln = threadIdx.x / groups;
-  const long long p0 = (long long)blockIdx.x * chunk;
-  const long long p1 = min(p0 + chunk, P);
-  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0}, v[8];
-  if (ln < lanes)
-    for (long long p = p0 + ln; p < p1; p += lanes) {
-      const int b = (int)(p / HW);
-      const long long yx = p - b * HW;
-      ld8(dy.p + (((long long)b * dy.cg + dy.g0 + g) * HW + yx) * 8, v);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) acc[j] += v[j];
-    }
-#pragma unroll
-  for (int j = 0; j < 8; ++j) sh[threadIdx.x][j] = acc[j];
-  __syncthreads();
-  const int c = threadIdx.x;
-  if (c < groups * 8) {
-    float t = 0.0f;
-    for (int l = 0; l < lanes; ++l) t += sh[l * groups + c / 8][c % 8];
-    part[(long long)blockIdx.x * groups * 8 + c] = t;
-  }
-}
 // out[j] = sum_k part[k][j] in a fixed order: one warp per column, lane l sums
 // k = l, l + 32, ..., then a fixed shuffle tree.
 __global__ void k_colsum_reduce(const float *part, int nparts, int c, float *out) {
@@ -462,25 +432,53 @@ __global__ void k_compose_guess(const float *g, const float *corr, int W, int H,
 // launchers
 // ----------------------------------------------------------------------------
 // (the weight gradient's final sum, launched by launch_wgrad_reduce)
-// Sum the per-chunk partials in chunk order: dW[co][tap][ci] (fp32).
-// One warp per weight: lane l sums chunks l, l + 32, ... and a fixed shuffle
-// tree combines the lanes.
-__global__ void k_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw) {
-  const int total = cout * 9 * cin, lane = threadIdx.x & 31;
-  const int nwarps = gridDim.x * blockDim.x / 32;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += nwarps) {
-    const int co = i / (9 * cin), r = i - co * 9 * cin, tap = r / cin, ci = r - tap * cin;
-    float s = 0.0f;
-    for (int k = lane; k < nchunks; k += 32) s += part[(((long long)k * 9 + tap) * cout + co) * cin + ci];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) dw[i] = s;
+// Sum the per-chunk partials in chunk order: dW[co][tap][ci] (fp32), then,
+// with db, db[co] from its [chunks][cout] partials. One thread per output,
+// consecutive threads on consecutive partials of a chunk (coalesced): the
+// thread keeps 32 running sums, sum l over chunks l, l + 32, ... in chunk
+// order, and combines them by the fixed tree s[l] += s[l + o], o = 16, 8, 4,
+// 2, 1.
+__global__ void k_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, const float *db_part,
+                               float *db) {
+  const long long wtotal = (long long)cout * 9 * cin;
+  const long long total = wtotal + (db ? cout : 0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float *src;
+    long long stride;
+    if (i < wtotal) {
+      const int co = (int)(i / (9 * cin)), r = (int)(i - (long long)co * 9 * cin), tap = r / cin, ci = r - tap * cin;
+      src = part + ((long long)tap * cout + co) * cin + ci;
+      stride = wtotal;
+    } else {
+      src = db_part + (i - wtotal);
+      stride = cout;
+    }
+    float s[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) s[l] = 0.0f;
+    for (int k0 = 0; k0 < nchunks; k0 += 32) {
+#pragma unroll
+      for (int l = 0; l < 32; ++l)
+        if (k0 + l < nchunks) s[l] += src[(long long)(k0 + l) * stride];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int l = 0; l < o; ++l) s[l] += s[l + o];
+    if (i < wtotal)
+      dw[i] = s[0];
+    else
+      db[i - wtotal] = s[0];
   }
 }
 
-cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st) {
-  long long blocks = ((long long)cout * 9 * cin * 32 + 255) / 256;
+cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, const float *db_part,
+                                float *db, cudaStream_t st) {
+  const long long total = (long long)cout * 9 * cin + (db ? cout : 0);
+  long long blocks = (total + 127) / 128;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  k_wgrad_reduce<<<(unsigned)blocks, 256, 0, st>>>(part, nchunks, cout, cin, dw);
+  k_wgrad_reduce<<<(unsigned)blocks, 128, 0, st>>>(part, nchunks, cout, cin, dw, db_part, db);
   return cudaGetLastError();
 }
 
@@ -492,18 +490,6 @@ static unsigned blocks_for(long long n, int threads) {
 
 cudaError_t launch_reduce_rows(const float *part, int nparts, int c, float *out, cudaStream_t st) {
   k_colsum_reduce<<<c, 32, 0, st>>>(part, nparts, c, out);
-  return cudaGetLastError();
-}
-
-constexpr int kColsumChunk = 1024;  // pixels per bias-gradient block
-int colsum_parts(long long P) { return (int)((P + kColsumChunk - 1) / kColsumChunk); }
-cudaError_t launch_colsum(const ActView &dy, int groups, int B, int H, int W, float *part, float *out,
-                          cudaStream_t st) {
-  if (groups < 1 || groups > 32 || 256 % groups != 0) return cudaErrorInvalidValue;
-  const long long P = (long long)B * H * W;
-  const int nparts = colsum_parts(P);
-  k_colsum<<<nparts, 256, 0, st>>>(dy, groups, B, H, W, kColsumChunk, part);
-  k_colsum_reduce<<<groups * 8, 32, 0, st>>>(part, nparts, groups * 8, out);
   return cudaGetLastError();
 }
 

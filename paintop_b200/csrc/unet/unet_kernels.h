@@ -50,6 +50,8 @@ struct WgradArgs {
   int B, H, W;
   float *part;              // [chunks][9][cout][cin] partials
   float *dw;                // [cout][9][cin] result
+  float *db_part;           // [chunks][cout] bias-gradient partials (with db)
+  float *db;                // [cout] bias gradient sum_p dY[p][co], or nullptr
   int *err;
 };
 
@@ -61,10 +63,8 @@ cudaError_t launch_wgrad(const WgradArgs &a, cudaStream_t st);
 // unet_kernels.cu
 // out[j] = sum over k = 0 .. nparts-1 (in order) of part[k][j], j < c
 cudaError_t launch_reduce_rows(const float *part, int nparts, int c, float *out, cudaStream_t st);
-cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, cudaStream_t st);
-int colsum_parts(long long P);
-cudaError_t launch_colsum(const ActView &dy, int groups, int B, int H, int W, float *part, float *out,
-                          cudaStream_t st);
+cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, const float *db_part,
+                                float *db, cudaStream_t st);
 cudaError_t launch_avgpool2(const ActView &in, const ActView &out, int B, int H, int W, int groups,
                             cudaStream_t st);
 cudaError_t launch_unpool_add_mask(const ActView &dskip, const ActView &dpool, const ActView &act,
