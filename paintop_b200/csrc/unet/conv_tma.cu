@@ -23,14 +23,15 @@
 // k_conv_tma<N> (forward / backward-data): per output row, GEMM rows = the
 // segment's pixels (M = 128; rows past SW are never stored), columns = N
 // output channels (the CTA's part [n0, n0 + N) of them: blockIdx.y), K = (tap,
-// channel) taken in chunks of up to 64 channels per pipeline stage: K groups
-// (g, g+1) of one tap are (R + 2) * HP entries apart. The CTA's weights stay resident in shared
-// memory. Roles: one warp's lane 0 issues TMA loads into a ring of stages
-// (full/empty mbarriers); two issuer warps (lane 0 of each) issue the MMAs
-// into one buffer per epilogue warpgroup, issuer i taking the accumulators
-// of output rows i, i + 2, ... (the first also allocates TMEM); two
-// warpgroups take alternate tiles through the epilogue (bias, ReLU, ReLU
-// mask -> bf16).
+// channel) taken in chunks of cg channel groups (chosen per layer, at most
+// 64 channels) per pipeline stage: K groups (g, g+1) of one tap are (R + 2) *
+// HP entries apart. The CTA's weights stay resident in shared memory. Roles:
+// one warp's lane 0 issues TMA loads into a ring of stages (full/empty
+// mbarriers); up to four issuer warps (lane 0 of each) issue the MMAs into
+// one buffer per epilogue warpgroup, issuer i taking the accumulators of
+// output rows i, i + nis, ... (nis = min(4, R); the first issuer also
+// allocates TMEM); two warpgroups take alternate tiles through the epilogue
+// (bias, ReLU, ReLU mask -> bf16).
 //
 // k_wgrad_tma<CP> (backward-weights, R = 1): D[co][tap][ci] += sum over the
 // segment's pixels of dY[p][co] X[p + off(tap)][ci]. GEMM rows = output
@@ -42,7 +43,9 @@
 // start entry. A CTA owns a fixed
 // range of segments, one part of the channels and one or all three dx values,
 // accumulates in TMEM and writes one fp32 partial per (tap, co, ci); the
-// partials are summed in chunk order by k_wgrad_reduce. The CTAs of the
+// partials are summed in chunk order by k_wgrad_reduce. The transposed form
+// (cout <= 32) issues the three dx accumulators from three warps and, with 16
+// channels per part (48 GEMM rows), uses M = 64 MMAs. The CTAs of the
 // first channel part also sum dY over their segments for the bias gradient
 // (one partial per chunk and output channel, summed by the same reduce).
 //
@@ -73,8 +76,12 @@ __device__ __forceinline__ unsigned long long now_ns() {
   return t;
 }
 // Bounded wait on an mbarrier phase (wall-clock limit, kWaitNs by default).
+// The clock is read only once a first round of polls has missed: most waits
+// in the pipelines find their phase complete, and a global-timer read costs
+// far more than a poll.
 __device__ __forceinline__ bool wait_phase(uint64_t *mbar, uint32_t parity,
                                            unsigned long long limit_ns = kWaitNs) {
+  if (mbar_wait(mbar, parity, 8)) return true;
   const unsigned long long t0 = now_ns();
   while (true) {
     if (mbar_wait(mbar, parity, 64)) return true;
@@ -102,18 +109,20 @@ struct SegGeom {
 struct ConvTmaGeom {
   SegGeom s;
   int w_bytes;          // resident weight bytes of the CTA's part (rounded to 1024)
+  int cg;               // channel groups per K chunk (pipeline stage): even, <= kMaxChunkGroups
 };
 
 constexpr int kEpiGroups = 2;  // epilogue warpgroups (one accumulator each)
 // MMA issuers: one thread issues a tcgen05.mma about every 156 cycles
 // whatever its shape, while the tensor core takes an M = 128, K = 16 MMA of
-// N <= 32 every ~37 cycles (its 4 KB A operand read from shared memory); with
-// two CTAs per SM, two issuing warps per CTA come within a few percent of that.
-constexpr int kIssuers = 2;
+// N <= 32 every ~37 cycles (its 4 KB A operand read from shared memory); one
+// issuer per output row of a tile (up to four per CTA) keeps the small-N
+// layers on the tensor core's bound instead of the issue rate.
+constexpr int kIssuers = 4;
 constexpr int kConvThreads = 32 * (4 * kEpiGroups + 1 + kIssuers);  // + producer warp + issuers
 constexpr int kProdWarp = 4 * kEpiGroups, kMmaWarp = 4 * kEpiGroups + 1;  // first issuer
 
-constexpr int kChunkGroups = 8;  // channel groups (64 channels) per pipeline stage
+constexpr int kMaxChunkGroups = 8;  // channel groups (64 channels) per pipeline stage, at most
 
 template <int N>
 __global__ void __launch_bounds__(kConvThreads, 2)
@@ -126,9 +135,10 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g8 = a.cin / 8;           // channel groups of the input
   const int KK = 9 * g8;              // 8-element K groups of the weights
-  const int nkc = (g8 + kChunkGroups - 1) / kChunkGroups;  // K chunks per tile
+  const int CG = g.cg;                 // channel groups per K chunk
+  const int nkc = (g8 + CG - 1) / CG;  // K chunks per tile
   const int SW = g.s.SW, HP = g.s.HP, CW = g.s.CW, R = g.s.R, nst = g.s.nst, ntiles = g.s.nseg;
-  const int GB = min(g8, kChunkGroups);  // planes per chunk box
+  const int GB = min(g8, CG);            // planes per chunk box
   const int gstride = (R + 2) * HP;      // entries between channel groups of a stage
   const int stage_bytes = GB * gstride * 16;
   const int n0 = blockIdx.y * N;      // the CTA's output channels
@@ -186,7 +196,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
           }
           // the box is GB planes; planes past the buffer read as zero
           mbar_arrive_expect_tx(&full[s], (uint32_t)stage_bytes);
-          tma_load_5d(sA + s * stage_bytes, &xmap, 0, x0 / CW - 1, rg * R - 1, a.x.g0 + c * kChunkGroups, b,
+          tma_load_5d(sA + s * stage_bytes, &xmap, 0, x0 / CW - 1, rg * R - 1, a.x.g0 + c * CG, b,
                       &full[s]);
           s_issued = it + 1;
         }
@@ -223,7 +233,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
             break;
           }
           tc_fence_after_sync();
-          const int gcn = min(kChunkGroups, g8 - c * kChunkGroups);
+          const int gcn = min(CG, g8 - c * CG);
           const uint64_t adesc0 = smem_desc(smem_u32(sA + s * stage_bytes), gstride * 16, 128);
 #pragma unroll 1
           for (int rr = issuer; rr < R; rr += nis) {
@@ -232,7 +242,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
             for (int tap = 0; tap < 9; ++tap) {
               // entries of 16 bytes
               uint64_t ad = adesc0 + (uint32_t)((rr + tap / 3) * HP + CW - 1 + (tap % 3));
-              uint64_t bd = bdesc0 + (uint32_t)(tap * g8 + c * kChunkGroups) * bgrp;
+              uint64_t bd = bdesc0 + (uint32_t)(tap * g8 + c * CG) * bgrp;
               for (int j = 0; j < gcn; j += 2) {
                 mma_bf16(d, ad, bd, idesc, accumulate);
                 accumulate = 1;
@@ -362,6 +372,9 @@ __global__ void __launch_bounds__(kWgThreads, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int G8 = CP / 8;          // channel groups of the part
   constexpr int NC = 3 * CP;          // GEMM columns per dx: (group, dy, channel)
+  // GEMM rows: with T and 3 CP <= 64 an M = 64 MMA (half the A operand read
+  // per MMA); its accumulator row m sits in TMEM lane (m % 16) + 32 (m / 16)
+  constexpr int kMT = (T && 3 * CP <= 64) ? 64 : 128;
   const int SW = g.s.SW, HP = g.s.HP, CW = g.s.CW, nst = g.s.nst;
   const int rowb = HP * 16;
   const int ga = a.cout / 8;
@@ -416,7 +429,7 @@ __global__ void __launch_bounds__(kWgThreads, 2)
   } else if (warp >= 5) {
     const int issuer = warp - 5;
     if (lane == 0 && issuer < nis) {
-      const uint32_t idesc = instr_desc_bf16(128, T ? a.cout : NC, true, true);
+      const uint32_t idesc = instr_desc_bf16(kMT, T ? a.cout : NC, true, true);
       for (int it = 0; it < nitems; ++it) {
         const int s = it % nst;
         if (!wait_phase(&full[s], (it / nst) & 1) || *(volatile int *)&s_abort) {
@@ -510,8 +523,12 @@ __global__ void __launch_bounds__(kWgThreads, 2)
   ok = !s_abort;
   if (ok && warp < 4 && T) {
     tc_fence_after_sync();
-    // lane m = GEMM row: halo group k = m / 8 = 3 * group + (dy + 1), channel m % 8
-    const int m = 32 * warp + lane, k = m >> 3, grp = k / 3, dyi = k - 3 * grp;
+    // GEMM row m: halo group k = m / 8 = 3 * group + (dy + 1), channel m % 8;
+    // warp w reads TMEM lanes 32 w .. 32 w + 31, which hold rows 32 w + lane
+    // (M = 128) or, for lanes below 16, rows 16 w + lane (M = 64)
+    const int m = kMT == 64 ? 16 * warp + lane : 32 * warp + lane;
+    const bool row_here = kMT == 128 || lane < 16;
+    const int k = m >> 3, grp = k / 3, dyi = k - 3 * grp;
     const int ci = c0 + 8 * grp + (m & 7);
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
     for (int t = 0; t < g.ndx; ++t) {
@@ -520,7 +537,7 @@ __global__ void __launch_bounds__(kWgThreads, 2)
       for (int c16 = 0; c16 < a.cout / 16; ++c16) {
         uint32_t rr[16];
         tmem_ld16(tm + lane_base + t * dcols + c16 * 16, rr);
-        if (m < 3 * CP) {
+        if (row_here && m < 3 * CP) {
 #pragma unroll
           for (int j = 0; j < 16; ++j)
             a.part[(((long long)blockIdx.x * 9 + tap) * a.cout + c16 * 16 + j) * a.cin + ci] =
@@ -641,7 +658,7 @@ static SegGeom seg_geom(int B, int H, int W, int R) {
 // larger MMAs and fewer reloads of the input halo.
 static int conv_part(int n, int cin, int W) {
   const int HP = seg_geom(1, 1, W, 1).HP;
-  const int stage1 = std::min(cin / 8, kChunkGroups) * 3 * HP * 16;
+  const int stage1 = std::min(cin / 8, kMaxChunkGroups) * 3 * HP * 16;
   for (int p = n; p >= 16; p -= 16) {
     const int w_bytes = (p * 9 * cin * 2 + 1023) / 1024 * 1024;
     if (n % p == 0 && p <= 96 && p * 9 * cin * 2 <= 110 * 1024 && w_bytes + 2 * stage1 + kTail <= kSmemCap)
@@ -654,24 +671,44 @@ template <int NP>
 static cudaError_t launch_conv_tma_t(const ConvArgs &a, int parts, cudaStream_t st) {
   ConvTmaGeom g{};
   g.w_bytes = (NP * 9 * a.cin * 2 + 1023) / 1024 * 1024;
-  const int GB = std::min(a.cin / 8, kChunkGroups);
-  // rows per tile: as many as the TMEM (two buffers of R accumulators within
-  // 256 columns) and three stages of shared memory allow
-  int R = 256 / (2 * (int)pow2_cols(NP));
-  if (R > 4) R = 4;
-  while (R > 1 && g.w_bytes + 3 * GB * (R + 2) * seg_geom(a.B, a.H, a.W, R).HP * 16 + kTail > kSmemCap) R >>= 1;
+  const int g8 = a.cin / 8;
+  // Geometry: CTAs per SM (2 or 1), rows per tile R (TMEM: two buffers of R
+  // accumulators within the CTA's share, 256 columns with two CTAs per SM
+  // and 512 with one; at most 4) and channel groups per K chunk, with at
+  // least 3 stages in the ring. Preferred: the most MMA issuers per SM (CTAs
+  // x min(issuers, R)), then the larger R (fewer halo rows re-read), then the
+  // larger chunk (fewer barrier round trips).
+  int best_score = -1, per_sm = 1;
+  for (int ps = 2; ps >= 1; --ps) {
+    int rmax = (ps == 2 ? 256 : 512) / (2 * (int)pow2_cols(NP));
+    if (rmax > 4) rmax = 4;
+    const int budget = (ps == 2 ? kHalfSm : kSmemCap) - kTail - g.w_bytes;
+    for (int R = rmax; R >= 1; R >>= 1) {
+      const int HP = seg_geom(a.B, a.H, a.W, R).HP;
+      for (int cg = std::min(g8, kMaxChunkGroups); cg >= 2; cg -= 2) {
+        if (g8 % cg != 0 && cg != std::min(g8, kMaxChunkGroups)) continue;  // whole chunks, or the widest
+        const int stage = cg * (R + 2) * HP * 16;
+        if (budget / stage < 3) continue;
+        const int score = (ps * std::min(kIssuers, R)) * 1000 + R * 100 + cg;
+        if (score > best_score) best_score = score, per_sm = ps, g.s.R = R, g.cg = cg;
+        break;  // the widest chunk that fits at this R
+      }
+    }
+  }
+  if (best_score < 0) return cudaErrorInvalidValue;
+  const int R = g.s.R, GB = g.cg;
   g.s = seg_geom(a.B, a.H, a.W, R);
   CUtensorMap xm;
   if (!act_map(&xm, a.x, a.B, a.H, a.W, g.s.CW, g.s.HP / g.s.CW, R + 2, GB)) return cudaErrorInvalidValue;
   const int stage = GB * (R + 2) * g.s.HP * 16;
-  // two CTAs per SM when that leaves at least 3 stages each, else one CTA
-  // with the deepest ring that fits
-  int per_sm = 2, budget = kHalfSm - kTail;
-  if ((budget - g.w_bytes) / stage < 3) per_sm = 1, budget = kSmemCap - kTail;
+  const int budget = per_sm == 2 ? kHalfSm - kTail : kSmemCap - kTail;
   g.s.nst = (budget - g.w_bytes) / stage;
   if (g.s.nst > kMaxStages) g.s.nst = kMaxStages;
   if (g.s.nst < 2) return cudaErrorInvalidValue;
-  const int smem = g.w_bytes + g.s.nst * stage + kTail;
+  int smem = g.w_bytes + g.s.nst * stage + kTail;
+  // one CTA per SM: take enough shared memory that a second cannot share the
+  // SM (and its TMEM)
+  if (per_sm == 1 && smem < kHalfSm + 8 * 1024) smem = kHalfSm + 8 * 1024;
   cudaError_t e = cudaFuncSetAttribute(k_conv_tma<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   int gx = per_sm * num_sms() / parts;

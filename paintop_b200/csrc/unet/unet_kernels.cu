@@ -10,6 +10,7 @@
 // deterministic.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "unet_kernels.h"
@@ -71,21 +72,39 @@ __global__ void k_avgpool2(ActView in, ActView out, int B, int H, int W, int gro
   }
 }
 
+// Row-oriented elementwise kernels: threadIdx.y picks a row r = (b * groups +
+// g) * H + y of one 8-channel plane (a grid-stride loop over rows),
+// threadIdx.x the pixels x of the row; the row's plane and source rows are
+// resolved once per row, and consecutive threads touch consecutive 16-byte
+// pixels.
+__device__ __forceinline__ void row_of(int r, int groups, int H, int &b, int &g, int &y) {
+  y = r % H;
+  const int bg = r / H;
+  g = bg % groups;
+  b = bg / groups;
+}
+
 // de = (dskip + unpool(dpool)) * (act > 0): the total gradient of a skip
 // activation that feeds both the pooling and the decoder concatenation.
 __global__ void k_unpool_add_mask(ActView dskip, ActView dpool, ActView act, ActView out, int B, int H, int W,
                                   int groups) {
-  const long long total = (long long)B * groups * H * W;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const Pix q = pix_of(i, groups, H, W);
-    float ds[8], dp[8], av[8], o[8];
-    ld8(dskip.p + act_index(dskip, q.b, q.g, q.y, q.x, H, W), ds);
-    ld8(dpool.p + act_index(dpool, q.b, q.g, q.y / 2, q.x / 2, H / 2, W / 2), dp);
-    ld8(act.p + act_index(act, q.b, q.g, q.y, q.x, H, W), av);
+  const int rows = B * groups * H;
+  for (int r = blockIdx.x * blockDim.y + threadIdx.y; r < rows; r += gridDim.x * blockDim.y) {
+    int b, g, y;
+    row_of(r, groups, H, b, g, y);
+    const __nv_bfloat16 *ds_row = dskip.p + act_index(dskip, b, g, y, 0, H, W);
+    const __nv_bfloat16 *dp_row = dpool.p + act_index(dpool, b, g, y / 2, 0, H / 2, W / 2);
+    const __nv_bfloat16 *av_row = act.p + act_index(act, b, g, y, 0, H, W);
+    __nv_bfloat16 *o_row = out.p + act_index(out, b, g, y, 0, H, W);
+    for (int x = threadIdx.x; x < W; x += blockDim.x) {
+      float ds[8], dp[8], av[8], o[8];
+      ld8(ds_row + (long long)x * 8, ds);
+      ld8(dp_row + (long long)(x / 2) * 8, dp);
+      ld8(av_row + (long long)x * 8, av);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) o[j] = av[j] > 0.0f ? ds[j] + 0.25f * dp[j] : 0.0f;
-    st8(out.p + act_index(out, q.b, q.g, q.y, q.x, H, W), o);
+      for (int j = 0; j < 8; ++j) o[j] = av[j] > 0.0f ? ds[j] + 0.25f * dp[j] : 0.0f;
+      st8(o_row + (long long)x * 8, o);
+    }
   }
 }
 
@@ -100,65 +119,81 @@ __device__ __forceinline__ void up_taps(int o, int n, int &i0, int &i1, float &w
 }
 __global__ void k_upsample2(ActView in, ActView out, int B, int Hi, int Wi, int groups) {
   const int Ho = 2 * Hi, Wo = 2 * Wi;
-  const long long total = (long long)B * groups * Ho * Wo;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const Pix q = pix_of(i, groups, Ho, Wo);
-    int y0, y1, x0, x1;
-    float wy0, wy1, wx0, wx1;
-    up_taps(q.y, Hi, y0, y1, wy0, wy1);
-    up_taps(q.x, Wi, x0, x1, wx0, wx1);
-    float a00[8], a01[8], a10[8], a11[8], o[8];
-    ld8(in.p + act_index(in, q.b, q.g, y0, x0, Hi, Wi), a00);
-    ld8(in.p + act_index(in, q.b, q.g, y0, x1, Hi, Wi), a01);
-    ld8(in.p + act_index(in, q.b, q.g, y1, x0, Hi, Wi), a10);
-    ld8(in.p + act_index(in, q.b, q.g, y1, x1, Hi, Wi), a11);
+  const int rows = B * groups * Ho;
+  for (int r = blockIdx.x * blockDim.y + threadIdx.y; r < rows; r += gridDim.x * blockDim.y) {
+    int b, g, y;
+    row_of(r, groups, Ho, b, g, y);
+    int y0, y1;
+    float wy0, wy1;
+    up_taps(y, Hi, y0, y1, wy0, wy1);
+    const __nv_bfloat16 *r0 = in.p + act_index(in, b, g, y0, 0, Hi, Wi);
+    const __nv_bfloat16 *r1 = in.p + act_index(in, b, g, y1, 0, Hi, Wi);
+    __nv_bfloat16 *o_row = out.p + act_index(out, b, g, y, 0, Ho, Wo);
+    for (int x = threadIdx.x; x < Wo; x += blockDim.x) {
+      int x0, x1;
+      float wx0, wx1;
+      up_taps(x, Wi, x0, x1, wx0, wx1);
+      float a00[8], a01[8], a10[8], a11[8], o[8];
+      ld8(r0 + (long long)x0 * 8, a00);
+      ld8(r0 + (long long)x1 * 8, a01);
+      ld8(r1 + (long long)x0 * 8, a10);
+      ld8(r1 + (long long)x1 * 8, a11);
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-      o[j] = wy0 * (wx0 * a00[j] + wx1 * a01[j]) + wy1 * (wx0 * a10[j] + wx1 * a11[j]);
-    st8(out.p + act_index(out, q.b, q.g, q.y, q.x, Ho, Wo), o);
+      for (int j = 0; j < 8; ++j)
+        o[j] = wy0 * (wx0 * a00[j] + wx1 * a01[j]) + wy1 * (wx0 * a10[j] + wx1 * a11[j]);
+      st8(o_row + (long long)x * 8, o);
+    }
   }
 }
 // Adjoint of k_upsample2 (a gather over the outputs that read each input),
 // times the ReLU mask of the upsampled activation.
 __global__ void k_upsample2_bwd(ActView dout, ActView act, ActView din, int B, int Hi, int Wi, int groups) {
   const int Ho = 2 * Hi, Wo = 2 * Wi;
-  const long long total = (long long)B * groups * Hi * Wi;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const Pix q = pix_of(i, groups, Hi, Wi);
+  const int rows = B * groups * Hi;
+  for (int r = blockIdx.x * blockDim.y + threadIdx.y; r < rows; r += gridDim.x * blockDim.y) {
+    int b, g, y;
+    row_of(r, groups, Hi, b, g, y);
     // output rows that read input row y: 2y, 2y+1 (weight 0.75), 2y-1 and 2y+2
     // (weight 0.25), plus the clamped border rows
-    float wyv[4], wxv[4];
-    int oy[4], ox[4];
-    int ny = 0, nx = 0;
-    for (int o = max(2 * q.y - 1, 0); o <= min(2 * q.y + 2, Ho - 1); ++o) {
+    float wyv[4];
+    int oy[4];
+    int ny = 0;
+    for (int o = max(2 * y - 1, 0); o <= min(2 * y + 2, Ho - 1); ++o) {
       int i0, i1;
       float w0, w1;
       up_taps(o, Hi, i0, i1, w0, w1);
-      const float wgt = (i0 == q.y ? w0 : 0.0f) + (i1 == q.y ? w1 : 0.0f);
+      const float wgt = (i0 == y ? w0 : 0.0f) + (i1 == y ? w1 : 0.0f);
       if (wgt != 0.0f) { oy[ny] = o; wyv[ny] = wgt; ++ny; }
     }
-    for (int o = max(2 * q.x - 1, 0); o <= min(2 * q.x + 2, Wo - 1); ++o) {
-      int i0, i1;
-      float w0, w1;
-      up_taps(o, Wi, i0, i1, w0, w1);
-      const float wgt = (i0 == q.x ? w0 : 0.0f) + (i1 == q.x ? w1 : 0.0f);
-      if (wgt != 0.0f) { ox[nx] = o; wxv[nx] = wgt; ++nx; }
-    }
-    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0}, v[8], av[8];
-    for (int a1 = 0; a1 < ny; ++a1)
-      for (int a2 = 0; a2 < nx; ++a2) {
-        ld8(dout.p + act_index(dout, q.b, q.g, oy[a1], ox[a2], Ho, Wo), v);
-        const float wgt = wyv[a1] * wxv[a2];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) s[j] += wgt * v[j];
+    const __nv_bfloat16 *av_row = act.p + act_index(act, b, g, y, 0, Hi, Wi);
+    __nv_bfloat16 *o_row = din.p + act_index(din, b, g, y, 0, Hi, Wi);
+    for (int x = threadIdx.x; x < Wi; x += blockDim.x) {
+      float wxv[4];
+      int ox[4];
+      int nx = 0;
+      for (int o = max(2 * x - 1, 0); o <= min(2 * x + 2, Wo - 1); ++o) {
+        int i0, i1;
+        float w0, w1;
+        up_taps(o, Wi, i0, i1, w0, w1);
+        const float wgt = (i0 == x ? w0 : 0.0f) + (i1 == x ? w1 : 0.0f);
+        if (wgt != 0.0f) { ox[nx] = o; wxv[nx] = wgt; ++nx; }
       }
-    ld8(act.p + act_index(act, q.b, q.g, q.y, q.x, Hi, Wi), av);
+      float s[8] = {0, 0, 0, 0, 0, 0, 0, 0}, v[8], av[8];
+      for (int a1 = 0; a1 < ny; ++a1) {
+        const __nv_bfloat16 *d_row = dout.p + act_index(dout, b, g, oy[a1], 0, Ho, Wo);
+        for (int a2 = 0; a2 < nx; ++a2) {
+          ld8(d_row + (long long)ox[a2] * 8, v);
+          const float wgt = wyv[a1] * wxv[a2];
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-      if (!(av[j] > 0.0f)) s[j] = 0.0f;
-    st8(din.p + act_index(din, q.b, q.g, q.y, q.x, Hi, Wi), s);
+          for (int j = 0; j < 8; ++j) s[j] += wgt * v[j];
+        }
+      }
+      ld8(av_row + (long long)x * 8, av);
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (!(av[j] > 0.0f)) s[j] = 0.0f;
+      st8(o_row + (long long)x * 8, s);
+    }
   }
 }
 
@@ -433,53 +468,71 @@ __global__ void k_compose_guess(const float *g, const float *corr, int W, int H,
 // ----------------------------------------------------------------------------
 // (the weight gradient's final sum, launched by launch_wgrad_reduce)
 // Sum the per-chunk partials in chunk order: dW[co][tap][ci] (fp32), then,
-// with db, db[co] from its [chunks][cout] partials. One thread per output,
-// consecutive threads on consecutive partials of a chunk (coalesced): the
-// thread keeps 32 running sums, sum l over chunks l, l + 32, ... in chunk
-// order, and combines them by the fixed tree s[l] += s[l + o], o = 16, 8, 4,
-// 2, 1.
-__global__ void k_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, const float *db_part,
-                               float *db) {
+// with db, db[co] from its [chunks][cout] partials. A block takes 32
+// consecutive outputs (lane = output, so each warp's loads are coalesced);
+// warp w forms the running sum over chunks w, w + 32, ... in chunk order, and
+// warp 0 combines the 32 sums by the fixed tree s[l] += s[l + o], o = 16, 8,
+// 4, 2, 1.
+__global__ void __launch_bounds__(1024) k_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw,
+                                                       const float *db_part, float *db) {
+  __shared__ float sh[32][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long long wtotal = (long long)cout * 9 * cin;
   const long long total = wtotal + (db ? cout : 0);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const float *src;
-    long long stride;
-    if (i < wtotal) {
-      const int co = (int)(i / (9 * cin)), r = (int)(i - (long long)co * 9 * cin), tap = r / cin, ci = r - tap * cin;
-      src = part + ((long long)tap * cout + co) * cin + ci;
-      stride = wtotal;
-    } else {
-      src = db_part + (i - wtotal);
-      stride = cout;
+  for (long long i0 = blockIdx.x * 32LL; i0 < total; i0 += gridDim.x * 32LL) {
+    const long long i = i0 + lane;
+    float s = 0.0f;
+    if (i < total) {
+      const float *src;
+      long long stride;
+      if (i < wtotal) {
+        const int co = (int)(i / (9 * cin)), r = (int)(i - (long long)co * 9 * cin), tap = r / cin, ci = r - tap * cin;
+        src = part + ((long long)tap * cout + co) * cin + ci;
+        stride = wtotal;
+      } else {
+        src = db_part + (i - wtotal);
+        stride = cout;
+      }
+      for (int k = w; k < nchunks; k += 32) s += src[(long long)k * stride];
     }
-    float s[32];
+    sh[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && i < total) {
+      float v[32];
 #pragma unroll
-    for (int l = 0; l < 32; ++l) s[l] = 0.0f;
-    for (int k0 = 0; k0 < nchunks; k0 += 32) {
+      for (int l = 0; l < 32; ++l) v[l] = sh[l][lane];
 #pragma unroll
-      for (int l = 0; l < 32; ++l)
-        if (k0 + l < nchunks) s[l] += src[(long long)(k0 + l) * stride];
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int l = 0; l < o; ++l) v[l] += v[l + o];
+      if (i < wtotal)
+        dw[i] = v[0];
+      else
+        db[i - wtotal] = v[0];
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-      for (int l = 0; l < o; ++l) s[l] += s[l + o];
-    if (i < wtotal)
-      dw[i] = s[0];
-    else
-      db[i - wtotal] = s[0];
+    __syncthreads();
   }
 }
 
 cudaError_t launch_wgrad_reduce(const float *part, int nchunks, int cout, int cin, float *dw, const float *db_part,
                                 float *db, cudaStream_t st) {
   const long long total = (long long)cout * 9 * cin + (db ? cout : 0);
-  long long blocks = (total + 127) / 128;
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  k_wgrad_reduce<<<(unsigned)blocks, 128, 0, st>>>(part, nchunks, cout, cin, dw, db_part, db);
+  long long blocks = (total + 31) / 32;
+  if (blocks > 148 * 2) blocks = 148 * 2;
+  k_wgrad_reduce<<<(unsigned)blocks, 1024, 0, st>>>(part, nchunks, cout, cin, dw, db_part, db);
   return cudaGetLastError();
+}
+
+// Row kernels: 256-thread blocks of row_threads(w) threads across a row (a
+// multiple of 32, at most 256) times 256 / row_threads(w) rows, rows in a
+// grid-stride loop over a fixed number of blocks.
+static dim3 row_threads(int w) {
+  const unsigned tx = (unsigned)std::min(256, std::max(32, (w + 31) / 32 * 32));
+  return dim3(tx, 256 / tx);
+}
+static unsigned row_blocks(long long rows, int w) {
+  const long long per = 256 / row_threads(w).x;
+  return (unsigned)std::min<long long>(std::max<long long>((rows + per - 1) / per, 1), 148 * 16);
 }
 
 static unsigned blocks_for(long long n, int threads) {
@@ -500,18 +553,18 @@ cudaError_t launch_avgpool2(const ActView &in, const ActView &out, int B, int H,
 }
 cudaError_t launch_unpool_add_mask(const ActView &dskip, const ActView &dpool, const ActView &act,
                                    const ActView &out, int B, int H, int W, int groups, cudaStream_t st) {
-  k_unpool_add_mask<<<blocks_for((long long)B * groups * H * W, 256), 256, 0, st>>>(dskip, dpool, act, out, B, H,
-                                                                                    W, groups);
+  k_unpool_add_mask<<<row_blocks((long long)B * groups * H, W), row_threads(W), 0, st>>>(dskip, dpool, act, out, B, H,
+                                                                                       W, groups);
   return cudaGetLastError();
 }
 cudaError_t launch_upsample2(const ActView &in, const ActView &out, int B, int Hi, int Wi, int groups,
                              cudaStream_t st) {
-  k_upsample2<<<blocks_for((long long)B * groups * Hi * Wi * 4, 256), 256, 0, st>>>(in, out, B, Hi, Wi, groups);
+  k_upsample2<<<row_blocks((long long)B * groups * 2 * Hi, 2 * Wi), row_threads(2 * Wi), 0, st>>>(in, out, B, Hi, Wi, groups);
   return cudaGetLastError();
 }
 cudaError_t launch_upsample2_bwd(const ActView &dout, const ActView &act, const ActView &din, int B, int Hi,
                                  int Wi, int groups, cudaStream_t st) {
-  k_upsample2_bwd<<<blocks_for((long long)B * groups * Hi * Wi, 256), 256, 0, st>>>(dout, act, din, B, Hi, Wi,
+  k_upsample2_bwd<<<row_blocks((long long)B * groups * Hi, Wi), row_threads(Wi), 0, st>>>(dout, act, din, B, Hi, Wi,
                                                                                     groups);
   return cudaGetLastError();
 }
