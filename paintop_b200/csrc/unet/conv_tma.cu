@@ -21,7 +21,8 @@
 // nine taps of all R rows.
 //
 // k_conv_tma<N> (forward / backward-data): per output row, GEMM rows = the
-// segment's pixels (M = 128; rows past SW are never stored), columns = N
+// segment's pixels (M = 128, or 64 when SW <= 64; rows past SW are never
+// stored), columns = N
 // output channels (the CTA's part [n0, n0 + N) of them: blockIdx.y), K = (tap,
 // channel) taken in chunks of cg channel groups (chosen per layer, at most
 // 64 channels) per pipeline stage: K groups (g, g+1) of one tap are (R + 2) *
@@ -143,6 +144,10 @@ __global__ void __launch_bounds__(kConvThreads, 2)
   const int stage_bytes = GB * gstride * 16;
   const int n0 = blockIdx.y * N;      // the CTA's output channels
   const int nis = min(kIssuers, R);   // issuers with rows: issuer i takes rows i, i + nis, ...
+  // GEMM rows per MMA: 64 when the segment has at most 64 pixels (half the A
+  // operand read per MMA); the accumulator's row m then sits in TMEM lane
+  // (m % 16) + 32 (m / 16)
+  const int MT = g.s.SW <= 64 ? 64 : 128;
   const unsigned long long wait_ns = a.wait_ns ? a.wait_ns : kWaitNs;
   unsigned char *sW = sm;
   unsigned char *sA = sm + g.w_bytes;
@@ -206,7 +211,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
     // ---------------- MMA issuers: each owns the accumulators of its rows ----------------
     const int issuer = warp - kMmaWarp;
     if (lane == 0 && issuer < nis) {
-      const uint32_t idesc = instr_desc_bf16(128, N, false, false);
+      const uint32_t idesc = instr_desc_bf16(MT, N, false, false);
       // descriptors advance by adding (bytes >> 4) to their address field
       const uint64_t bdesc0 = smem_desc(smem_u32(sW), (N / 8) * 128, 128);
       const uint32_t bgrp = (uint32_t)((N / 8) * 128) >> 4;   // one K group of the weights
@@ -262,7 +267,11 @@ __global__ void __launch_bounds__(kConvThreads, 2)
     // ------- epilogue: warpgroup wg takes tiles wg, wg + kEpiGroups, ...;
     //         warp w reads TMEM lanes 32 (w % 4) .. + 31 -------
     const int wg = warp / 4, q = warp % 4;
-    const int m = 32 * q + lane;  // GEMM row = pixel of the segment
+    // GEMM row = pixel m of the segment; warp q reads TMEM lanes 32 q .. 32 q +
+    // 31, which hold rows 32 q + lane (M = 128) or, for lanes below 16, rows
+    // 16 q + lane (M = 64)
+    const int m = MT == 64 ? 16 * q + lane : 32 * q + lane;
+    const bool row_here = MT == 128 || lane < 16;
     int k = 0;
     for (int tile = blockIdx.x + wg * gridDim.x; tile < ntiles; tile += kEpiGroups * gridDim.x, ++k) {
       // lane 0 decides for the warp: tmem loads below are warp-collective
@@ -274,7 +283,7 @@ __global__ void __launch_bounds__(kConvThreads, 2)
       if (!__shfl_sync(0xffffffffu, go, 0)) break;
       tc_fence_after_sync();
       const int b = tile / HW, r = tile - b * HW, rg = r / g.s.segs_x, x = (r - rg * g.s.segs_x) * SW + m;
-      const bool valid = m < SW && x < a.W;
+      const bool valid = row_here && m < SW && x < a.W;
 #pragma unroll 1
       for (int orow = 0; orow < R; ++orow) {
       const int y = rg * R + orow;
