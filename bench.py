@@ -952,9 +952,10 @@ def gpu_arm(args):
                     "d2h_bytes_per_step": d2h,
                     "inputs_bytes_per_step": 4 * (2 * n_img + n_mask),
                     "note": "pinned host buffers through pt_poisson_solve; the library uploads the masks, then "
-                            "source and target only in the tile row bands holding interior cells and one row "
-                            "either side, and downloads only those bands of the output; the other output rows "
-                            "are the target, copied on the host inside the call"},
+                            "source and target only in the tile row bands holding interior cells, each band as "
+                            "one rectangle (its span of interior tile columns, one pixel and one row either "
+                            "side), and downloads only the bands' spans of the output; the rest of the output "
+                            "is the target, copied on the host inside the call"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "dram_frac": (traffic / (float(kms.mean()) / 1e3) / 1e9 / peak) if traffic else None,

@@ -260,10 +260,11 @@ pt_status pt_ctx_last_timing(const pt_ctx *ctx, double *solve_kernel_ms, double 
 /* Bytes the context's last red-black solve call (pt_poisson_solve or
  * pt_poisson_solve_batch without PT_FLAG_MULTIGRID) moved between host and
  * device. With host buffers a solve uploads the masks, then source, target
- * and guess only in the tile row bands that hold interior cells and one row
- * either side (the rows the solve reads), and downloads only those bands of
- * the output; the other output rows are the target, copied on the host. Other
- * calls set both counts to 0 (not counted). */
+ * and guess only in the tile row bands that hold interior cells, each band as
+ * one rectangle (its span of interior tile columns, one pixel and one row
+ * either side: the part the solve reads), and downloads only the bands'
+ * spans of the output; the rest of the output is the target, copied on the
+ * host. Other calls set both counts to 0 (not counted). */
 pt_status pt_ctx_last_transfer(const pt_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 
 /* ---- tile configurations and the autotuner (no reference counterpart: the

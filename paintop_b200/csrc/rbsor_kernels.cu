@@ -499,12 +499,19 @@ __global__ void k_emit(KParams P, int sys0, int TW, int TH) {
 // tile with interior cells, else 0. The solve reads an image's source and
 // target only in those bands and one row either side; the output of every
 // other band is the target, bit for bit (k_emit).
-__global__ void k_band_flags(KParams P, int sys0, int *flags) {
+// Per row band of tiles: the first and last tile column holding interior
+// cells, or -1, -1 when the band holds none (two ints per band).
+__global__ void k_band_flags(KParams P, int sys0, int *spans) {
   const SysDesc d = P.sys[sys0];
   for (int ty = threadIdx.x; ty < d.nty; ty += blockDim.x) {
-    int any = 0;
-    for (int tx = 0; tx < d.ntx && !any; ++tx) any = P.tcount[d.tile0 + ty * d.ntx + tx] > 0;
-    flags[ty] = any;
+    int lo = -1, hi = -1;
+    for (int tx = 0; tx < d.ntx; ++tx)
+      if (P.tcount[d.tile0 + ty * d.ntx + tx] > 0) {
+        if (lo < 0) lo = tx;
+        hi = tx;
+      }
+    spans[2 * ty] = lo;
+    spans[2 * ty + 1] = hi;
   }
 }
 
@@ -1095,8 +1102,8 @@ cudaError_t launch_tile_count(const KParams &P, const TileConfig &tc, cudaStream
   return cudaGetLastError();
 }
 
-cudaError_t launch_band_flags(const KParams &P, int sys0, int *flags, cudaStream_t stream) {
-  k_band_flags<<<1, 256, 0, stream>>>(P, sys0, flags);
+cudaError_t launch_band_flags(const KParams &P, int sys0, int *spans, cudaStream_t stream) {
+  k_band_flags<<<1, 256, 0, stream>>>(P, sys0, spans);
   return cudaGetLastError();
 }
 

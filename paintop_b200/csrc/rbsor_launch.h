@@ -28,9 +28,10 @@ cudaError_t prepare_solve(const KParams &P, int cfg, int sms, int *grid);
 cudaError_t launch_prepared(const KParams &P, int cfg, int grid, cudaStream_t stream);
 // k_tile_count alone (interior cells and box per tile; reads only the masks).
 cudaError_t launch_tile_count(const KParams &P, const TileConfig &tc, cudaStream_t stream);
-// flags[ty] = whether row band ty of image sys0 holds a tile with interior
-// cells (the solve reads the image only there and one row either side).
-cudaError_t launch_band_flags(const KParams &P, int sys0, int *flags, cudaStream_t stream);
+// spans[2 ty], spans[2 ty + 1] = the first and last tile column of row band ty
+// of image sys0 that hold interior cells, or -1, -1 (the solve reads the
+// image only there, one pixel around).
+cudaError_t launch_band_flags(const KParams &P, int sys0, int *spans, cudaStream_t stream);
 // Interleave one image's channels sys0 .. sys0+C-1 into its output.
 cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,
                         cudaStream_t stream);

@@ -97,7 +97,8 @@ struct Layout {
       mask, out, regions, label, rsize, rmax, bands, total;
 };
 
-// Row bands of every image (one flag each, host-buffer solves).
+// Row bands of every image (host-buffer solves: two ints each, the band's
+// span of tile columns with interior cells).
 size_t band_count(const Plan &pl) {
   size_t n = 0;
   for (const SysDesc &d : pl.sys)
@@ -136,7 +137,7 @@ Layout layout(const Plan &pl, bool stage) {
   L.label = take((size_t)pl.rpix * sizeof(int));
   L.rsize = take((size_t)pl.rpix * sizeof(int));
   L.rmax = take(pl.regions.size() * sizeof(int));
-  L.bands = stage ? take(band_count(pl) * sizeof(int)) : 0;
+  L.bands = stage ? take(2 * band_count(pl) * sizeof(int)) : 0;
   L.total = o;
   return L;
 }
@@ -321,53 +322,53 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   P.rsize = reinterpret_cast<int *>(base + L.rsize);
   P.rmax = reinterpret_cast<int *>(base + L.rmax);
 
-  // ---- host buffers: upload only the rows the solve reads. The tiles are
-  // counted from the masks, and for each image the row bands that hold an
-  // interior tile come back to the host (one int per band). The solve reads
-  // source, target and guess only at interior cells and their four
-  // neighbours, so those bands and one row either side go up; the output rows
-  // of the other bands are the target bit for bit and are filled on the host
+  // ---- host buffers: upload only the part of the images the solve reads.
+  // The tiles are counted from the masks, and for each image and row band of
+  // tiles the first and last tile column holding interior cells come back to
+  // the host (two ints per band). The solve reads source, target and guess
+  // only at interior cells and their four neighbours, so each such band goes
+  // up as one rectangle: its rows and one row either side, its span of tile
+  // columns and one pixel either side. Only the band's span comes down; the
+  // rest of the output is the target bit for bit and is filled on the host
   // while the GPU works.
-  std::vector<int> bandf;
+  std::vector<int> spans;
+  const size_t tw = (size_t)pl.tc.tw, th = (size_t)pl.tc.th;
   if (!devptr) {
     int *bands = reinterpret_cast<int *>(base + L.bands);
     ce = launch_tile_count(P, pl.tc, st);
     size_t nb = 0;
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
       if (ps[i].channels == 0) continue;
-      ce = launch_band_flags(P, sys0[i], bands + nb, st);
+      ce = launch_band_flags(P, sys0[i], bands + 2 * nb, st);
       nb += (size_t)pl.sys[sys0[i]].nty;
     }
-    bandf.assign(nb, 0);
+    spans.assign(2 * nb, -1);
     if (ce == cudaSuccess && nb)
-      ce = cudaMemcpyAsync(bandf.data(), bands, nb * sizeof(int), cudaMemcpyDeviceToHost, st);
+      ce = cudaMemcpyAsync(spans.data(), bands, 2 * nb * sizeof(int), cudaMemcpyDeviceToHost, st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "band flags");
-    d2h += nb * sizeof(int);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "band spans");
+    d2h += 2 * nb * sizeof(int);
     size_t boff = 0;
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
       const pt_problem &p = ps[i];
       if (p.channels == 0) continue;
       const SysDesc &d0 = pl.sys[sys0[i]];
-      const size_t row = (size_t)p.width * p.channels, TH = (size_t)pl.tc.th, H = p.height;
-      const int *f = bandf.data() + boff;
-      for (int ty = 0; ty < d0.nty && ce == cudaSuccess;) {
-        int ty1 = ty + 1;
-        while (ty1 < d0.nty && f[ty1] == f[ty]) ++ty1;
-        if (f[ty]) {
-          const size_t r0 = ty * TH > 0 ? ty * TH - 1 : 0, r1 = std::min(H, ty1 * TH + 1);
-          const size_t off = r0 * row, bytes = (r1 - r0) * row * sizeof(float);
-          ce = cudaMemcpyAsync(const_cast<float *>(d0.src) + off, p.source_or_guidance + off, bytes,
+      const size_t C = p.channels, W = p.width, H = p.height, pitch = W * C * sizeof(float);
+      const int *f = spans.data() + 2 * boff;
+      for (int ty = 0; ty < d0.nty && ce == cudaSuccess; ++ty) {
+        if (f[2 * ty] < 0) continue;
+        const size_t r0 = ty * th > 0 ? ty * th - 1 : 0, r1 = std::min(H, (ty + 1) * th + 1);
+        const size_t x0 = f[2 * ty] * tw > 0 ? f[2 * ty] * tw - 1 : 0, x1 = std::min(W, (f[2 * ty + 1] + 1) * tw + 1);
+        const size_t off = r0 * W * C + x0 * C, wb = (x1 - x0) * C * sizeof(float), rows = r1 - r0;
+        ce = cudaMemcpy2DAsync(const_cast<float *>(d0.src) + off, pitch, p.source_or_guidance + off, pitch, wb, rows,
                                cudaMemcpyHostToDevice, st);
-          if (ce == cudaSuccess)
-            ce = cudaMemcpyAsync(const_cast<float *>(d0.tgt) + off, p.target_or_anchor + off, bytes,
+        if (ce == cudaSuccess)
+          ce = cudaMemcpy2DAsync(const_cast<float *>(d0.tgt) + off, pitch, p.target_or_anchor + off, pitch, wb, rows,
                                  cudaMemcpyHostToDevice, st);
-          if (ce == cudaSuccess && (p.flags & PT_FLAG_WARM_START))
-            ce = cudaMemcpyAsync(const_cast<float *>(d0.guess) + off, p.initial_guess + off, bytes,
+        if (ce == cudaSuccess && (p.flags & PT_FLAG_WARM_START))
+          ce = cudaMemcpy2DAsync(const_cast<float *>(d0.guess) + off, pitch, p.initial_guess + off, pitch, wb, rows,
                                  cudaMemcpyHostToDevice, st);
-          h2d += bytes * ((p.flags & PT_FLAG_WARM_START) ? 3 : 2);
-        }
-        ty = ty1;
+        h2d += wb * rows * ((p.flags & PT_FLAG_WARM_START) ? 3 : 2);
       }
       boff += (size_t)d0.nty;
     }
@@ -447,8 +448,9 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   d2h += nsys * sizeof(SysState) + sizeof(int);
   ce = cudaMemcpyAsync(states.data(), base + L.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&kerr, base + L.err, sizeof(int), cudaMemcpyDeviceToHost, st);
-  // host buffers: the bands with interior tiles come down after the emit;
-  // the other rows are the target (filled on the host below)
+  // host buffers: each band's span of interior tiles comes down after the
+  // emit; the rest of the output is the target (segments of rows, filled on
+  // the host below)
   struct HostRows { float *out; const float *tgt; size_t off, n; };
   std::vector<HostRows> host_rows;
   if (!devptr && ce == cudaSuccess) {
@@ -456,19 +458,29 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
       if (ps[i].channels == 0) continue;
       const SysDesc &d0 = pl.sys[sys0[i]];
-      const size_t row = (size_t)ps[i].width * ps[i].channels, TH = (size_t)pl.tc.th, H = ps[i].height;
-      const int *f = bandf.data() + boff;
+      const size_t C = ps[i].channels, W = ps[i].width, H = ps[i].height, row = W * C;
+      const int *f = spans.data() + 2 * boff;
       for (int ty = 0; ty < d0.nty && ce == cudaSuccess;) {
-        int ty1 = ty + 1;
-        while (ty1 < d0.nty && f[ty1] == f[ty]) ++ty1;
-        const size_t r0 = ty * TH, r1 = std::min(H, ty1 * TH), off = r0 * row, cnt = (r1 - r0) * row;
-        if (f[ty]) {
-          ce = cudaMemcpyAsync(outs[i] + off, d0.out + off, cnt * sizeof(float), cudaMemcpyDeviceToHost, st);
-          d2h += cnt * sizeof(float);
-        } else {
-          host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, off, cnt});
+        const size_t r0 = ty * th;
+        if (f[2 * ty] < 0) {  // a run of bands without interior tiles: whole rows
+          int ty1 = ty + 1;
+          while (ty1 < d0.nty && f[2 * ty1] < 0) ++ty1;
+          const size_t r1 = std::min(H, ty1 * th);
+          host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, r0 * row, (r1 - r0) * row});
+          ty = ty1;
+          continue;
         }
-        ty = ty1;
+        const size_t r1 = std::min(H, (ty + 1) * th);
+        const size_t x0 = f[2 * ty] * tw, x1 = std::min(W, (f[2 * ty + 1] + 1) * tw);
+        const size_t off = r0 * row + x0 * C, wb = (x1 - x0) * C * sizeof(float);
+        ce = cudaMemcpy2DAsync(outs[i] + off, row * sizeof(float), d0.out + off, row * sizeof(float), wb, r1 - r0,
+                               cudaMemcpyDeviceToHost, st);
+        d2h += wb * (r1 - r0);
+        for (size_t y = r0; y < r1; ++y) {
+          if (x0 > 0) host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, y * row, x0 * C});
+          if (x1 < W) host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, y * row + x1 * C, (W - x1) * C});
+        }
+        ++ty;
       }
       boff += (size_t)d0.nty;
     }
@@ -489,10 +501,10 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   }
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "result download");
   cudaEventRecord(ctx->ev[3], st);
-  // while the device works: the output rows that are the target. One host
-  // thread copies about 10 GB/s, a fifth of PCIe, so a large fill is split
-  // over up to eight threads, each taking one contiguous stretch of the
-  // concatenated rows.
+  // while the device works: the output that is the target. One host thread
+  // copies about 10 GB/s, a fifth of PCIe, so a large fill is split over up
+  // to eight threads, each taking one contiguous stretch of the concatenated
+  // segments.
   {
     size_t total = 0;
     for (const HostRows &r : host_rows) total += r.n;

@@ -456,14 +456,16 @@ def test_non_finite_inputs_follow_the_reference(ctx, oracle, case):
     assert np.array_equal(~np.isfinite(out), ~np.isfinite(ref))
 
 
-def test_host_buffers_move_only_the_rows_the_solve_reads(ctx):
+def test_host_buffers_move_only_the_part_the_solve_reads(ctx):
     """A host-buffer solve uploads source and target only in the tile row bands
-    that hold interior cells (and one row either side), downloads only those
-    bands, and fills the other output rows with the target on the host. Its
-    output and reports equal the device-pointer solve's (which reads whole
-    images) bit for bit, even after an earlier call left other images in the
-    staging buffers; a NaN in the target far from the region comes out
-    unchanged; and the bytes moved are the rows that were needed."""
+    that hold interior cells, each band as one rectangle (its span of interior
+    tile columns, one pixel and one row either side), downloads only the
+    bands' spans, and fills the rest of the output with the target on the
+    host. Its output and reports equal the device-pointer solve's (which reads
+    whole images) bit for bit, even after an earlier call left other images in
+    the staging buffers; NaNs in the target outside the spans (in a band
+    without interior cells, and beside the span in a band with them) come out
+    unchanged; and the bytes moved are the rectangles that were needed."""
     import torch
     from paintop_b200 import _lib
     w, h, c = 640, 600, 3
@@ -474,6 +476,7 @@ def test_host_buffers_move_only_the_rows_the_solve_reads(ctx):
     mask[250:330, 200:420] = 1.0
     tgt3 = tgt.reshape(h, w, c)
     tgt3[20, 30, 1] = np.nan  # far from the region: a target-only band
+    tgt3[260, 10, 0] = np.nan  # a band with interior cells, left of its span
     # fill the staging buffers with another image first
     other = random_problem(9, w, h, c, density=0.8)
     ctx.solve(*other, w, h, c, lam=0.01)
@@ -496,15 +499,21 @@ def test_host_buffers_move_only_the_rows_the_solve_reads(ctx):
         assert reps[k].final_residual == per_h[k]["final_residual"]
         assert hist[k * 2000: k * 2000 + reps[k].iterations].tolist() == per_h[k]["residual_history"]
     assert np.isnan(out_h.reshape(h, w, c)[20, 30, 1])
-    # bytes: the bands holding rows 250..329 (and one row either side) went up
-    # as source and target, plus the mask; only those bands came down
+    assert np.isnan(out_h.reshape(h, w, c)[260, 10, 0])
+    # bytes: each band holding rows 250..329 went up as one rectangle of source
+    # and target (its rows and one either side; the tile columns spanning
+    # 200..419 and one pixel either side), plus the mask; the bands' spans
+    # came down
     s_, tw_, th_ = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.lib().pt_tile_config_info(ctx.last_config(), C.byref(s_), C.byref(tw_), C.byref(th_))
-    th = th_.value
-    b0, b1 = 250 // th, 329 // th + 1
-    r0, r1 = max(0, b0 * th - 1), min(h, b1 * th + 1)
-    row = w * c * 4
-    assert up >= 2 * (r1 - r0) * row + w * h * 4 and up < 2 * (r1 - r0) * row + w * h * 4 + (1 << 20)
-    down_rows = (min(h, b1 * th) - b0 * th) * row
-    assert down >= down_rows and down < down_rows + (1 << 20)
+    tw, th = tw_.value, th_.value
+    assert 10 < (200 // tw) * tw - 1  # the second NaN lies left of the span
+    x0, x1 = max(0, (200 // tw) * tw - 1), min(w, (419 // tw + 1) * tw + 1)
+    xd0, xd1 = (200 // tw) * tw, min(w, (419 // tw + 1) * tw)
+    up_rows = sum(min(h, (b + 1) * th + 1) - max(0, b * th - 1) for b in range(250 // th, 329 // th + 1))
+    down_rows = sum(min(h, (b + 1) * th) - b * th for b in range(250 // th, 329 // th + 1))
+    up_img = 2 * up_rows * (x1 - x0) * c * 4
+    assert up >= up_img + w * h * 4 and up < up_img + w * h * 4 + (1 << 20)
+    down_img = down_rows * (xd1 - xd0) * c * 4
+    assert down >= down_img and down < down_img + (1 << 20)
     assert up < 2 * w * h * c * 4
