@@ -333,6 +333,17 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   // while the GPU works.
   std::vector<int> spans;
   const size_t tw = (size_t)pl.tc.tw, th = (size_t)pl.tc.th;
+  // the output that is the target: segments of rows, copied on the host by
+  // worker threads while the device works (joined before the call returns,
+  // on every path: the joiner is destroyed before the segments)
+  struct HostRows { float *out; const float *tgt; size_t off, n; };
+  std::vector<HostRows> host_rows;
+  struct Joiner {
+    std::vector<std::thread> pool;
+    ~Joiner() {
+      for (auto &t : pool) t.join();
+    }
+  } fill_job;
   if (!devptr) {
     int *bands = reinterpret_cast<int *>(base + L.bands);
     ce = launch_tile_count(P, pl.tc, st);
@@ -373,6 +384,61 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       boff += (size_t)d0.nty;
     }
     if (ce != cudaSuccess) return cuda_fail(ctx, ce, "input upload");
+
+    // The output outside the bands' spans is the target bit for bit: whole
+    // rows of bands without interior tiles, the row segments beside each
+    // span. It does not depend on the solve, so it is copied now, beside the
+    // device work, on worker threads: one host thread copies about 10 GB/s,
+    // a fifth of PCIe, so a large fill is split over up to eight threads,
+    // each taking one contiguous stretch of the concatenated segments; a fill
+    // below 256 KB is done here.
+    boff = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      if (ps[i].channels == 0) continue;
+      const SysDesc &d0 = pl.sys[sys0[i]];
+      const size_t C = ps[i].channels, W = ps[i].width, H = ps[i].height, row = W * C;
+      const int *f = spans.data() + 2 * boff;
+      for (int ty = 0; ty < d0.nty;) {
+        const size_t r0 = ty * th;
+        if (f[2 * ty] < 0) {  // a run of bands without interior tiles: whole rows
+          int ty1 = ty + 1;
+          while (ty1 < d0.nty && f[2 * ty1] < 0) ++ty1;
+          const size_t r1 = std::min(H, ty1 * th);
+          host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, r0 * row, (r1 - r0) * row});
+          ty = ty1;
+          continue;
+        }
+        const size_t r1 = std::min(H, (ty + 1) * th);
+        const size_t x0 = f[2 * ty] * tw, x1 = std::min(W, (f[2 * ty + 1] + 1) * tw);
+        for (size_t y = r0; y < r1; ++y) {
+          if (x0 > 0) host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, y * row, x0 * C});
+          if (x1 < W) host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, y * row + x1 * C, (W - x1) * C});
+        }
+        ++ty;
+      }
+      boff += (size_t)d0.nty;
+    }
+    size_t total = 0;
+    for (const HostRows &r : host_rows) total += r.n;
+    const HostRows *segs = host_rows.data();
+    const size_t nsegs = host_rows.size();
+    auto fill = [segs, nsegs](size_t b0, size_t b1) {  // element range of the concatenation
+      size_t at = 0;
+      for (size_t k = 0; k < nsegs; ++k) {
+        const HostRows &r = segs[k];
+        const size_t lo = std::max(b0, at), hi = std::min(b1, at + r.n);
+        if (lo < hi) std::memcpy(r.out + r.off + (lo - at), r.tgt + r.off + (lo - at), (hi - lo) * sizeof(float));
+        at += r.n;
+      }
+    };
+    const size_t bytes = total * sizeof(float);
+    if (bytes < (256u << 10)) {
+      fill(0, total);
+    } else {
+      const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+      const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, bytes >> 22));
+      for (unsigned k = 0; k < nt; ++k) fill_job.pool.emplace_back(fill, total * k / nt, total * (k + 1) / nt);
+    }
   }
 
   int grid = 0;
@@ -449,10 +515,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   ce = cudaMemcpyAsync(states.data(), base + L.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&kerr, base + L.err, sizeof(int), cudaMemcpyDeviceToHost, st);
   // host buffers: each band's span of interior tiles comes down after the
-  // emit; the rest of the output is the target (segments of rows, filled on
-  // the host below)
-  struct HostRows { float *out; const float *tgt; size_t off, n; };
-  std::vector<HostRows> host_rows;
+  // emit (the rest of the output is being filled on the host)
   if (!devptr && ce == cudaSuccess) {
     size_t boff = 0;
     for (uint32_t i = 0; i < n && ce == cudaSuccess; ++i) {
@@ -460,27 +523,14 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
       const SysDesc &d0 = pl.sys[sys0[i]];
       const size_t C = ps[i].channels, W = ps[i].width, H = ps[i].height, row = W * C;
       const int *f = spans.data() + 2 * boff;
-      for (int ty = 0; ty < d0.nty && ce == cudaSuccess;) {
-        const size_t r0 = ty * th;
-        if (f[2 * ty] < 0) {  // a run of bands without interior tiles: whole rows
-          int ty1 = ty + 1;
-          while (ty1 < d0.nty && f[2 * ty1] < 0) ++ty1;
-          const size_t r1 = std::min(H, ty1 * th);
-          host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, r0 * row, (r1 - r0) * row});
-          ty = ty1;
-          continue;
-        }
-        const size_t r1 = std::min(H, (ty + 1) * th);
+      for (int ty = 0; ty < d0.nty && ce == cudaSuccess; ++ty) {
+        if (f[2 * ty] < 0) continue;
+        const size_t r0 = ty * th, r1 = std::min(H, (ty + 1) * th);
         const size_t x0 = f[2 * ty] * tw, x1 = std::min(W, (f[2 * ty + 1] + 1) * tw);
         const size_t off = r0 * row + x0 * C, wb = (x1 - x0) * C * sizeof(float);
         ce = cudaMemcpy2DAsync(outs[i] + off, row * sizeof(float), d0.out + off, row * sizeof(float), wb, r1 - r0,
                                cudaMemcpyDeviceToHost, st);
         d2h += wb * (r1 - r0);
-        for (size_t y = r0; y < r1; ++y) {
-          if (x0 > 0) host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, y * row, x0 * C});
-          if (x1 < W) host_rows.push_back(HostRows{outs[i], ps[i].target_or_anchor, y * row + x1 * C, (W - x1) * C});
-        }
-        ++ty;
       }
       boff += (size_t)d0.nty;
     }
@@ -501,32 +551,6 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   }
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "result download");
   cudaEventRecord(ctx->ev[3], st);
-  // while the device works: the output that is the target. One host thread
-  // copies about 10 GB/s, a fifth of PCIe, so a large fill is split over up
-  // to eight threads, each taking one contiguous stretch of the concatenated
-  // segments.
-  {
-    size_t total = 0;
-    for (const HostRows &r : host_rows) total += r.n;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned nt = total * sizeof(float) >= (8u << 20) ? std::min(8u, hw) : 1u;
-    auto fill = [&](size_t b0, size_t b1) {  // element range of the concatenation
-      size_t base = 0;
-      for (const HostRows &r : host_rows) {
-        const size_t lo = std::max(b0, base), hi = std::min(b1, base + r.n);
-        if (lo < hi) std::memcpy(r.out + r.off + (lo - base), r.tgt + r.off + (lo - base), (hi - lo) * sizeof(float));
-        base += r.n;
-      }
-    };
-    if (nt <= 1) {
-      fill(0, total);
-    } else {
-      std::vector<std::thread> pool;
-      for (unsigned k = 1; k < nt; ++k) pool.emplace_back(fill, total * k / nt, total * (k + 1) / nt);
-      fill(0, total / nt);
-      for (auto &th : pool) th.join();
-    }
-  }
   ce = cudaStreamSynchronize(st);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "stream synchronize");
   {
