@@ -52,14 +52,16 @@ extern "C" {
  * (crates/paintop-ir/src/error.rs:23-114): PT_NO_DEVICE -> Policy (exit 4,
  * mirrors E_GPU_UNAVAILABLE in crates/paintop-wgpu/src/gpu/error.rs:17);
  * PT_INVALID_ARG -> Schema/Semantic as reported in pt_error; the rest ->
- * Execution (exit 5). */
+ * Execution (exit 5). No C++ exception leaves any entry point: a host
+ * allocation failure inside a call returns PT_OOM, any other host-side
+ * exception PT_INTERNAL, with the message in pt_ctx_last_error. */
 typedef enum pt_status {
   PT_OK = 0,
   PT_NO_DEVICE = 1,     /* no CUDA device / driver, or the device is not sm_100 */
   PT_INVALID_ARG = 2,   /* a null pointer, a bad size, or an out-of-range control */
   PT_LAUNCH_FAILED = 3, /* a CUDA launch or copy failed */
   PT_TIMEOUT = 4,       /* the device watchdog expired (bounded waits, wall budget) */
-  PT_OOM = 5,           /* device or pinned-host allocation failed */
+  PT_OOM = 5,           /* device or host allocation failed */
   PT_INTERNAL = 6       /* any other failure */
 } pt_status;
 

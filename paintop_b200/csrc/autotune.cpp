@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/paintop_cuda.h"
+#include "abi_guard.h"
 #include "ctx.h"
 #include "rbsor_launch.h"
 
@@ -129,9 +130,11 @@ pt_status pt_tile_config_info(uint32_t idx, int32_t *sweeps_per_step, int32_t *t
 }
 
 pt_status pt_ctx_set_config(pt_ctx *ctx, int32_t cfg) {
-  if (!ctx || cfg >= ptk::tile_config_count()) return PT_INVALID_ARG;
-  ctx->forced_cfg = cfg < 0 ? -1 : cfg;
-  return PT_OK;
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx || cfg >= ptk::tile_config_count()) return PT_INVALID_ARG;
+    ctx->forced_cfg = cfg < 0 ? -1 : cfg;
+    return PT_OK;
+  });
 }
 
 int32_t pt_ctx_last_config(const pt_ctx *ctx) { return ctx ? ctx->last_cfg : -1; }
@@ -143,46 +146,48 @@ int32_t pt_ctx_last_config(const pt_ctx *ctx) { return ctx ? ctx->last_cfg : -1;
 pt_status pt_autotune(pt_ctx *ctx, const pt_problem *ps, uint32_t n, uint32_t repeats,
                       float *const *outs, pt_report *const *reports, int32_t *chosen,
                       double *ms_per_config) {
-  if (!ctx || !ps || n == 0 || !outs || !reports) return PT_INVALID_ARG;
-  if (repeats == 0) repeats = 1;
-  int best = -1;
-  double best_ms = 0.0;
-  std::vector<double> ms_cfg((size_t)ptk::tile_config_count(), -1.0);
-  for (int cfg = 0; cfg < ptk::tile_config_count(); ++cfg) {
-    double cfg_best = -1.0;
-    for (uint32_t r = 0; r < repeats; ++r) {
-      cudaEvent_t a, b;
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      cudaEventRecord(a, ctx->stream);
-      const pt_status st = ptk_solve_batch(ctx, ps, n, outs, reports, nullptr, cfg);
-      cudaEventRecord(b, ctx->stream);
-      cudaEventSynchronize(b);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, a, b);
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
-      if (st != PT_OK) return st;
-      if (cfg_best < 0 || ms < cfg_best) cfg_best = ms;
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx || !ps || n == 0 || !outs || !reports) return PT_INVALID_ARG;
+    if (repeats == 0) repeats = 1;
+    int best = -1;
+    double best_ms = 0.0;
+    std::vector<double> ms_cfg((size_t)ptk::tile_config_count(), -1.0);
+    for (int cfg = 0; cfg < ptk::tile_config_count(); ++cfg) {
+      double cfg_best = -1.0;
+      for (uint32_t r = 0; r < repeats; ++r) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, ctx->stream);
+        const pt_status st = ptk_solve_batch(ctx, ps, n, outs, reports, nullptr, cfg);
+        cudaEventRecord(b, ctx->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (st != PT_OK) return st;
+        if (cfg_best < 0 || ms < cfg_best) cfg_best = ms;
+      }
+      if (ms_per_config) ms_per_config[cfg] = cfg_best;
+      ms_cfg[(size_t)cfg] = cfg_best;
+      if (best < 0 || cfg_best < best_ms) { best = cfg; best_ms = cfg_best; }
     }
-    if (ms_per_config) ms_per_config[cfg] = cfg_best;
-    ms_cfg[(size_t)cfg] = cfg_best;
-    if (best < 0 || cfg_best < best_ms) { best = cfg; best_ms = cfg_best; }
-  }
-  int entry = best;
-  {
-    std::lock_guard<std::mutex> lock(g_mu);
-    load_table_locked();
-    const uint32_t key = shape_key(ps, n);
-    auto it = g_table.find(key);
-    if (it != g_table.end() && it->second != best &&
-        best_ms >= (1.0 - kReplaceMargin) * ms_cfg[(size_t)it->second])
-      entry = it->second;  // within the margin of the incumbent: keep it
-    g_table[key] = entry;
-    save_table_locked();
-  }
-  if (chosen) *chosen = entry;
-  return PT_OK;
+    int entry = best;
+    {
+      std::lock_guard<std::mutex> lock(g_mu);
+      load_table_locked();
+      const uint32_t key = shape_key(ps, n);
+      auto it = g_table.find(key);
+      if (it != g_table.end() && it->second != best &&
+          best_ms >= (1.0 - kReplaceMargin) * ms_cfg[(size_t)it->second])
+        entry = it->second;  // within the margin of the incumbent: keep it
+      g_table[key] = entry;
+      save_table_locked();
+    }
+    if (chosen) *chosen = entry;
+    return PT_OK;
+  });
 }
 
 }  // extern "C"

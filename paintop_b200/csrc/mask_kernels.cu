@@ -35,6 +35,7 @@
 
 #include "../../include/paintop_cuda.h"
 #include "ctx.h"
+#include "abi_guard.h"
 
 namespace {
 
@@ -321,91 +322,95 @@ pt_status mask_finish(pt_ctx *ctx, size_t npx, bool device_out, float *mask, con
 extern "C" pt_status pt_mask_ellipse(pt_ctx *ctx, uint32_t width, uint32_t height, double center_x,
                                      double center_y, double radius_x, double radius_y, double angle_rad,
                                      double half_width_px, float *mask, uint32_t flags) {
-  if (!ctx) return PT_INVALID_ARG;
-  const size_t npx = (size_t)width * height;
-  if (npx && !mask) return mfail(ctx, PT_INVALID_ARG, "null mask buffer");
-  // the checks of EllipseGeometry::resolve (ellipse.rs:119-158)
-  if (!std::isfinite(center_x) || !std::isfinite(center_y) || !std::isfinite(angle_rad))
-    return mfail(ctx, PT_INVALID_ARG, "non-finite ellipse center or angle");
-  if (!(std::isfinite(radius_x) && radius_x > 0.0) || !(std::isfinite(radius_y) && radius_y > 0.0))
-    return mfail(ctx, PT_INVALID_ARG, "ellipse radii must be finite and > 0");
-  if (!std::isfinite(half_width_px) || half_width_px < 0.0)
-    return mfail(ctx, PT_INVALID_ARG, "feather half-width must be finite and >= 0");
-  if (npx == 0) return PT_OK;
-  if (npx > (size_t)INT32_MAX * 4) return mfail(ctx, PT_INVALID_ARG, "mask too large");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  cudaError_t ce = cudaSetDevice(ctx->device);
-  if (ce != cudaSuccess) return mfail(ctx, PT_NO_DEVICE, cudaGetErrorString(ce));
-  const bool dev = (flags & PT_FLAG_DEVICE_POINTERS) != 0;
-  float *out = nullptr;
-  char *scratch = nullptr;
-  pt_status st = mask_target(ctx, npx, dev, mask, 0, &out, &scratch);
-  if (st != PT_OK) return st;
-  if ((st = mask_begin(ctx)) != PT_OK) return st;
-  const double sn = std::sin(angle_rad), cs = std::cos(angle_rad);
-  const long long blocks = std::min<long long>(((long long)npx + 255) / 256, (long long)ctx->sms * 16);
-  cudaEventRecord(ctx->ev[1], ctx->stream);
-  k_mask_ellipse<<<(unsigned)blocks, 256, 0, ctx->stream>>>((int)width, (int)height, center_x, center_y,
-                                                           radius_x, radius_y, sn, cs, half_width_px, out);
-  cudaEventRecord(ctx->ev[2], ctx->stream);
-  return mask_finish(ctx, npx, dev, mask, out, 1);
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx) return PT_INVALID_ARG;
+    const size_t npx = (size_t)width * height;
+    if (npx && !mask) return mfail(ctx, PT_INVALID_ARG, "null mask buffer");
+    // the checks of EllipseGeometry::resolve (ellipse.rs:119-158)
+    if (!std::isfinite(center_x) || !std::isfinite(center_y) || !std::isfinite(angle_rad))
+      return mfail(ctx, PT_INVALID_ARG, "non-finite ellipse center or angle");
+    if (!(std::isfinite(radius_x) && radius_x > 0.0) || !(std::isfinite(radius_y) && radius_y > 0.0))
+      return mfail(ctx, PT_INVALID_ARG, "ellipse radii must be finite and > 0");
+    if (!std::isfinite(half_width_px) || half_width_px < 0.0)
+      return mfail(ctx, PT_INVALID_ARG, "feather half-width must be finite and >= 0");
+    if (npx == 0) return PT_OK;
+    if (npx > (size_t)INT32_MAX * 4) return mfail(ctx, PT_INVALID_ARG, "mask too large");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaError_t ce = cudaSetDevice(ctx->device);
+    if (ce != cudaSuccess) return mfail(ctx, PT_NO_DEVICE, cudaGetErrorString(ce));
+    const bool dev = (flags & PT_FLAG_DEVICE_POINTERS) != 0;
+    float *out = nullptr;
+    char *scratch = nullptr;
+    pt_status st = mask_target(ctx, npx, dev, mask, 0, &out, &scratch);
+    if (st != PT_OK) return st;
+    if ((st = mask_begin(ctx)) != PT_OK) return st;
+    const double sn = std::sin(angle_rad), cs = std::cos(angle_rad);
+    const long long blocks = std::min<long long>(((long long)npx + 255) / 256, (long long)ctx->sms * 16);
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    k_mask_ellipse<<<(unsigned)blocks, 256, 0, ctx->stream>>>((int)width, (int)height, center_x, center_y,
+                                                             radius_x, radius_y, sn, cs, half_width_px, out);
+    cudaEventRecord(ctx->ev[2], ctx->stream);
+    return mask_finish(ctx, npx, dev, mask, out, 1);
+  });
 }
 
 extern "C" pt_status pt_mask_polygon(pt_ctx *ctx, uint32_t width, uint32_t height, const double *points_xy,
                                      uint32_t n_points, int32_t fill_rule, float *mask, uint32_t flags) {
-  if (!ctx) return PT_INVALID_ARG;
-  const size_t npx = (size_t)width * height;
-  if (npx && !mask) return mfail(ctx, PT_INVALID_ARG, "null mask buffer");
-  if (n_points && !points_xy) return mfail(ctx, PT_INVALID_ARG, "null points");
-  if (fill_rule != PT_FILL_NONZERO && fill_rule != PT_FILL_EVEN_ODD)
-    return mfail(ctx, PT_INVALID_ARG, "unknown fill rule");
-  for (size_t k = 0; k < 2 * (size_t)n_points; ++k)
-    if (!std::isfinite(points_xy[k])) return mfail(ctx, PT_INVALID_ARG, "non-finite polygon coordinate");
-  if (npx == 0) return PT_OK;
-  // subsample column indices (4 per pixel) are int32 in the kernel
-  if (width > (1u << 28) || height > (uint32_t)INT32_MAX) return mfail(ctx, PT_INVALID_ARG, "mask too large");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  cudaError_t ce = cudaSetDevice(ctx->device);
-  if (ce != cudaSuccess) return mfail(ctx, PT_NO_DEVICE, cudaGetErrorString(ce));
-  const bool dev = (flags & PT_FLAG_DEVICE_POINTERS) != 0;
-  float *out = nullptr;
-  char *scratch = nullptr;
-  pt_status st = mask_target(ctx, npx, dev, mask, (size_t)n_points * sizeof(double4), &out, &scratch);
-  if (st != PT_OK) return st;
-  if ((st = mask_begin(ctx)) != PT_OK) return st;
-  if (n_points < 3) {  // contains() is false everywhere (mask_polygon.rs:162-165)
-    cudaEventRecord(ctx->ev[1], ctx->stream);
-    ce = cudaMemsetAsync(out, 0, npx * sizeof(float), ctx->stream);
-    cudaEventRecord(ctx->ev[2], ctx->stream);
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx) return PT_INVALID_ARG;
+    const size_t npx = (size_t)width * height;
+    if (npx && !mask) return mfail(ctx, PT_INVALID_ARG, "null mask buffer");
+    if (n_points && !points_xy) return mfail(ctx, PT_INVALID_ARG, "null points");
+    if (fill_rule != PT_FILL_NONZERO && fill_rule != PT_FILL_EVEN_ODD)
+      return mfail(ctx, PT_INVALID_ARG, "unknown fill rule");
+    for (size_t k = 0; k < 2 * (size_t)n_points; ++k)
+      if (!std::isfinite(points_xy[k])) return mfail(ctx, PT_INVALID_ARG, "non-finite polygon coordinate");
+    if (npx == 0) return PT_OK;
+    // subsample column indices (4 per pixel) are int32 in the kernel
+    if (width > (1u << 28) || height > (uint32_t)INT32_MAX) return mfail(ctx, PT_INVALID_ARG, "mask too large");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaError_t ce = cudaSetDevice(ctx->device);
+    if (ce != cudaSuccess) return mfail(ctx, PT_NO_DEVICE, cudaGetErrorString(ce));
+    const bool dev = (flags & PT_FLAG_DEVICE_POINTERS) != 0;
+    float *out = nullptr;
+    char *scratch = nullptr;
+    pt_status st = mask_target(ctx, npx, dev, mask, (size_t)n_points * sizeof(double4), &out, &scratch);
+    if (st != PT_OK) return st;
+    if ((st = mask_begin(ctx)) != PT_OK) return st;
+    if (n_points < 3) {  // contains() is false everywhere (mask_polygon.rs:162-165)
+      cudaEventRecord(ctx->ev[1], ctx->stream);
+      ce = cudaMemsetAsync(out, 0, npx * sizeof(float), ctx->stream);
+      cudaEventRecord(ctx->ev[2], ctx->stream);
+      if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, cudaGetErrorString(ce));
+      return mask_finish(ctx, npx, dev, mask, out, 0);
+    }
+    std::vector<double4> edges(n_points);
+    double ymin = points_xy[1], ymax = points_xy[1];
+    for (uint32_t k = 0; k < n_points; ++k) {
+      const uint32_t q = (k + 1) % n_points;
+      edges[k] = make_double4(points_xy[2 * k], points_xy[2 * k + 1], points_xy[2 * q], points_xy[2 * q + 1]);
+      ymin = std::min(ymin, points_xy[2 * k + 1]);
+      ymax = std::max(ymax, points_xy[2 * k + 1]);
+    }
+    double4 *dedges = reinterpret_cast<double4 *>(scratch);
+    ce = cudaMemcpyAsync(dedges, edges.data(), edges.size() * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream);
     if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, cudaGetErrorString(ce));
-    return mask_finish(ctx, npx, dev, mask, out, 0);
-  }
-  std::vector<double4> edges(n_points);
-  double ymin = points_xy[1], ymax = points_xy[1];
-  for (uint32_t k = 0; k < n_points; ++k) {
-    const uint32_t q = (k + 1) % n_points;
-    edges[k] = make_double4(points_xy[2 * k], points_xy[2 * k + 1], points_xy[2 * q], points_xy[2 * q + 1]);
-    ymin = std::min(ymin, points_xy[2 * k + 1]);
-    ymax = std::max(ymax, points_xy[2 * k + 1]);
-  }
-  double4 *dedges = reinterpret_cast<double4 *>(scratch);
-  ce = cudaMemcpyAsync(dedges, edges.data(), edges.size() * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream);
-  if (ce != cudaSuccess) return mfail(ctx, PT_LAUNCH_FAILED, cudaGetErrorString(ce));
-  const uint32_t spans = (width + kSpan - 1) / kSpan;
-  const int vec4 = (width % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
-  const int even_odd = fill_rule == PT_FILL_EVEN_ODD ? 1 : 0;
-  cudaEventRecord(ctx->ev[1], ctx->stream);
-  if (n_points > (uint32_t)kRowThreads) {
-    const dim3 grid(spans, std::min<uint32_t>(height, 65535u));
-    k_mask_polygon_chunked<<<grid, kRowThreads, 0, ctx->stream>>>((int)width, (int)height, dedges,
-                                                                  (int)n_points, even_odd, ymin, ymax, vec4, out);
-  } else {
-    // two waves of 4 resident blocks per SM, each block looping over rows of its span
-    const uint32_t rows = std::max<uint32_t>(1u, (uint32_t)(ctx->sms * 8) / spans);
-    const dim3 grid(spans, std::min<uint32_t>(std::min<uint32_t>(height, rows), 65535u));
-    k_mask_polygon_rows<<<grid, kRowThreads, 0, ctx->stream>>>((int)width, (int)height, dedges, (int)n_points,
-                                                               even_odd, ymin, ymax, vec4, out);
-  }
-  cudaEventRecord(ctx->ev[2], ctx->stream);
-  return mask_finish(ctx, npx, dev, mask, out, 1);
+    const uint32_t spans = (width + kSpan - 1) / kSpan;
+    const int vec4 = (width % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
+    const int even_odd = fill_rule == PT_FILL_EVEN_ODD ? 1 : 0;
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    if (n_points > (uint32_t)kRowThreads) {
+      const dim3 grid(spans, std::min<uint32_t>(height, 65535u));
+      k_mask_polygon_chunked<<<grid, kRowThreads, 0, ctx->stream>>>((int)width, (int)height, dedges,
+                                                                    (int)n_points, even_odd, ymin, ymax, vec4, out);
+    } else {
+      // two waves of 4 resident blocks per SM, each block looping over rows of its span
+      const uint32_t rows = std::max<uint32_t>(1u, (uint32_t)(ctx->sms * 8) / spans);
+      const dim3 grid(spans, std::min<uint32_t>(std::min<uint32_t>(height, rows), 65535u));
+      k_mask_polygon_rows<<<grid, kRowThreads, 0, ctx->stream>>>((int)width, (int)height, dedges, (int)n_points,
+                                                                 even_odd, ymin, ymax, vec4, out);
+    }
+    cudaEventRecord(ctx->ev[2], ctx->stream);
+    return mask_finish(ctx, npx, dev, mask, out, 1);
+  });
 }

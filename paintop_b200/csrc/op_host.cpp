@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/paintop_cuda.h"
+#include "abi_guard.h"
 
 namespace pt_op {
 
@@ -534,157 +535,159 @@ extern "C" pt_status pt_op_compute_ex(pt_ctx *ctx, const char *op_id, const pt_p
                                       size_t candidate_count, pt_solver_data *solver,
                                       double *residual_history, uint32_t history_cap,
                                       int32_t *all_finite, pt_error *err, uint32_t solve_flags) {
-  if (err) std::memset(err, 0, sizeof(*err));
-  if (!op_id || (n_inputs && !inputs)) return PT_INVALID_ARG;
-  if (solve_flags & ~PT_FLAG_MULTIGRID) {
-    set_error(err, OpError{"execution", "E_CUDA_SOLVE_FLAGS",
-                           std::string("unsupported solve flags ") + std::to_string(solve_flags), ""});
-    return PT_INVALID_ARG;
-  }
-  if (std::strcmp(op_id, "mask.ellipse@1") == 0 || std::strcmp(op_id, "mask.polygon@1") == 0)
-    return mask_op_compute(ctx, op_id[5] == 'e', inputs, n_inputs, params_json, candidate, candidate_count,
-                           all_finite, err);
-  if (!solver) return PT_INVALID_ARG;
-  const OpSpec *spec = nullptr;
-  if (std::strcmp(op_id, "repair.poisson_blend@1") == 0) spec = &kBlend;
-  else if (std::strcmp(op_id, "repair.screened_poisson@1") == 0) spec = &kScreened;
-  else {
-    set_error(err, OpError{"reference", "E_OP_UNKNOWN", std::string("unknown operation ") + op_id, ""});
-    return PT_INVALID_ARG;
-  }
-  const OpSpec &s = *spec;
-
-  JsonValue params;
-  if (params_json && *params_json) {
-    JsonParser jp(params_json);
-    if (!jp.parse(&params)) {
-      set_error(err, OpError{"parse", s.e_param, std::string(s.op) + ": params are not valid JSON", ""});
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!op_id || (n_inputs && !inputs)) return PT_INVALID_ARG;
+    if (solve_flags & ~PT_FLAG_MULTIGRID) {
+      set_error(err, OpError{"execution", "E_CUDA_SOLVE_FLAGS",
+                             std::string("unsupported solve flags ") + std::to_string(solve_flags), ""});
       return PT_INVALID_ARG;
     }
-  }
-  BlendControls controls;
-  OpError oe;
-  if (!resolve_controls(s, params, &controls, &oe)) { set_error(err, oe); return PT_INVALID_ARG; }
-
-  // input_value (poisson_blend.rs:603-614): a missing port is a Reference error.
-  const pt_port *pa = nullptr, *pb = nullptr, *pm = nullptr;
-  const char *names[3] = {s.in_a, s.in_b, "mask"};
-  const pt_port **slots[3] = {&pa, &pb, &pm};
-  for (int k = 0; k < 3; ++k) {
-    *slots[k] = find_port(inputs, n_inputs, names[k]);
-    if (!*slots[k]) {
-      set_error(err, OpError{"reference", s.e_input,
-                             std::string(s.op) + " requires a `" + names[k] + "` input value", ""});
+    if (std::strcmp(op_id, "mask.ellipse@1") == 0 || std::strcmp(op_id, "mask.polygon@1") == 0)
+      return mask_op_compute(ctx, op_id[5] == 'e', inputs, n_inputs, params_json, candidate, candidate_count,
+                             all_finite, err);
+    if (!solver) return PT_INVALID_ARG;
+    const OpSpec *spec = nullptr;
+    if (std::strcmp(op_id, "repair.poisson_blend@1") == 0) spec = &kBlend;
+    else if (std::strcmp(op_id, "repair.screened_poisson@1") == 0) spec = &kScreened;
+    else {
+      set_error(err, OpError{"reference", "E_OP_UNKNOWN", std::string("unknown operation ") + op_id, ""});
       return PT_INVALID_ARG;
     }
-  }
-  // descriptor kinds (poisson_blend.rs:545-553): the wrong kind is a Type error.
-  const struct { const pt_port *p; const char *name; uint32_t kind; const char *word; } kinds[3] = {
-      {pa, s.in_a, PT_KIND_IMAGE, "image"}, {pb, s.in_b, PT_KIND_IMAGE, "image"},
-      {pm, "mask", PT_KIND_MASK, "mask"}};
-  for (const auto &k : kinds) {
-    if (k.p->kind != k.kind) {
-      set_error(err, OpError{"type", s.e_input,
-                             std::string(s.op) + " `" + k.name + "` input must be a " + k.word + " resource",
+    const OpSpec &s = *spec;
+
+    JsonValue params;
+    if (params_json && *params_json) {
+      JsonParser jp(params_json);
+      if (!jp.parse(&params)) {
+        set_error(err, OpError{"parse", s.e_param, std::string(s.op) + ": params are not valid JSON", ""});
+        return PT_INVALID_ARG;
+      }
+    }
+    BlendControls controls;
+    OpError oe;
+    if (!resolve_controls(s, params, &controls, &oe)) { set_error(err, oe); return PT_INVALID_ARG; }
+
+    // input_value (poisson_blend.rs:603-614): a missing port is a Reference error.
+    const pt_port *pa = nullptr, *pb = nullptr, *pm = nullptr;
+    const char *names[3] = {s.in_a, s.in_b, "mask"};
+    const pt_port **slots[3] = {&pa, &pb, &pm};
+    for (int k = 0; k < 3; ++k) {
+      *slots[k] = find_port(inputs, n_inputs, names[k]);
+      if (!*slots[k]) {
+        set_error(err, OpError{"reference", s.e_input,
+                               std::string(s.op) + " requires a `" + names[k] + "` input value", ""});
+        return PT_INVALID_ARG;
+      }
+    }
+    // descriptor kinds (poisson_blend.rs:545-553): the wrong kind is a Type error.
+    const struct { const pt_port *p; const char *name; uint32_t kind; const char *word; } kinds[3] = {
+        {pa, s.in_a, PT_KIND_IMAGE, "image"}, {pb, s.in_b, PT_KIND_IMAGE, "image"},
+        {pm, "mask", PT_KIND_MASK, "mask"}};
+    for (const auto &k : kinds) {
+      if (k.p->kind != k.kind) {
+        set_error(err, OpError{"type", s.e_input,
+                               std::string(s.op) + " `" + k.name + "` input must be a " + k.word + " resource",
+                               ""});
+        return PT_INVALID_ARG;
+      }
+      const uint32_t ch = k.kind == PT_KIND_MASK ? 1u : k.p->channels;
+      const size_t want = (size_t)k.p->width * k.p->height * ch;
+      if (k.p->sample_count != want || (want && !k.p->samples)) {
+        // a ResourceValue whose buffer disagrees with its descriptor cannot be
+        // built in the reference (value.rs:50-69)
+        set_error(err, OpError{"type", s.e_input,
+                               std::string(s.op) + " `" + k.name +
+                                   "` input buffer length does not match its descriptor",
+                               std::to_string(k.p->sample_count)});
+        return PT_INVALID_ARG;
+      }
+    }
+    // check_shapes (poisson_blend.rs:417-445); shape errors use E_POISSON_BLEND_SHAPE
+    // for both ops since the screened op reuses the blend's check.
+    auto shape = [&](const char *detail, const std::string &actual) {
+      set_error(err, OpError{"semantic", "E_POISSON_BLEND_SHAPE", std::string(s.op) + ": " + detail, actual});
+      return PT_INVALID_ARG;
+    };
+    char buf[96];
+    if (pa->width != pb->width || pa->height != pb->height) {
+      std::snprintf(buf, sizeof buf, "%s %ux%u vs %s %ux%u", s.in_a, pa->width, pa->height, s.in_b, pb->width,
+                    pb->height);
+      return shape("the source and target images must share an extent", buf);
+    }
+    if (pa->channels != pb->channels) {
+      std::snprintf(buf, sizeof buf, "%s %u channels vs %s %u channels", s.in_a, pa->channels, s.in_b,
+                    pb->channels);
+      return shape("the source and target images must share a channel layout", buf);
+    }
+    if (pm->width != pb->width || pm->height != pb->height) {
+      std::snprintf(buf, sizeof buf, "mask %ux%u vs image %ux%u", pm->width, pm->height, pb->width, pb->height);
+      return shape("the mask must share the images' extent", buf);
+    }
+    const size_t count = (size_t)pb->width * pb->height * pb->channels;
+    if (!candidate || candidate_count != count) {
+      set_error(err, OpError{"execution", s.e_buffer,
+                             std::string(s.op) + " produced a candidate buffer of unexpected length " +
+                                 std::to_string(candidate_count),
                              ""});
       return PT_INVALID_ARG;
     }
-    const uint32_t ch = k.kind == PT_KIND_MASK ? 1u : k.p->channels;
-    const size_t want = (size_t)k.p->width * k.p->height * ch;
-    if (k.p->sample_count != want || (want && !k.p->samples)) {
-      // a ResourceValue whose buffer disagrees with its descriptor cannot be
-      // built in the reference (value.rs:50-69)
-      set_error(err, OpError{"type", s.e_input,
-                             std::string(s.op) + " `" + k.name +
-                                 "` input buffer length does not match its descriptor",
-                             std::to_string(k.p->sample_count)});
-      return PT_INVALID_ARG;
-    }
-  }
-  // check_shapes (poisson_blend.rs:417-445); shape errors use E_POISSON_BLEND_SHAPE
-  // for both ops since the screened op reuses the blend's check.
-  auto shape = [&](const char *detail, const std::string &actual) {
-    set_error(err, OpError{"semantic", "E_POISSON_BLEND_SHAPE", std::string(s.op) + ": " + detail, actual});
-    return PT_INVALID_ARG;
-  };
-  char buf[96];
-  if (pa->width != pb->width || pa->height != pb->height) {
-    std::snprintf(buf, sizeof buf, "%s %ux%u vs %s %ux%u", s.in_a, pa->width, pa->height, s.in_b, pb->width,
-                  pb->height);
-    return shape("the source and target images must share an extent", buf);
-  }
-  if (pa->channels != pb->channels) {
-    std::snprintf(buf, sizeof buf, "%s %u channels vs %s %u channels", s.in_a, pa->channels, s.in_b,
-                  pb->channels);
-    return shape("the source and target images must share a channel layout", buf);
-  }
-  if (pm->width != pb->width || pm->height != pb->height) {
-    std::snprintf(buf, sizeof buf, "mask %ux%u vs image %ux%u", pm->width, pm->height, pb->width, pb->height);
-    return shape("the mask must share the images' extent", buf);
-  }
-  const size_t count = (size_t)pb->width * pb->height * pb->channels;
-  if (!candidate || candidate_count != count) {
-    set_error(err, OpError{"execution", s.e_buffer,
-                           std::string(s.op) + " produced a candidate buffer of unexpected length " +
-                               std::to_string(candidate_count),
-                           ""});
-    return PT_INVALID_ARG;
-  }
 
-  pt_problem p{};
-  p.width = pb->width;
-  p.height = pb->height;
-  p.channels = pb->channels;
-  p.source_or_guidance = pa->samples;
-  p.target_or_anchor = pb->samples;
-  p.mask = pm->samples;
-  p.lambda = controls.lambda;
-  p.max_iterations = controls.max_iterations;
-  p.tolerance = controls.tolerance;
-  p.omega = OMEGA;
-  p.flags = solve_flags;
-  if (!ctx) {
-    // validation passed but there is no device context: the backend is
-    // unavailable (the E_GPU_UNAVAILABLE analogue, a Policy error)
-    set_error(err, OpError{"policy", "E_CUDA_UNAVAILABLE",
-                           std::string(s.op) + ": the cuda backend has no device context", ""});
-    return PT_NO_DEVICE;
-  }
-  std::vector<pt_report> reps(p.channels + 1);
-  std::vector<double> hist((size_t)p.channels * p.max_iterations);
-  const pt_status st = pt_poisson_solve(ctx, &p, candidate, reps.data(), hist.empty() ? nullptr : hist.data());
-  if (st != PT_OK) {
-    set_error(err, OpError{st == PT_NO_DEVICE ? "policy" : "execution",
-                           st == PT_NO_DEVICE ? "E_CUDA_UNAVAILABLE" : "E_CUDA_EXECUTION",
-                           std::string(s.op) + ": " + pt_status_str(st) + ": " + pt_ctx_last_error(ctx), ""});
-    return st;
-  }
-  const pt_report &w = reps[p.channels];  // worst channel (blend_channels' report)
-  std::memset(solver, 0, sizeof(*solver));
-  std::snprintf(solver->kind, sizeof(solver->kind), "%s", s.kind);
-  // solver_data (poisson_blend.rs:249-266)
-  solver->steps = w.iterations;
-  solver->stability_number = 0.0;
-  solver->stability_limit = 0.0;
-  solver->stable = 1;
-  solver->total_energy = 0.0;
-  solver->iterations = w.iterations;
-  solver->stop_reason = w.stop_reason;
-  solver->converged = w.converged;
-  solver->tolerance = w.tolerance;
-  solver->final_residual = w.final_residual;
-  solver->history_len = w.history_len;
-  if (residual_history && w.channel >= 0) {
-    const uint32_t m = w.history_len < history_cap ? w.history_len : history_cap;
-    std::memcpy(residual_history, hist.data() + (size_t)w.channel * p.max_iterations, m * sizeof(double));
-  }
-  if (all_finite) {
-    int32_t f = 1;
-    for (size_t k = 0; k < count; ++k)
-      if (!std::isfinite(candidate[k])) { f = 0; break; }
-    *all_finite = f;
-  }
-  return PT_OK;
+    pt_problem p{};
+    p.width = pb->width;
+    p.height = pb->height;
+    p.channels = pb->channels;
+    p.source_or_guidance = pa->samples;
+    p.target_or_anchor = pb->samples;
+    p.mask = pm->samples;
+    p.lambda = controls.lambda;
+    p.max_iterations = controls.max_iterations;
+    p.tolerance = controls.tolerance;
+    p.omega = OMEGA;
+    p.flags = solve_flags;
+    if (!ctx) {
+      // validation passed but there is no device context: the backend is
+      // unavailable (the E_GPU_UNAVAILABLE analogue, a Policy error)
+      set_error(err, OpError{"policy", "E_CUDA_UNAVAILABLE",
+                             std::string(s.op) + ": the cuda backend has no device context", ""});
+      return PT_NO_DEVICE;
+    }
+    std::vector<pt_report> reps(p.channels + 1);
+    std::vector<double> hist((size_t)p.channels * p.max_iterations);
+    const pt_status st = pt_poisson_solve(ctx, &p, candidate, reps.data(), hist.empty() ? nullptr : hist.data());
+    if (st != PT_OK) {
+      set_error(err, OpError{st == PT_NO_DEVICE ? "policy" : "execution",
+                             st == PT_NO_DEVICE ? "E_CUDA_UNAVAILABLE" : "E_CUDA_EXECUTION",
+                             std::string(s.op) + ": " + pt_status_str(st) + ": " + pt_ctx_last_error(ctx), ""});
+      return st;
+    }
+    const pt_report &w = reps[p.channels];  // worst channel (blend_channels' report)
+    std::memset(solver, 0, sizeof(*solver));
+    std::snprintf(solver->kind, sizeof(solver->kind), "%s", s.kind);
+    // solver_data (poisson_blend.rs:249-266)
+    solver->steps = w.iterations;
+    solver->stability_number = 0.0;
+    solver->stability_limit = 0.0;
+    solver->stable = 1;
+    solver->total_energy = 0.0;
+    solver->iterations = w.iterations;
+    solver->stop_reason = w.stop_reason;
+    solver->converged = w.converged;
+    solver->tolerance = w.tolerance;
+    solver->final_residual = w.final_residual;
+    solver->history_len = w.history_len;
+    if (residual_history && w.channel >= 0) {
+      const uint32_t m = w.history_len < history_cap ? w.history_len : history_cap;
+      std::memcpy(residual_history, hist.data() + (size_t)w.channel * p.max_iterations, m * sizeof(double));
+    }
+    if (all_finite) {
+      int32_t f = 1;
+      for (size_t k = 0; k < count; ++k)
+        if (!std::isfinite(candidate[k])) { f = 0; break; }
+      *all_finite = f;
+    }
+    return PT_OK;
+  });
 }
 
 extern "C" pt_status pt_op_compute(pt_ctx *ctx, const char *op_id, const pt_port *inputs,

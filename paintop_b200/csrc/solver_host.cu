@@ -9,16 +9,18 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <new>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "../../include/paintop_cuda.h"
+#include "abi_guard.h"
 #include "ctx.h"
 #include "rbsor_launch.h"
 
@@ -166,6 +168,7 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
   if (fault == 1) return fail(ctx, PT_NO_DEVICE, "injected: no device");
   if (fault == 2) return fail(ctx, PT_OOM, "injected: allocation failure");
   if (fault == 3) return fail(ctx, PT_LAUNCH_FAILED, "injected: launch failure");
+  abi_test_fault();
 
   const bool mg = n > 0 && (ps[0].flags & PT_FLAG_MULTIGRID);
   for (uint32_t i = 0; i < n; ++i)
@@ -437,7 +440,14 @@ pt_status ptk_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *
     } else {
       const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
       const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, bytes >> 22));
-      for (unsigned k = 0; k < nt; ++k) fill_job.pool.emplace_back(fill, total * k / nt, total * (k + 1) / nt);
+      // a stretch whose thread cannot be started is copied here instead
+      for (unsigned k = 0; k < nt; ++k) {
+        try {
+          fill_job.pool.emplace_back(fill, total * k / nt, total * (k + 1) / nt);
+        } catch (const std::system_error &) {
+          fill(total * k / nt, total * (k + 1) / nt);
+        }
+      }
     }
   }
 
@@ -641,30 +651,36 @@ pt_status pt_ctx_create(int device, pt_ctx **out) {
 }
 
 pt_status pt_ctx_destroy(pt_ctx *ctx) {
-  if (!ctx) return PT_OK;
-  {
-    std::lock_guard<std::mutex> lock(ctx->mu);
-    cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    ctx->release();
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  }
-  delete ctx;
-  return PT_OK;
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx) return PT_OK;
+    {
+      std::lock_guard<std::mutex> lock(ctx->mu);
+      cudaSetDevice(ctx->device);
+      if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+      ctx->release();
+      if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return PT_OK;
+  });
 }
 
 pt_status pt_poisson_solve(pt_ctx *ctx, const pt_problem *p, float *out_candidate, pt_report *reports,
                            double *history) {
-  if (!ctx || !p || !reports) return PT_INVALID_ARG;
-  float *outs[1] = {out_candidate};
-  pt_report *reps[1] = {reports};
-  double *hists[1] = {history};
-  return ptk_solve_batch(ctx, p, 1, outs, reps, hists, -1);
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx || !p || !reports) return PT_INVALID_ARG;
+    float *outs[1] = {out_candidate};
+    pt_report *reps[1] = {reports};
+    double *hists[1] = {history};
+    return ptk_solve_batch(ctx, p, 1, outs, reps, hists, -1);
+  });
 }
 
 pt_status pt_poisson_solve_batch(pt_ctx *ctx, const pt_problem *ps, uint32_t n, float *const *outs,
                                  pt_report *const *reports, double *const *histories) {
-  return ptk_solve_batch(ctx, ps, n, outs, reports, histories, -1);
+  return abi_guard(ctx, [&]() -> pt_status {
+    return ptk_solve_batch(ctx, ps, n, outs, reports, histories, -1);
+  });
 }
 
 const char *pt_status_str(pt_status s) {
@@ -701,10 +717,12 @@ pt_status pt_ctx_last_transfer(const pt_ctx *ctx, uint64_t *h2d_bytes, uint64_t 
 }
 
 pt_status pt_ctx_set_budget(pt_ctx *ctx, double seconds) {
-  if (!ctx || !(seconds > 0.0) || !std::isfinite(seconds)) return PT_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  ctx->budget_s = seconds;
-  return PT_OK;
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx || !(seconds > 0.0) || !std::isfinite(seconds)) return PT_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->budget_s = seconds;
+    return PT_OK;
+  });
 }
 
 }  // extern "C"

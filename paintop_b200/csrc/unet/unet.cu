@@ -27,6 +27,7 @@
 #include "../../../include/paintop_cuda.h"
 #include "../ctx.h"
 #include "unet_kernels.h"
+#include "../abi_guard.h"
 
 using namespace unet;
 
@@ -339,256 +340,282 @@ pt_status check_shape(uint32_t B, uint32_t H, uint32_t W) {
 extern "C" {
 
 pt_status pt_unet_create(pt_ctx *ctx, uint64_t seed, pt_unet **out) {
-  if (!ctx || !out) return PT_INVALID_ARG;
-  *out = nullptr;
-  pt_unet *n = new (std::nothrow) pt_unet();
-  if (!n) return PT_OOM;
-  n->ctx = ctx;
-  size_t off = 0, boff = 0;
-  for (int l = 0; l < 14; ++l) {
-    n->w_off[l] = off;
-    off += (size_t)kLayers[l].cout * 9 * kLayers[l].cin;
-    n->b_off[l] = off;
-    off += kLayers[l].cout;
-    n->wb_off[l] = boff;
-    boff += (size_t)kLayers[l].cout * 9 * kLayers[l].cin;
-    n->wt_off[l] = boff;
-    boff += (size_t)kLayers[l].cout * 9 * kLayers[l].cin;
-  }
-  n->head_w = off;
-  off += kHeadIn;
-  n->head_b = off;
-  off += 1;
-  n->nparam = off;
-  // He-normal initialisation (std sqrt(2 / fan_in)) from a seeded SplitMix64;
-  // biases zero; padded input channels of layer 0 zero.
-  std::vector<float> h(off, 0.0f);
-  uint64_t s = seed ^ 0x5eed5eed5eedull;
-  for (int l = 0; l < 14; ++l) {
-    const int ci_real = l == 0 ? kInReal : kLayers[l].cin;
-    const double sd = std::sqrt(2.0 / (9.0 * ci_real));
-    for (int co = 0; co < kLayers[l].cout; ++co)
-      for (int t = 0; t < 9; ++t)
-        for (int ci = 0; ci < kLayers[l].cin; ++ci)
-          h[n->w_off[l] + ((size_t)co * 9 + t) * kLayers[l].cin + ci] = ci < ci_real ? (float)(sd * normal(s)) : 0.0f;
-  }
-  for (int k = 0; k < kHeadIn; ++k) h[n->head_w + k] = (float)(std::sqrt(1.0 / kHeadIn) * normal(s));
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  cudaSetDevice(ctx->device);
-  bool okm = cudaMalloc(&n->params, off * 4) == cudaSuccess && cudaMalloc(&n->m, off * 4) == cudaSuccess &&
-             cudaMalloc(&n->v, off * 4) == cudaSuccess && cudaMalloc(&n->grad, off * 4) == cudaSuccess &&
-             cudaMalloc(&n->wbf, boff * 2) == cudaSuccess;
-  if (!okm) {
-    cudaGetLastError();
-    cudaFree(n->params); cudaFree(n->m); cudaFree(n->v); cudaFree(n->grad); cudaFree(n->wbf);
-    delete n;
-    return PT_OOM;
-  }
-  cudaMemcpy(n->params, h.data(), off * 4, cudaMemcpyHostToDevice);
-  cudaMemset(n->m, 0, off * 4);
-  cudaMemset(n->v, 0, off * 4);
-  cudaMemset(n->grad, 0, off * 4);
-  if (refresh_weights(n) != PT_OK || cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
-    pt_unet_destroy(n);
-    return PT_LAUNCH_FAILED;
-  }
-  *out = n;
-  return PT_OK;
+  return abi_guard(ctx, [&]() -> pt_status {
+    if (!ctx || !out) return PT_INVALID_ARG;
+    *out = nullptr;
+    pt_unet *n = new (std::nothrow) pt_unet();
+    if (!n) return PT_OOM;
+    n->ctx = ctx;
+    size_t off = 0, boff = 0;
+    for (int l = 0; l < 14; ++l) {
+      n->w_off[l] = off;
+      off += (size_t)kLayers[l].cout * 9 * kLayers[l].cin;
+      n->b_off[l] = off;
+      off += kLayers[l].cout;
+      n->wb_off[l] = boff;
+      boff += (size_t)kLayers[l].cout * 9 * kLayers[l].cin;
+      n->wt_off[l] = boff;
+      boff += (size_t)kLayers[l].cout * 9 * kLayers[l].cin;
+    }
+    n->head_w = off;
+    off += kHeadIn;
+    n->head_b = off;
+    off += 1;
+    n->nparam = off;
+    // He-normal initialisation (std sqrt(2 / fan_in)) from a seeded SplitMix64;
+    // biases zero; padded input channels of layer 0 zero.
+    std::vector<float> h(off, 0.0f);
+    uint64_t s = seed ^ 0x5eed5eed5eedull;
+    for (int l = 0; l < 14; ++l) {
+      const int ci_real = l == 0 ? kInReal : kLayers[l].cin;
+      const double sd = std::sqrt(2.0 / (9.0 * ci_real));
+      for (int co = 0; co < kLayers[l].cout; ++co)
+        for (int t = 0; t < 9; ++t)
+          for (int ci = 0; ci < kLayers[l].cin; ++ci)
+            h[n->w_off[l] + ((size_t)co * 9 + t) * kLayers[l].cin + ci] = ci < ci_real ? (float)(sd * normal(s)) : 0.0f;
+    }
+    for (int k = 0; k < kHeadIn; ++k) h[n->head_w + k] = (float)(std::sqrt(1.0 / kHeadIn) * normal(s));
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    bool okm = cudaMalloc(&n->params, off * 4) == cudaSuccess && cudaMalloc(&n->m, off * 4) == cudaSuccess &&
+               cudaMalloc(&n->v, off * 4) == cudaSuccess && cudaMalloc(&n->grad, off * 4) == cudaSuccess &&
+               cudaMalloc(&n->wbf, boff * 2) == cudaSuccess;
+    if (!okm) {
+      cudaGetLastError();
+      cudaFree(n->params); cudaFree(n->m); cudaFree(n->v); cudaFree(n->grad); cudaFree(n->wbf);
+      delete n;
+      return PT_OOM;
+    }
+    cudaMemcpy(n->params, h.data(), off * 4, cudaMemcpyHostToDevice);
+    cudaMemset(n->m, 0, off * 4);
+    cudaMemset(n->v, 0, off * 4);
+    cudaMemset(n->grad, 0, off * 4);
+    if (refresh_weights(n) != PT_OK || cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      pt_unet_destroy(n);
+      return PT_LAUNCH_FAILED;
+    }
+    *out = n;
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_destroy(pt_unet *n) {
-  if (!n) return PT_OK;
-  if (n->ctx) {
-    std::lock_guard<std::mutex> lock(n->ctx->mu);
-    cudaSetDevice(n->ctx->device);
-    cudaStreamSynchronize(n->ctx->stream);
-    cudaFree(n->params); cudaFree(n->m); cudaFree(n->v); cudaFree(n->grad); cudaFree(n->wbf);
-    cudaFree(n->act_mem);
-    cudaFree(n->gmem);
-  }
-  delete n;
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n) return PT_OK;
+    if (n->ctx) {
+      std::lock_guard<std::mutex> lock(n->ctx->mu);
+      cudaSetDevice(n->ctx->device);
+      cudaStreamSynchronize(n->ctx->stream);
+      cudaFree(n->params); cudaFree(n->m); cudaFree(n->v); cudaFree(n->grad); cudaFree(n->wbf);
+      cudaFree(n->act_mem);
+      cudaFree(n->gmem);
+    }
+    delete n;
+    return PT_OK;
+  });
 }
 
 uint64_t pt_unet_param_count(const pt_unet *n) { return n ? n->nparam : 0; }
 
 pt_status pt_unet_get_params(pt_unet *n, float *host) {
-  if (!n || !host) return PT_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  CK(cudaMemcpy(host, n->params, n->nparam * 4, cudaMemcpyDeviceToHost), "get params");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !host) return PT_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    CK(cudaMemcpy(host, n->params, n->nparam * 4, cudaMemcpyDeviceToHost), "get params");
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_set_params(pt_unet *n, const float *host) {
-  if (!n || !host) return PT_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  CK(cudaMemcpy(n->params, host, n->nparam * 4, cudaMemcpyHostToDevice), "set params");
-  RET(refresh_weights(n));
-  CK(cudaStreamSynchronize(n->ctx->stream), "sync");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !host) return PT_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    CK(cudaMemcpy(n->params, host, n->nparam * 4, cudaMemcpyHostToDevice), "set params");
+    RET(refresh_weights(n));
+    CK(cudaStreamSynchronize(n->ctx->stream), "sync");
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_features(pt_unet *n, const float *guidance, const float *anchor, const float *mask,
                            uint32_t batch, uint32_t h, uint32_t w, float *features) {
-  if (!n || !guidance || !anchor || !mask || !features || !batch || !h || !w) return PT_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  CK(launch_features(guidance, anchor, mask, (int)batch, (int)h, (int)w, features, n->ctx->stream), "features");
-  CK(cudaStreamSynchronize(n->ctx->stream), "sync");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !guidance || !anchor || !mask || !features || !batch || !h || !w) return PT_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    CK(launch_features(guidance, anchor, mask, (int)batch, (int)h, (int)w, features, n->ctx->stream), "features");
+    CK(cudaStreamSynchronize(n->ctx->stream), "sync");
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_forward(pt_unet *n, const float *features, uint32_t batch, uint32_t h, uint32_t w, float *pred) {
-  if (!n || !features || !pred) return PT_INVALID_ARG;
-  RET(check_shape(batch, h, w));
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  cudaSetDevice(n->ctx->device);
-  RET(ensure_acts(n, (int)batch, (int)h, (int)w));
-  RET(forward(n, features));
-  const long long P0 = npix(n, 0);
-  CK(cudaMemcpyAsync(pred, n->pred, P0 * 4, cudaMemcpyDeviceToDevice, n->ctx->stream), "pred copy");
-  int kerr = 0;
-  CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, n->ctx->stream), "err copy");
-  CK(cudaStreamSynchronize(n->ctx->stream), "sync");
-  if (kerr) {
-    n->ctx->last_error = "a tensor-core pipeline wait gave up";
-    return PT_TIMEOUT;
-  }
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !features || !pred) return PT_INVALID_ARG;
+    RET(check_shape(batch, h, w));
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    cudaSetDevice(n->ctx->device);
+    RET(ensure_acts(n, (int)batch, (int)h, (int)w));
+    RET(forward(n, features));
+    const long long P0 = npix(n, 0);
+    CK(cudaMemcpyAsync(pred, n->pred, P0 * 4, cudaMemcpyDeviceToDevice, n->ctx->stream), "pred copy");
+    int kerr = 0;
+    CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, n->ctx->stream), "err copy");
+    CK(cudaStreamSynchronize(n->ctx->stream), "sync");
+    if (kerr) {
+      n->ctx->last_error = "a tensor-core pipeline wait gave up";
+      return PT_TIMEOUT;
+    }
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_loss_grad(pt_unet *n, const float *features, const float *target, const float *loss_mask,
                             uint32_t batch, uint32_t h, uint32_t w, double *loss, float *grad_host) {
-  if (!n || !features || !target || !loss_mask) return PT_INVALID_ARG;
-  RET(check_shape(batch, h, w));
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  cudaSetDevice(n->ctx->device);
-  RET(ensure_acts(n, (int)batch, (int)h, (int)w));
-  RET(forward(n, features));
-  RET(backward(n, target, loss_mask, loss));
-  if (grad_host) CK(cudaMemcpy(grad_host, n->grad, n->nparam * 4, cudaMemcpyDeviceToHost), "grad copy");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !features || !target || !loss_mask) return PT_INVALID_ARG;
+    RET(check_shape(batch, h, w));
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    cudaSetDevice(n->ctx->device);
+    RET(ensure_acts(n, (int)batch, (int)h, (int)w));
+    RET(forward(n, features));
+    RET(backward(n, target, loss_mask, loss));
+    if (grad_host) CK(cudaMemcpy(grad_host, n->grad, n->nparam * 4, cudaMemcpyDeviceToHost), "grad copy");
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_train_step(pt_unet *n, const float *features, const float *target, const float *loss_mask,
                              uint32_t batch, uint32_t h, uint32_t w, float lr, double *loss) {
-  if (!n || !features || !target || !loss_mask || !(lr > 0.0f)) return PT_INVALID_ARG;
-  RET(check_shape(batch, h, w));
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  cudaSetDevice(n->ctx->device);
-  RET(ensure_acts(n, (int)batch, (int)h, (int)w));
-  RET(forward(n, features));
-  RET(backward(n, target, loss_mask, loss));
-  n->step += 1;
-  CK(launch_adam(n->params, n->m, n->v, n->grad, nullptr, (long long)n->nparam, lr, n->step, n->ctx->stream),
-     "adam");
-  RET(refresh_weights(n));
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !features || !target || !loss_mask || !(lr > 0.0f)) return PT_INVALID_ARG;
+    RET(check_shape(batch, h, w));
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    cudaSetDevice(n->ctx->device);
+    RET(ensure_acts(n, (int)batch, (int)h, (int)w));
+    RET(forward(n, features));
+    RET(backward(n, target, loss_mask, loss));
+    n->step += 1;
+    CK(launch_adam(n->params, n->m, n->v, n->grad, nullptr, (long long)n->nparam, lr, n->step, n->ctx->stream),
+       "adam");
+    RET(refresh_weights(n));
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_grad_record(pt_unet *n, const float *features, const float *target, const float *loss_mask,
                               uint32_t batch, uint32_t h, uint32_t w, double *loss, float *record) {
-  if (!n || !features || !target || !loss_mask || !record) return PT_INVALID_ARG;
-  RET(check_shape(batch, h, w));
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  cudaSetDevice(n->ctx->device);
-  RET(ensure_acts(n, (int)batch, (int)h, (int)w));
-  RET(forward(n, features));
-  RET(backward(n, target, loss_mask, loss));
-  cudaStream_t st = n->ctx->stream;
-  CK(cudaMemcpyAsync(record, n->grad, n->nparam * 4, cudaMemcpyDeviceToDevice, st), "record copy");
-  CK(cudaMemcpyAsync(record + n->nparam, n->count, 4, cudaMemcpyDeviceToDevice, st), "count copy");
-  CK(cudaStreamSynchronize(st), "sync");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !features || !target || !loss_mask || !record) return PT_INVALID_ARG;
+    RET(check_shape(batch, h, w));
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    cudaSetDevice(n->ctx->device);
+    RET(ensure_acts(n, (int)batch, (int)h, (int)w));
+    RET(forward(n, features));
+    RET(backward(n, target, loss_mask, loss));
+    cudaStream_t st = n->ctx->stream;
+    CK(cudaMemcpyAsync(record, n->grad, n->nparam * 4, cudaMemcpyDeviceToDevice, st), "record copy");
+    CK(cudaMemcpyAsync(record + n->nparam, n->count, 4, cudaMemcpyDeviceToDevice, st), "count copy");
+    CK(cudaStreamSynchronize(st), "sync");
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_apply_records(pt_unet *n, const float *records, uint32_t replicas, float lr) {
-  if (!n || !records || replicas == 0 || !(lr > 0.0f)) return PT_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  cudaSetDevice(n->ctx->device);
-  n->step += 1;
-  CK(launch_adam_records(n->params, n->m, n->v, records, (int)replicas, (long long)n->nparam, lr, n->step,
-                         n->ctx->stream),
-     "adam");
-  RET(refresh_weights(n));
-  CK(cudaStreamSynchronize(n->ctx->stream), "sync");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !records || replicas == 0 || !(lr > 0.0f)) return PT_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    cudaSetDevice(n->ctx->device);
+    n->step += 1;
+    CK(launch_adam_records(n->params, n->m, n->v, records, (int)replicas, (long long)n->nparam, lr, n->step,
+                           n->ctx->stream),
+       "adam");
+    RET(refresh_weights(n));
+    CK(cudaStreamSynchronize(n->ctx->stream), "sync");
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_guess(pt_unet *n, const float *guidance, const float *anchor, const float *mask,
                         uint32_t width, uint32_t height, uint32_t channels, uint32_t scale, float *guess) {
-  if (!n || !guidance || !anchor || !mask || !guess || !width || !height || !channels || !scale)
-    return PT_INVALID_ARG;
-  if (scale > 64 || channels > 64) return PT_INVALID_ARG;
-  const int W = (int)width, H = (int)height, C = (int)channels, s = (int)scale;
-  const int hv = (H + s - 1) / s, wv = (W + s - 1) / s;
-  const int Hc = (std::max(hv, 8) + 7) / 8 * 8, Wc = (std::max(wv, 8) + 7) / 8 * 8;
-  RET(check_shape((uint32_t)C, (uint32_t)Hc, (uint32_t)Wc));
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  cudaSetDevice(n->ctx->device);
-  const size_t cells = (size_t)C * Hc * Wc, need = cells * 7 * sizeof(float);
-  if (need > n->gmem_bytes) {
-    cudaFree(n->gmem);
-    n->gmem = nullptr;
-    n->gmem_bytes = 0;
-    if (cudaMalloc(&n->gmem, need) != cudaSuccess) {
-      cudaGetLastError();
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !guidance || !anchor || !mask || !guess || !width || !height || !channels || !scale)
+      return PT_INVALID_ARG;
+    if (scale > 64 || channels > 64) return PT_INVALID_ARG;
+    const int W = (int)width, H = (int)height, C = (int)channels, s = (int)scale;
+    const int hv = (H + s - 1) / s, wv = (W + s - 1) / s;
+    const int Hc = (std::max(hv, 8) + 7) / 8 * 8, Wc = (std::max(wv, 8) + 7) / 8 * 8;
+    RET(check_shape((uint32_t)C, (uint32_t)Hc, (uint32_t)Wc));
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    cudaSetDevice(n->ctx->device);
+    const size_t cells = (size_t)C * Hc * Wc, need = cells * 7 * sizeof(float);
+    if (need > n->gmem_bytes) {
+      cudaFree(n->gmem);
       n->gmem = nullptr;
-      return PT_OOM;
+      n->gmem_bytes = 0;
+      if (cudaMalloc(&n->gmem, need) != cudaSuccess) {
+        cudaGetLastError();
+        n->gmem = nullptr;
+        return PT_OOM;
+      }
+      n->gmem_bytes = need;
     }
-    n->gmem_bytes = need;
-  }
-  float *cg = n->gmem, *ca = cg + cells, *cm = ca + cells, *feat = cm + cells;
-  cudaStream_t st = n->ctx->stream;
-  CK(launch_pool_inputs(guidance, anchor, mask, W, H, C, s, Wc, Hc, cg, ca, cm, st), "pool inputs");
-  CK(launch_features(cg, ca, cm, C, Hc, Wc, feat, st), "features");
-  RET(ensure_acts(n, C, Hc, Wc));
-  RET(forward(n, feat));
-  CK(launch_compose_guess(guidance, n->pred, W, H, C, s, Wc, Hc, guess, st), "compose guess");
-  int kerr = 0;
-  CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, st), "err copy");
-  CK(cudaStreamSynchronize(st), "sync");
-  if (kerr) {
-    n->ctx->last_error = "a tensor-core pipeline wait gave up";
-    return PT_TIMEOUT;
-  }
-  return PT_OK;
+    float *cg = n->gmem, *ca = cg + cells, *cm = ca + cells, *feat = cm + cells;
+    cudaStream_t st = n->ctx->stream;
+    CK(launch_pool_inputs(guidance, anchor, mask, W, H, C, s, Wc, Hc, cg, ca, cm, st), "pool inputs");
+    CK(launch_features(cg, ca, cm, C, Hc, Wc, feat, st), "features");
+    RET(ensure_acts(n, C, Hc, Wc));
+    RET(forward(n, feat));
+    CK(launch_compose_guess(guidance, n->pred, W, H, C, s, Wc, Hc, guess, st), "compose guess");
+    int kerr = 0;
+    CK(cudaMemcpyAsync(&kerr, n->err, sizeof(int), cudaMemcpyDeviceToHost, st), "err copy");
+    CK(cudaStreamSynchronize(st), "sync");
+    if (kerr) {
+      n->ctx->last_error = "a tensor-core pipeline wait gave up";
+      return PT_TIMEOUT;
+    }
+    return PT_OK;
+  });
 }
 
 pt_status pt_unet_save(pt_unet *n, const char *path) {
-  if (!n || !path) return PT_INVALID_ARG;
-  std::vector<float> h(n->nparam * 3);
-  {
-    std::lock_guard<std::mutex> lock(n->ctx->mu);
-    CK(cudaMemcpy(h.data(), n->params, n->nparam * 4, cudaMemcpyDeviceToHost), "save");
-    CK(cudaMemcpy(h.data() + n->nparam, n->m, n->nparam * 4, cudaMemcpyDeviceToHost), "save");
-    CK(cudaMemcpy(h.data() + 2 * n->nparam, n->v, n->nparam * 4, cudaMemcpyDeviceToHost), "save");
-  }
-  FILE *f = std::fopen(path, "wb");
-  if (!f) return PT_INVALID_ARG;
-  const uint64_t hdr[3] = {0x70746e6574763031ull, n->nparam, (uint64_t)n->step};
-  const bool ok = std::fwrite(hdr, sizeof(hdr), 1, f) == 1 && std::fwrite(h.data(), 4, h.size(), f) == h.size();
-  std::fclose(f);
-  return ok ? PT_OK : PT_INTERNAL;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !path) return PT_INVALID_ARG;
+    std::vector<float> h(n->nparam * 3);
+    {
+      std::lock_guard<std::mutex> lock(n->ctx->mu);
+      CK(cudaMemcpy(h.data(), n->params, n->nparam * 4, cudaMemcpyDeviceToHost), "save");
+      CK(cudaMemcpy(h.data() + n->nparam, n->m, n->nparam * 4, cudaMemcpyDeviceToHost), "save");
+      CK(cudaMemcpy(h.data() + 2 * n->nparam, n->v, n->nparam * 4, cudaMemcpyDeviceToHost), "save");
+    }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return PT_INVALID_ARG;
+    const uint64_t hdr[3] = {0x70746e6574763031ull, n->nparam, (uint64_t)n->step};
+    const bool ok = std::fwrite(hdr, sizeof(hdr), 1, f) == 1 && std::fwrite(h.data(), 4, h.size(), f) == h.size();
+    std::fclose(f);
+    return ok ? PT_OK : PT_INTERNAL;
+  });
 }
 
 pt_status pt_unet_load(pt_unet *n, const char *path) {
-  if (!n || !path) return PT_INVALID_ARG;
-  FILE *f = std::fopen(path, "rb");
-  if (!f) return PT_INVALID_ARG;
-  uint64_t hdr[3] = {0, 0, 0};
-  std::vector<float> h(n->nparam * 3);
-  const bool ok = std::fread(hdr, sizeof(hdr), 1, f) == 1 && hdr[0] == 0x70746e6574763031ull &&
-                  hdr[1] == n->nparam && std::fread(h.data(), 4, h.size(), f) == h.size();
-  std::fclose(f);
-  if (!ok) return PT_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(n->ctx->mu);
-  CK(cudaMemcpy(n->params, h.data(), n->nparam * 4, cudaMemcpyHostToDevice), "load");
-  CK(cudaMemcpy(n->m, h.data() + n->nparam, n->nparam * 4, cudaMemcpyHostToDevice), "load");
-  CK(cudaMemcpy(n->v, h.data() + 2 * n->nparam, n->nparam * 4, cudaMemcpyHostToDevice), "load");
-  n->step = (int)hdr[2];
-  RET(refresh_weights(n));
-  CK(cudaStreamSynchronize(n->ctx->stream), "sync");
-  return PT_OK;
+  return abi_guard(n ? n->ctx : nullptr, [&]() -> pt_status {
+    if (!n || !path) return PT_INVALID_ARG;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return PT_INVALID_ARG;
+    uint64_t hdr[3] = {0, 0, 0};
+    std::vector<float> h(n->nparam * 3);
+    const bool ok = std::fread(hdr, sizeof(hdr), 1, f) == 1 && hdr[0] == 0x70746e6574763031ull &&
+                    hdr[1] == n->nparam && std::fread(h.data(), 4, h.size(), f) == h.size();
+    std::fclose(f);
+    if (!ok) return PT_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(n->ctx->mu);
+    CK(cudaMemcpy(n->params, h.data(), n->nparam * 4, cudaMemcpyHostToDevice), "load");
+    CK(cudaMemcpy(n->m, h.data() + n->nparam, n->nparam * 4, cudaMemcpyHostToDevice), "load");
+    CK(cudaMemcpy(n->v, h.data() + 2 * n->nparam, n->nparam * 4, cudaMemcpyHostToDevice), "load");
+    n->step = (int)hdr[2];
+    RET(refresh_weights(n));
+    CK(cudaStreamSynchronize(n->ctx->stream), "sync");
+    return PT_OK;
+  });
 }
 
 }  // extern "C"

@@ -2,7 +2,10 @@
 
 * Host-injected failures (PAINTOP_CUDA_FAULT=oom | launch): the solve returns
   PT_OOM / PT_LAUNCH_FAILED before any device work, the op layer maps them to
-  its execution error, and the same context then solves normally. The
+  its execution error, and the same context then solves normally. With
+  host-oom | host-exception a C++ exception is thrown inside the call and the
+  entry point's guard returns PT_OOM / PT_INTERNAL instead of unwinding
+  through the C ABI. The
   reference's analogue is the typed GPU-unavailable error
   (crates/paintop-wgpu/src/gpu/error.rs:17, probe.rs:223).
 * A bounded device wait that runs out (PAINTOP_CUDA_FAULT=unet-stall): the
@@ -55,6 +58,25 @@ def test_injected_host_failure_returns_its_status_and_the_context_survives(ctx, 
             ctx.solve(src, tgt, mask, W, H, Ch, lam=0.01)
     assert e.value.status == getattr(_lib, status)
     assert "injected" in ctx.last_error()
+    got, per2, _ = ctx.solve(src, tgt, mask, W, H, Ch, lam=0.01)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert [r["iterations"] for r in per2] == [r["iterations"] for r in per]
+
+
+@pytest.mark.parametrize("fault,status,msg", [("host-oom", "PT_OOM", "host memory allocation failed"),
+                                              ("host-exception", "PT_INTERNAL", "unexpected host-side exception")])
+def test_host_exception_in_a_solve_returns_a_status_and_the_context_survives(ctx, fault, status, msg):
+    """A C++ exception inside pt_poisson_solve (thrown by the test hook after
+    the argument checks) comes back as a status with the message on the
+    context; the context's lock is released and the next solve is unchanged."""
+    from paintop_b200 import _lib
+    src, tgt, mask, W, H, Ch = _problem()
+    want, per, _ = ctx.solve(src, tgt, mask, W, H, Ch, lam=0.01)
+    with injected(fault):
+        with pytest.raises(_lib.CudaError) as e:
+            ctx.solve(src, tgt, mask, W, H, Ch, lam=0.01)
+    assert e.value.status == getattr(_lib, status)
+    assert msg in ctx.last_error()
     got, per2, _ = ctx.solve(src, tgt, mask, W, H, Ch, lam=0.01)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     assert [r["iterations"] for r in per2] == [r["iterations"] for r in per]

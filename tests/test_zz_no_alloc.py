@@ -155,3 +155,16 @@ def test_noalloc_size_limit_is_checked_before_the_gpu(cuda_lib):
     p = _problem(width=2048, height=2048, channels=4, max_it=2000)
     assert cuda_lib.pt_poisson_solve_noalloc(C.byref(p), 0x1000, (_lib.PtReport * 5)(), None,
                                              None) == _lib.PT_OOM
+
+
+@pytest.mark.parametrize("fault,status", [("host-oom", "PT_OOM"), ("host-exception", "PT_INTERNAL")])
+def test_noalloc_host_exception_becomes_a_status(cuda_lib, monkeypatch, fault, status):
+    """A C++ exception thrown inside the entry point (here by the test hook,
+    after the argument checks and before any device work) is returned as a
+    status: host allocation failure as PT_OOM, anything else as PT_INTERNAL.
+    Nothing unwinds through the C ABI."""
+    from paintop_b200 import _lib
+    monkeypatch.setenv("PAINTOP_CUDA_FAULT", fault)
+    p = _problem()
+    st = cuda_lib.pt_poisson_solve_noalloc(C.byref(p), 0x1000, (_lib.PtReport * 4)(), None, None)
+    assert st == getattr(_lib, status)
