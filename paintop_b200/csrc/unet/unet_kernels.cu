@@ -117,31 +117,54 @@ __device__ __forceinline__ void up_taps(int o, int n, int &i0, int &i1, float &w
   w0 = 0.75f;
   w1 = 0.25f;
 }
+// One thread per input pixel x of input row y writes the 2x2 output block
+// (2y .. 2y+1, 2x .. 2x+1): it loads the input's 3x3 neighbourhood once
+// (clamped at the border), interpolates each of the three rows horizontally
+// for output columns 2x and 2x+1, then those vertically. Every output is
+// w0 (w0 a + w1 b) + w1 (w0 c + w1 d), the same expression as a per-output
+// gather, so the result does not depend on the traversal.
 __global__ void k_upsample2(ActView in, ActView out, int B, int Hi, int Wi, int groups) {
   const int Ho = 2 * Hi, Wo = 2 * Wi;
-  const int rows = B * groups * Ho;
+  const int rows = B * groups * Hi;
+  constexpr float w0 = 0.75f, w1 = 0.25f;
   for (int r = blockIdx.x * blockDim.y + threadIdx.y; r < rows; r += gridDim.x * blockDim.y) {
     int b, g, y;
-    row_of(r, groups, Ho, b, g, y);
-    int y0, y1;
-    float wy0, wy1;
-    up_taps(y, Hi, y0, y1, wy0, wy1);
-    const __nv_bfloat16 *r0 = in.p + act_index(in, b, g, y0, 0, Hi, Wi);
-    const __nv_bfloat16 *r1 = in.p + act_index(in, b, g, y1, 0, Hi, Wi);
-    __nv_bfloat16 *o_row = out.p + act_index(out, b, g, y, 0, Ho, Wo);
-    for (int x = threadIdx.x; x < Wo; x += blockDim.x) {
-      int x0, x1;
-      float wx0, wx1;
-      up_taps(x, Wi, x0, x1, wx0, wx1);
-      float a00[8], a01[8], a10[8], a11[8], o[8];
-      ld8(r0 + (long long)x0 * 8, a00);
-      ld8(r0 + (long long)x1 * 8, a01);
-      ld8(r1 + (long long)x0 * 8, a10);
-      ld8(r1 + (long long)x1 * 8, a11);
+    row_of(r, groups, Hi, b, g, y);
+    const __nv_bfloat16 *rm = in.p + act_index(in, b, g, max(y - 1, 0), 0, Hi, Wi);
+    const __nv_bfloat16 *rc = in.p + act_index(in, b, g, y, 0, Hi, Wi);
+    const __nv_bfloat16 *rp = in.p + act_index(in, b, g, min(y + 1, Hi - 1), 0, Hi, Wi);
+    __nv_bfloat16 *o0 = out.p + act_index(out, b, g, 2 * y, 0, Ho, Wo);
+    __nv_bfloat16 *o1 = out.p + act_index(out, b, g, 2 * y + 1, 0, Ho, Wo);
+    for (int x = threadIdx.x; x < Wi; x += blockDim.x) {
+      const int xl = max(x - 1, 0), xr = min(x + 1, Wi - 1);
+      // horizontal: L = output column 2x (with x - 1), R = 2x + 1 (with x + 1)
+      float mL[8], mR[8], cL[8], cR[8], pL[8], pR[8];
+      {
+        float v[8], l[8], rr[8];
+        ld8(rm + x * 8, v); ld8(rm + xl * 8, l); ld8(rm + xr * 8, rr);
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        o[j] = wy0 * (wx0 * a00[j] + wx1 * a01[j]) + wy1 * (wx0 * a10[j] + wx1 * a11[j]);
-      st8(o_row + (long long)x * 8, o);
+        for (int j = 0; j < 8; ++j) { mL[j] = w0 * v[j] + w1 * l[j]; mR[j] = w0 * v[j] + w1 * rr[j]; }
+        ld8(rc + x * 8, v); ld8(rc + xl * 8, l); ld8(rc + xr * 8, rr);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) { cL[j] = w0 * v[j] + w1 * l[j]; cR[j] = w0 * v[j] + w1 * rr[j]; }
+        ld8(rp + x * 8, v); ld8(rp + xl * 8, l); ld8(rp + xr * 8, rr);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) { pL[j] = w0 * v[j] + w1 * l[j]; pR[j] = w0 * v[j] + w1 * rr[j]; }
+      }
+      // vertical: output row 2y takes rows y, y - 1; row 2y + 1 rows y, y + 1
+      float o[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) o[j] = w0 * cL[j] + w1 * mL[j];
+      st8(o0 + (2 * x) * 8, o);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) o[j] = w0 * cR[j] + w1 * mR[j];
+      st8(o0 + (2 * x + 1) * 8, o);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) o[j] = w0 * cL[j] + w1 * pL[j];
+      st8(o1 + (2 * x) * 8, o);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) o[j] = w0 * cR[j] + w1 * pR[j];
+      st8(o1 + (2 * x + 1) * 8, o);
     }
   }
 }
@@ -559,7 +582,7 @@ cudaError_t launch_unpool_add_mask(const ActView &dskip, const ActView &dpool, c
 }
 cudaError_t launch_upsample2(const ActView &in, const ActView &out, int B, int Hi, int Wi, int groups,
                              cudaStream_t st) {
-  k_upsample2<<<row_blocks((long long)B * groups * 2 * Hi, 2 * Wi), row_threads(2 * Wi), 0, st>>>(in, out, B, Hi, Wi, groups);
+  k_upsample2<<<row_blocks((long long)B * groups * Hi, Wi), row_threads(Wi), 0, st>>>(in, out, B, Hi, Wi, groups);
   return cudaGetLastError();
 }
 cudaError_t launch_upsample2_bwd(const ActView &dout, const ActView &act, const ActView &din, int B, int Hi,
