@@ -456,44 +456,27 @@ __global__ void k_compact(KParams P) {
 
 // Interleave the result: interior cells take (float)u (the reference's `as f32`,
 // poisson_blend.rs:211-219); every other pixel copies the target bit for bit.
-// A block takes one (row, tile column) segment at a time: its thread t the
-// pixel tile column * TW + t (TW <= 112 < 128 threads), so the tile's activity
-// is uniform and no per-pixel division is needed. The channels' plane offsets
-// and their "output stays the target" flags (the solve's final state) are
-// read once per block.
-constexpr int kEmitThreads = 128;
-constexpr int kEmitMaxC = 8;  // channels with block-shared descriptors; more are read per pixel
-static_assert(kLW - 2 * halo_x(1) <= kEmitThreads, "a tile row fits one emit block");
-__global__ void __launch_bounds__(kEmitThreads) k_emit(KParams P, int sys0, int TW, int TH) {
-  __shared__ long long s_off[kEmitMaxC];
-  __shared__ int s_keep[kEmitMaxC];
+__global__ void k_emit(KParams P, int sys0, int TW, int TH) {
   const SysDesc d0 = P.sys[sys0];
-  const int C = d0.C, W = d0.W, ntx = d0.ntx;
-  if (threadIdx.x < C && threadIdx.x < kEmitMaxC) {
-    s_off[threadIdx.x] = P.sys[sys0 + threadIdx.x].off;
-    s_keep[threadIdx.x] = P.st[sys0 + threadIdx.x].out_anchor;
-  }
-  __syncthreads();
+  const long long npx = (long long)d0.W * d0.H;
+  const int C = d0.C;
   // four channels with 16-byte aligned images: one vector load and store per pixel
   const bool vec4 = C == 4 && ((reinterpret_cast<uintptr_t>(d0.tgt) | reinterpret_cast<uintptr_t>(d0.out)) & 15) == 0;
-  const int nseg = d0.H * ntx;
-  for (int sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
-    const int y = sg / ntx, tx = sg - y * ntx;
-    const int x = tx * TW + (int)threadIdx.x;
-    if ((int)threadIdx.x >= TW || x >= W) continue;
+  for (long long px = blockIdx.x * (long long)blockDim.x + threadIdx.x; px < npx;
+       px += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(px / d0.W), x = (int)(px - (long long)y * d0.W);
+    const int tx = x / TW, ty = y / TH;
+    const int c = (x + y) & 1, i = x >> 1;
     // the channels share the tile counts (k_tile_count stores one per channel)
-    const bool active = P.tcount[d0.tile0 + (y / TH) * ntx + tx] > 0;
-    const long long px = (long long)y * W + x;
-    // the pixel's cell within a channel's pools: colour plane, row, index
-    const long long cell = (long long)((x + y) & 1) * d0.plane + (long long)y * d0.pw + (x >> 1);
+    const bool active = P.tcount[d0.tile0 + ty * d0.ntx + tx] > 0;
     if (vec4) {
       float4 v = *reinterpret_cast<const float4 *>(d0.tgt + px * 4);
       if (active) {
         float *vv = reinterpret_cast<float *>(&v);
 #pragma unroll
         for (int ch = 0; ch < 4; ++ch) {
-          if (s_keep[ch]) continue;
-          const long long o = s_off[ch] + cell;
+          if (P.st[sys0 + ch].out_anchor) continue;
+          const long long o = plane_index(P.sys[sys0 + ch], c, y, i);
           if (P.cell[o]) vv[ch] = (float)P.u[o];
         }
       }
@@ -501,13 +484,13 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit(KParams P, int sys0, int 
       continue;
     }
     for (int ch = 0; ch < C; ++ch) {
-      float v = d0.tgt[px * C + ch];
-      const bool keep = ch < kEmitMaxC ? s_keep[ch] != 0 : P.st[sys0 + ch].out_anchor != 0;
-      if (active && !keep) {
-        const long long o = (ch < kEmitMaxC ? s_off[ch] : P.sys[sys0 + ch].off) + cell;
+      const SysDesc &d = P.sys[sys0 + ch];
+      float v = d.tgt[px * C + ch];
+      if (active && !P.st[sys0 + ch].out_anchor) {
+        const long long o = plane_index(d, c, y, i);
         if (P.cell[o]) v = (float)P.u[o];
       }
-      d0.out[px * C + ch] = v;
+      d.out[px * C + ch] = v;
     }
   }
 }
@@ -1126,10 +1109,9 @@ cudaError_t launch_band_flags(const KParams &P, int sys0, int *spans, cudaStream
 cudaError_t launch_emit(const KParams &P, int sys0, const TileConfig &tc, long long npx,
                         cudaStream_t stream) {
   if (npx <= 0) return cudaSuccess;
-  // one block per (row, tile column) segment, at most 16 per SM
-  long long segs = (npx + tc.tw - 1) / tc.tw;  // no more than the image has segments
-  if (segs > 148 * 16) segs = 148 * 16;
-  k_emit<<<(int)segs, kEmitThreads, 0, stream>>>(P, sys0, tc.tw, tc.th);
+  long long blocks = (npx + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_emit<<<(int)blocks, 256, 0, stream>>>(P, sys0, tc.tw, tc.th);
   return cudaGetLastError();
 }
 
